@@ -1,0 +1,397 @@
+#!/usr/bin/env python
+"""Benchmark of the flat EZ field update on the 512^3 force-free turbulence
+problem: cell-updates per second of the full LSRK(5,4) step (5 stages + the
+Kreiss-Oliger pass) in FP32, with the algorithmic HBM bandwidth per step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: 512^3 interior points + 3 guards per side, periodic unit box,
+dt = 0.5 dx, seeded random force-free turbulence (B = xhat + 32 Fourier modes
+with |n| in [2, 8], |dB_k|^2 ~ k^-2, rms dB = 0.3; E = -v x B with an 8-mode
+drift |v| <= 0.45), the semantics of the reference's CPU build.  The fields
+(21 arrays x 556 MB resident) exceed the 126 MB L2 many times over, so no
+L2 flush is needed between steps.
+
+A "step" is one evolve_fields call over the whole grid.  The timed region is
+K steps in one call of the library on the torch stream, bracketed by a
+barrier and device synchronisation; with --gpus N (under torchrun) every rank
+advances its own replica and the time is the max over ranks.
+
+--impl reference times the reference's own CPU build (oracle/_ref, compiled
+from its sources; else the oracle restatement) on the host cores: one
+single-threaded process per core, each on a 512 x 512 x 8 periodic slab of
+the same problem, aggregate cell-updates/s.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s & HBM GB/s per RK step; time-to-steady-state warm vs cold"
+UNIT = "cell-updates/s"
+N_SIDE = 512
+# algorithmic bytes (FP32) per interior point: 112 per LSRK stage (read
+# U[7] + dU[7], write U'[7] + dU'[7]); 56 for the KO pass; 616 per step
+BYTES_STAGE = 112
+BYTES_STEP = 616
+SLAB_Z = 8
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _profiled_traffic():
+    """DRAM bytes per interior point of one stage launch, from the committed
+    ncu summary (profiles/ez_stage_kernel.md), or None."""
+    path = os.path.join(ROOT, "profiles", "ez_stage_kernel.md")
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"dram_bytes_per_point:\s*([0-9.]+)", txt)
+    return float(m.group(1)) if m else None
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 100 ms."""
+
+    QUERY = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.device)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+        time.sleep(0.4)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.time(), line.strip()))
+
+    def stop(self, t0, t1):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sel = [ln for (ts, ln) in self.lines if t0 - 0.05 <= ts <= t1 + 0.15]
+        if not sel:
+            sel = [ln for (_, ln) in self.lines[-3:]]
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in sel:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 10:
+                continue
+            try:
+                sm.append(float(parts[2]))
+                smax.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[6:10]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------- CPU reference
+
+def _slab_input(tmpdir, steps_dtype="f32"):
+    import numpy as np
+
+    from coffee_b200 import problems
+    from coffee_b200.fld import write_fld
+
+    p = problems.turbulence_params(N_SIDE)
+    p.N = [N_SIDE, N_SIDE, SLAB_Z]
+    p.size = [1.0, 1.0, SLAB_Z / N_SIDE]
+    f = problems.turbulence_fields(p, np.float32)
+    path = os.path.join(tmpdir, "slab.fld")
+    write_fld(path, f, guard=tuple(p.guard))
+    cfg = os.path.join(tmpdir, "config.toml")
+    p.write_toml(cfg)
+    return p, path, cfg
+
+
+def cpu_reference_run(steps: int, warmup: int, nproc: int | None = None):
+    """Run the reference CPU build (or the restatement) on host cores.
+
+    Returns dict(value, cores, kind, sample, seconds)."""
+    from oracle import oracle
+
+    cores = nproc or len(os.sched_getaffinity(0))
+    cores = max(1, min(cores, 128))
+    tmp = tempfile.mkdtemp(prefix="coffee_cpu_")
+    try:
+        p, fin, cfg = _slab_input(tmp)
+        cells = N_SIDE * N_SIDE * SLAB_Z
+        if oracle.reference_available():
+            exe = oracle.ref_binary()
+            env = dict(os.environ, COFFEE_ORACLE_CONFIG=cfg)
+            procs = []
+            for r in range(cores):
+                out = os.path.join(tmp, f"out{r}.fld")
+                procs.append(subprocess.Popen([exe, fin, out, str(steps), "--warmup", str(warmup)],
+                                              cwd=tmp, env=env, stdout=subprocess.PIPE,
+                                              stderr=subprocess.PIPE, text=True))
+            secs = []
+            for pr in procs:
+                o, e = pr.communicate()
+                if pr.returncode != 0:
+                    raise RuntimeError(f"reference CPU build failed: {e[-500:]}")
+                secs.append(json.loads(o.strip().splitlines()[-1])["seconds"])
+            wall = max(secs)
+            kind = "reference"
+            sample = (f"{cores} concurrent single-threaded processes of the reference CPU build "
+                      f"(oracle/_ref/coffee_ref_float), each a periodic {N_SIDE}x{N_SIDE}x{SLAB_Z} "
+                      f"slab of the turbulence problem, {steps} timed steps after {warmup} warm-up")
+        else:
+            import numpy as np
+
+            from coffee_b200.fld import read_fld
+
+            f = [a.copy() for a in read_fld(fin).arrays]
+            oracle.run_port(p, f, warmup)
+            t0 = time.perf_counter()
+            oracle.run_port(p, f, steps)
+            wall = time.perf_counter() - t0
+            cores = len(os.sched_getaffinity(0))
+            kind = "port"
+            sample = (f"oracle restatement (OpenMP, {cores} threads) on one periodic "
+                      f"{N_SIDE}x{N_SIDE}x{SLAB_Z} slab, {steps} steps")
+            cells = N_SIDE * N_SIDE * SLAB_Z
+            return {"value": cells * steps / wall, "cores": cores, "kind": kind,
+                    "sample": sample, "seconds": wall}
+        return {"value": cells * cores * steps / wall, "cores": cores, "kind": kind,
+                "sample": sample, "seconds": wall}
+    finally:
+        for fn in os.listdir(tmp):
+            os.unlink(os.path.join(tmp, fn))
+        os.rmdir(tmp)
+
+
+# ------------------------------------------------------------------ arms
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_reference_arm(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    r = cpu_reference_run(args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * r["seconds"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded random force-free turbulence)",
+        "config": {"workload": "turbulence512 (CPU sample: 512x512x8 slabs)", "grid": [512, 512, 512],
+                   "guard": 3, "periodic": True, "cfl": 0.5, "semantics": "reference CPU build"},
+        "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+                         "sample": r["sample"]},
+        "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from coffee_b200 import problems
+    from coffee_b200.solver import FieldSolverEZ, SimData, SimEnvironment
+
+    ws, rank, local = _dist()
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier(device_ids=[local])
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    p = problems.turbulence_params(N_SIDE)
+    cells = N_SIDE ** 3
+    env = SimEnvironment(p, device=local)
+    data = SimData(env, np.float32)
+    modes = problems.turbulence_modes()
+    data.init_fourier((1.0, 0.0, 0.0), *modes)
+    solver = FieldSolverEZ(data, env, "cpu", stream=stream.cuda_stream)
+    dt = np.float32(p.dt)
+
+    # warm-up (untimed)
+    t = np.float32(0.0)
+    solver.step(float(t), args.warmup)
+    for _ in range(args.warmup):
+        t = np.float32(t + dt)
+    barrier()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    solver.set_timing(True)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    w0 = time.time()
+    e0.record(stream)
+    solver.step(float(t), args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    w1 = time.time()
+    barrier()
+    clk = clocks.stop(w0, w1)
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(ms)
+    timing = solver.last_timing()
+    solver.set_timing(False)
+    solver.check_finite()
+
+    value = cells * args.steps * ws / (ms_max / 1e3)
+    step_ms = ms_max / args.steps
+    hbm_gbs = BYTES_STEP * cells / (step_ms / 1e3) / 1e9
+    n_stage = timing["launches"]["stage"]
+    avg_stage_ms = timing["ms"]["stage"] / max(1, n_stage)
+    achieved = BYTES_STAGE * cells / (avg_stage_ms / 1e3) / 1e9
+    peak, peak_kind = _peaks()
+    traffic_pp = _profiled_traffic()
+
+    # ---- end to end through the public API with host buffers
+    nbytes = 7 * data.env.dims[0] * data.env.dims[1] * data.env.dims[2] * 4
+    host = torch.empty(nbytes // 4, dtype=torch.float32, pin_memory=True)
+    hnp = host.numpy()
+    data.download_packed(hnp)
+    barrier()
+    tt = np.float32(0.0)
+    w0 = time.perf_counter()
+    data.upload_packed(hnp)
+    energies = []
+    for _ in range(args.steps):
+        solver.step(float(tt), 1)
+        tt = np.float32(tt + dt)
+        energies.append(solver.total_energy("B"))
+    data.download_packed(hnp)
+    torch.cuda.synchronize(dev)
+    e2e_s = max_over_ranks(time.perf_counter() - w0)
+    barrier()
+    e2e_value = cells * args.steps * ws / e2e_s
+    d2h_diag = 8 * (148 * 4)  # FP64 partials read back per energy diagnostic
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_run(steps=2, warmup=1)
+        cpu = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": cpu["kind"],
+               "sample": cpu["sample"]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded random force-free turbulence, seed 20261203)",
+            "config": {"workload": "turbulence512", "grid": [N_SIDE] * 3, "guard": 3,
+                       "periodic": True, "cfl": 0.5, "semantics": "reference CPU build",
+                       "l2": "inputs larger than L2 (21 arrays x 556 MB resident), no flush",
+                       "parallelism": f"replicas x{ws}"},
+            "hbm_gbs": hbm_gbs,
+            "roofline": {"kernel": "ez_stage_kernel (LSRK stages 2-5)", "bound": "hbm",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": (traffic_pp * cells if traffic_pp else None),
+                         "algorithmic_bytes_per_launch": BYTES_STAGE * cells,
+                         "avg_launch_ms": avg_stage_ms},
+            "kernels_ms": {k: v for k, v in timing["ms"].items()},
+            "kernel_launches": timing["launches"],
+            "gpu_launches": sum(timing["launches"].values()),
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": nbytes / args.steps,
+                    "d2h_bytes_per_step": nbytes / args.steps + d2h_diag},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    data.close()
+    env.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

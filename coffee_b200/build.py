@@ -1,0 +1,62 @@
+"""Build libcoffee_b200.so in-tree with nvcc for sm_100a.
+
+    python -m coffee_b200.build [--verbose-ptxas]
+
+The library is compiled for B200 only (-gencode arch=compute_100a,code=sm_100a)
+and placed next to this file, where coffee_b200._lib loads it.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+LIB = os.path.join(HERE, "libcoffee_b200.so")
+
+SOURCES = ["coffee_abi.cu", "coffee_params.cpp"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc_path() -> str:
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _newest_input() -> float:
+    paths = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
+    paths += [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE)]
+    return max(os.path.getmtime(p) for p in paths if os.path.isfile(p))
+
+
+def build(force: bool = False, ptxas_verbose: bool = False, log=None) -> str:
+    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _newest_input():
+        return LIB
+    cmd = [nvcc_path(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "--shared",
+           "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+           "-I", INCLUDE, "-I", CSRC, "-DCOFFEE_BUILDING_LIBRARY",
+           "-o", LIB + ".tmp"]
+    if ptxas_verbose:
+        cmd += ["-Xptxas", "-v"]
+    cmd += [os.path.join(CSRC, s) for s in SOURCES]
+    cmd += ["-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    out = r.stdout + r.stderr
+    if log is not None:
+        log.write(out)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed ({r.returncode}):\n{out[-6000:]}")
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    verbose = "--verbose-ptxas" in sys.argv
+    build(force=True, ptxas_verbose=verbose, log=sys.stdout if verbose else None)
+    print(LIB)

@@ -1,0 +1,958 @@
+// C ABI of the B200 field-update library (declared in include/coffee_b200.h):
+// environment, field storage, the flat EZ solver and its diagnostics.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "coffee_b200.h"
+#include "coffee_fld.h"
+#include "coffee_internal.h"
+#include "ez_kernels.cuh"
+
+#define COFFEE_VERSION_STRING "coffee_b200 0.1 (sm_100a)"
+
+namespace coffee {
+
+static thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+void clear_error() { g_last_error.clear(); }
+
+}  // namespace coffee
+
+using namespace coffee;
+
+// ------------------------------------------------------------------ handles
+
+struct coffee_env {
+  coffee_params p;
+  coffee_grid grid;
+  int device;
+};
+
+struct coffee_fields {
+  coffee_env* env;
+  int elem;                          // 4 or 8
+  size_t n;                          // points per array, guards included
+  void* d[COFFEE_NUM_FIELDS];        // device arrays; J/divE/divB allocated on demand
+  uint64_t generation;               // bumped whenever the host may have changed the fields
+};
+
+struct coffee_solver {
+  coffee_env* env;
+  coffee_fields* f;
+  int variant;
+  int semantics;
+  cudaStream_t stream;
+  void* B[7];   // second field buffer (stages alternate A -> B -> A ...)
+  void* dU[7];  // LSRK accumulators dE, dB, dP
+  void* Un[7];  // start-of-step copy, read by the absorbing layer
+  bool absorbing;
+  int aux;
+  int timing;
+  uint64_t synced_generation;
+  int kchunk_stage, kchunk_ko;
+  dim3 grid_stage, grid_ko;
+  std::vector<cudaEvent_t> events;   // pairs around each launch (timing mode)
+  std::vector<int> event_kind;       // COFFEE_KERNEL_* of each pair
+  int events_used;
+  cudaEvent_t ev_begin, ev_end;
+  double* d_partials;
+  int* d_count;
+  int partial_blocks;
+};
+
+// ------------------------------------------------------------ kernel shapes
+
+namespace {
+
+template <typename T> struct Shape;
+template <> struct Shape<float> {
+  static constexpr int STX = 32, STY = 8, SPF = 2;  // stage tile, prefetch depth
+  static constexpr int KTX = 32, KTY = 4, KPF = 3;  // KO tile, prefetch depth
+};
+template <> struct Shape<double> {
+  static constexpr int STX = 32, STY = 4, SPF = 1;
+  static constexpr int KTX = 32, KTY = 4, KPF = 1;
+};
+
+template <typename T>
+size_t stage_smem(bool first) {
+  using S = Shape<T>;
+  return first ? TileCfg<T, S::STX, S::STY, 2, S::SPF, false>::smem_bytes
+               : TileCfg<T, S::STX, S::STY, 2, S::SPF, true>::smem_bytes;
+}
+template <typename T>
+size_t ko_smem() {
+  using S = Shape<T>;
+  return TileCfg<T, S::KTX, S::KTY, 3, S::KPF, false>::smem_bytes;
+}
+
+// LSRK(5,4) coefficients of the reference (field_solver_EZ.cpp:1009-1014)
+const double kAs[5] = {0, -0.4178904745, -1.192151694643, -1.697784692471, -1.514183444257};
+const double kBs[5] = {0.1496590219993, 0.3792103129999, 0.8229550293869, 0.6994504559488,
+                       0.1530572479681};
+const double kCs[5] = {0, 0.1496590219993, 0.3704009573644, 0.6222557631345, 0.9582821306784};
+
+// Choose the z chunk of a CTA: enough CTAs to fill the GPU in whole waves,
+// while the 2H halo planes each chunk re-reads stay a small fraction.
+int pick_kchunk(int nz, int nxy_tiles, int slots, int halo) {
+  int best = nz;
+  double best_cost = 1e300;
+  for (int kc = 4; kc <= nz + 3; kc += 4) {
+    const int kk = std::min(kc, nz);
+    const long long ctas = (long long)nxy_tiles * ((nz + kk - 1) / kk);
+    const double waves = std::ceil((double)ctas / (double)slots);
+    const double cost = waves * (kk + 0.5 * halo);
+    if (cost < best_cost - 1e-9) {
+      best_cost = cost;
+      best = kk;
+    }
+    if (kk == nz) break;
+  }
+  return best;
+}
+
+template <typename T>
+void build_const(const coffee_env* env, int semantics, EzConst<T>* c) {
+  const coffee_params& p = env->p;
+  const coffee_grid& gr = env->grid;
+  std::memset(c, 0, sizeof(*c));
+  GridGeom& g = c->g;
+  for (int a = 0; a < 3; ++a) {
+    g.dims[a] = gr.dims[a];
+    g.guard[a] = gr.guard[a];
+    g.N[a] = gr.dims[a] - 2 * gr.guard[a];
+    g.lo[a] = gr.guard[a] - p.shift_ghost;
+    g.hi[a] = gr.dims[a] - gr.guard[a] + p.shift_ghost;
+    g.periodic[a] = p.periodic_boundary[a] ? 1 : 0;
+    c->delta[a] = (T)(T(p.size[a]) / (T)p.N[a]);
+    c->inv_delta[a] = (T)(1.0 / (double)c->delta[a]);
+    c->lower[a] = (T)p.lower[a];
+  }
+  g.sy = gr.dims[0];
+  g.sz = (long long)gr.dims[0] * gr.dims[1];
+  c->dt = (T)p.dt;
+  c->ch2 = (T)p.ch2;
+  c->tau = (T)p.tau;
+  // -KOeps * KO_const with KO_const = -1/64 (FFE_DISSIPATION_ORDER 6)
+  c->ko_c = -(T)p.KOeps * (T)(-1.0 / 64.0);
+  c->gam_dt = (T)p.damp_gamma / (T)p.dt;
+  c->use_edotb = p.use_edotb_damping;
+  c->divB_clean = p.divB_clean;
+  c->clean_ep = p.clean_ep;
+  c->check_egb = p.check_egb;
+  c->semantics = semantics;
+  c->taper_lanes = (sizeof(T) == 4) ? 16 : 8;  // AVX-512 width of the reference CPU build
+  c->problem = p.problem;
+  bool abs_any = p.shift_ghost > 0;
+  for (int a = 0; a < 3; ++a) {
+    const T pm = (T)p.pml[a] * c->delta[a];
+    c->pml_hi[a] = (T)p.lower[a] + (T)p.size[a] - pm;
+    c->pml_lo[a] = (T)p.lower[a] + pm;
+    c->pml_scale[a] = (T)p.pmllen * (semantics == SEM_CPU_REF ? c->delta[a] : c->delta[0]);
+    if (p.pml[a] > 0) abs_any = true;
+  }
+  c->absorbing = abs_any ? 1 : 0;
+  c->sigpml = (T)p.sigpml;
+  c->radius = (T)p.radius;
+  c->omega = (T)p.omega;
+  c->b0 = (T)p.b0;
+  c->p1 = (T)p.p1; c->p2 = (T)p.p2; c->p3 = (T)p.p3;
+  c->q11 = (T)p.q11; c->q12 = (T)p.q12; c->q13 = (T)p.q13; c->q22 = (T)p.q22;
+  c->q23 = (T)p.q23;
+  c->qox = (T)p.q_offset_x; c->qoy = (T)p.q_offset_y; c->qoz = (T)p.q_offset_z;
+  c->tp_start = (T)p.tp_start; c->tp_end = (T)p.tp_end; c->rpert1 = (T)p.rpert1;
+  c->rpert2 = (T)p.rpert2; c->dw0 = (T)p.dw0; c->nT = (T)p.nT; c->ph1 = (T)p.ph1;
+  c->ph2 = (T)p.ph2; c->dph = (T)p.dph; c->theta0 = (T)p.theta0; c->drpert = (T)p.drpert;
+  c->tp_start1 = (T)p.tp_start1; c->tp_end1 = (T)p.tp_end1; c->rpert11 = (T)p.rpert11;
+  c->rpert21 = (T)p.rpert21; c->dw1 = (T)p.dw1; c->nT1 = (T)p.nT1; c->ph11 = (T)p.ph11;
+  c->ph21 = (T)p.ph21; c->dph1 = (T)p.dph1;
+  c->pert_type = p.pert_type;
+}
+
+template <typename T>
+F7<T> f7(void* const* a) {
+  F7<T> r;
+  for (int f = 0; f < 7; ++f) r.p[f] = static_cast<T*>(a[f]);
+  return r;
+}
+template <typename T>
+F7<const T> f7c(void* const* a) {
+  F7<const T> r;
+  for (int f = 0; f < 7; ++f) r.p[f] = static_cast<const T*>(a[f]);
+  return r;
+}
+
+// Periodic guard fill of all 7 arrays: every guard point of a periodic axis
+// takes the value of the interior point at the wrapped coordinates.
+template <typename T>
+__global__ void fill_guards_kernel(const GridGeom g, const F7<T> u, const long long n) {
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx % g.dims[0]);
+    const int j = (int)((idx / g.dims[0]) % g.dims[1]);
+    const int k = (int)(idx / g.sz);
+    int c[3] = {i, j, k};
+    bool moved = false;
+    for (int a = 0; a < 3; ++a) {
+      if (!g.periodic[a]) continue;
+      if (c[a] < g.guard[a]) { c[a] += g.N[a]; moved = true; }
+      else if (c[a] >= g.dims[a] - g.guard[a]) { c[a] -= g.N[a]; moved = true; }
+    }
+    if (!moved) continue;
+    const long long src = (long long)c[2] * g.sz + (long long)c[1] * g.sy + c[0];
+    for (int f = 0; f < 7; ++f) u.p[f][idx] = u.p[f][src];
+  }
+}
+
+// ----------------------------------------------------------- diagnostics
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// One FP64 partial per block over the interior points.  what: see
+// COFFEE_DIAG_*.  The energy region is that of total_energy
+// (field_solver_EZ.cu:755-795): outside the star (problem 1) and strictly
+// inside the absorbing layers.
+template <typename T>
+__global__ void diag_kernel(const EzConst<T> c, const F7<const T> u, const int what,
+                            const T pml_xl0, const T pml_xl1, const T pml_xl2, const T pml_xh0,
+                            const T pml_xh1, const T pml_xh2, double* partials) {
+  const GridGeom& g = c.g;
+  const int n0 = g.N[0], n1 = g.N[1], n2 = g.N[2];
+  const long long total = (long long)n0 * n1 * n2;
+  const bool is_max = (what == COFFEE_DIAG_MAX_EDOTB || what == COFFEE_DIAG_MAX_EOVERB);
+  double acc = 0.0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int i = g.guard[0] + (int)(q % n0);
+    const int j = g.guard[1] + (int)((q / n0) % n1);
+    const int k = g.guard[2] + (int)(q / ((long long)n0 * n1));
+    const long long o = (long long)k * g.sz + (long long)j * g.sy + i;
+    double v = 0.0;
+    if (what == COFFEE_DIAG_ENERGY_E || what == COFFEE_DIAG_ENERGY_B) {
+      const T x = grid_pos(c, 0, i), y = grid_pos(c, 1, j), z = grid_pos(c, 2, k);
+      const T r = sqrt(x * x + y * y + z * z);
+      const bool in_star = (c.problem == 1 && r < c.radius);
+      if (!in_star && x < pml_xh0 && x > pml_xl0 && y < pml_xh1 && y > pml_xl1 &&
+          z < pml_xh2 && z > pml_xl2) {
+        const int b = (what == COFFEE_DIAG_ENERGY_E) ? 0 : 3;
+        for (int a = 0; a < 3; ++a) {
+          const double f = (double)u.p[b + a][o];
+          v += f * f;
+        }
+      }
+    } else if (what == COFFEE_DIAG_DIVB_L2) {
+      double d = 0.0;
+      const long long s[3] = {1, g.sy, g.sz};
+      for (int a = 0; a < 3; ++a) {
+        const T* f = u.p[3 + a];
+        const double m2 = f[o - 2 * s[a]], m1 = f[o - s[a]], p1 = f[o + s[a]], p2 = f[o + 2 * s[a]];
+        d += ((m2 - p2) + 8.0 * (p1 - m1)) / 12.0 * (double)c.inv_delta[a];
+      }
+      v = d * d;
+    } else {
+      const double ex = u.p[0][o], ey = u.p[1][o], ez = u.p[2][o];
+      const double bx = u.p[3][o], by = u.p[4][o], bz = u.p[5][o];
+      const double B2 = fmax(bx * bx + by * by + bz * bz, (double)Tiny<T>::v);
+      if (what == COFFEE_DIAG_MAX_EDOTB)
+        v = fabs(ex * bx + ey * by + ez * bz) / B2;
+      else
+        v = sqrt((ex * ex + ey * ey + ez * ez) / B2);
+    }
+    acc = is_max ? fmax(acc, v) : acc + v;
+  }
+  __shared__ double red[32];
+  acc = is_max ? warp_max(acc) : warp_sum(acc);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) red[wid] = acc;
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    double v = lane < nw ? red[lane] : 0.0;
+    v = is_max ? warp_max(v) : warp_sum(v);
+    if (lane == 0) partials[blockIdx.x] = v;
+  }
+}
+
+template <typename T>
+__global__ void count_nonfinite_kernel(const F7<const T> u, const long long n, int* count) {
+  int local = 0;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+       idx += (long long)gridDim.x * blockDim.x)
+    for (int f = 0; f < 7; ++f)
+      if (!isfinite((double)u.p[f][idx])) ++local;
+  for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+  if ((threadIdx.x & 31) == 0 && local) atomicAdd(count, local);
+}
+
+int num_sms(int device) {
+  int n = 148;
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device);
+  return n;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ errors
+
+extern "C" const char* coffee_last_error_string(void) { return g_last_error.c_str(); }
+extern "C" const char* coffee_version(void) { return COFFEE_VERSION_STRING; }
+
+// --------------------------------------------------------------- env
+
+extern "C" int coffee_env_create(const coffee_params* p, int device, coffee_env** out) {
+  clear_error();
+  if (!p || !out) return fail(COFFEE_E_INVALID, "coffee_env_create: null argument");
+  *out = nullptr;
+  for (int a = 0; a < 3; ++a) {
+    if (p->N[a] < 1) return fail(COFFEE_E_CONFIG, "N[%d] = %d must be >= 1", a, p->N[a]);
+    if (p->guard[a] < p->shift_ghost + 3)
+      return fail(COFFEE_E_CONFIG,
+                  "guard[%d] = %d: the KO stencil needs guard >= shift_ghost + 3 = %d", a,
+                  p->guard[a], p->shift_ghost + 3);
+    if (p->periodic_boundary[a] && p->N[a] < p->guard[a])
+      return fail(COFFEE_E_CONFIG, "periodic axis %d needs N >= guard (N=%d, guard=%d)", a,
+                  p->N[a], p->guard[a]);
+    if (!(p->size[a] > 0)) return fail(COFFEE_E_CONFIG, "size[%d] must be > 0", a);
+  }
+  if (p->shift_ghost < 0) return fail(COFFEE_E_CONFIG, "shift_ghost must be >= 0");
+  if (!(p->dt > 0)) return fail(COFFEE_E_CONFIG, "dt must be > 0");
+  if (p->tau == 0) return fail(COFFEE_E_CONFIG, "tau must be nonzero");
+  const long long pts = (long long)(p->N[0] + 2 * p->guard[0]) * (p->N[1] + 2 * p->guard[1]) *
+                        (p->N[2] + 2 * p->guard[2]);
+  if (pts > (1LL << 40)) return fail(COFFEE_E_CONFIG, "grid too large");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(COFFEE_E_CUDA, "no CUDA device available");
+  if (device < 0 || device >= ndev) return fail(COFFEE_E_INVALID, "device %d out of range", device);
+  coffee_env* e = new (std::nothrow) coffee_env;
+  if (!e) return fail(COFFEE_E_NOMEM, "out of host memory");
+  e->p = *p;
+  e->device = device;
+  // sim_environment::sim_environment (src/sim_env_impl.hpp:52-60), one rank
+  for (int a = 0; a < 3; ++a) {
+    e->grid.guard[a] = p->guard[a];
+    e->grid.sizes[a] = (float)p->size[a];
+    e->grid.lower[a] = p->lower[a];
+    e->grid.dims[a] = p->N[a] + 2 * p->guard[a];
+    e->grid.delta[a] = p->size[a] / p->N[a];
+    e->grid.inv_delta[a] = 1.0 / e->grid.delta[a];
+    e->grid.offset[a] = 0;
+  }
+  *out = e;
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_env_destroy(coffee_env* env) {
+  delete env;
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_env_grid(const coffee_env* env, coffee_grid* grid) {
+  if (!env || !grid) return fail(COFFEE_E_INVALID, "coffee_env_grid: null argument");
+  *grid = env->grid;
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_env_params(const coffee_env* env, coffee_params* p) {
+  if (!env || !p) return fail(COFFEE_E_INVALID, "coffee_env_params: null argument");
+  *p = env->p;
+  return COFFEE_OK;
+}
+
+// ------------------------------------------------------------------ fields
+
+extern "C" int coffee_fields_create(coffee_env* env, int elem_size, coffee_fields** out) {
+  clear_error();
+  if (!env || !out) return fail(COFFEE_E_INVALID, "coffee_fields_create: null argument");
+  if (elem_size != 4 && elem_size != 8)
+    return fail(COFFEE_E_INVALID, "elem_size must be 4 or 8, got %d", elem_size);
+  *out = nullptr;
+  COFFEE_CUDA_TRY(cudaSetDevice(env->device));
+  coffee_fields* f = new (std::nothrow) coffee_fields;
+  if (!f) return fail(COFFEE_E_NOMEM, "out of host memory");
+  std::memset(f, 0, sizeof(*f));
+  f->env = env;
+  f->elem = elem_size;
+  f->n = (size_t)env->grid.dims[0] * env->grid.dims[1] * env->grid.dims[2];
+  for (int a = 0; a < 7; ++a) {
+    cudaError_t err = cudaMalloc(&f->d[a], f->n * elem_size);
+    if (err == cudaSuccess) err = cudaMemset(f->d[a], 0, f->n * elem_size);
+    if (err != cudaSuccess) {
+      for (int b = 0; b <= a; ++b) cudaFree(f->d[b]);
+      delete f;
+      return fail(COFFEE_E_NOMEM, "cudaMalloc of field %d (%zu bytes) failed: %s", a,
+                  f->n * (size_t)elem_size, cudaGetErrorString(err));
+    }
+  }
+  f->generation = 1;
+  *out = f;
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_fields_destroy(coffee_fields* f) {
+  if (!f) return COFFEE_OK;
+  cudaSetDevice(f->env->device);
+  for (int a = 0; a < COFFEE_NUM_FIELDS; ++a)
+    if (f->d[a]) cudaFree(f->d[a]);
+  delete f;
+  return COFFEE_OK;
+}
+
+static int ensure_field(coffee_fields* f, int id) {
+  if (id < 0 || id >= COFFEE_NUM_FIELDS) return fail(COFFEE_E_INVALID, "field id %d out of range", id);
+  if (!f->d[id]) {
+    COFFEE_CUDA_TRY(cudaSetDevice(f->env->device));
+    COFFEE_CUDA_TRY(cudaMalloc(&f->d[id], f->n * f->elem));
+    COFFEE_CUDA_TRY(cudaMemset(f->d[id], 0, f->n * f->elem));
+  }
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_fields_ptr(coffee_fields* f, int id, void** dev_ptr) {
+  clear_error();
+  if (!f || !dev_ptr) return fail(COFFEE_E_INVALID, "coffee_fields_ptr: null argument");
+  int rc = ensure_field(f, id);
+  if (rc) return rc;
+  *dev_ptr = f->d[id];
+  if (id < 7) ++f->generation;  // the caller may write through it
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_fields_upload(coffee_fields* f, int id, const void* host) {
+  clear_error();
+  if (!f || !host) return fail(COFFEE_E_INVALID, "coffee_fields_upload: null argument");
+  COFFEE_CUDA_TRY(cudaSetDevice(f->env->device));
+  const size_t bytes = f->n * f->elem;
+  if (id == -1) {
+    for (int a = 0; a < 7; ++a)
+      COFFEE_CUDA_TRY(cudaMemcpy(f->d[a], (const char*)host + a * bytes, bytes,
+                                 cudaMemcpyHostToDevice));
+  } else {
+    int rc = ensure_field(f, id);
+    if (rc) return rc;
+    COFFEE_CUDA_TRY(cudaMemcpy(f->d[id], host, bytes, cudaMemcpyHostToDevice));
+  }
+  ++f->generation;
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_fields_download(coffee_fields* f, int id, void* host) {
+  clear_error();
+  if (!f || !host) return fail(COFFEE_E_INVALID, "coffee_fields_download: null argument");
+  COFFEE_CUDA_TRY(cudaSetDevice(f->env->device));
+  COFFEE_CUDA_TRY(cudaDeviceSynchronize());
+  const size_t bytes = f->n * f->elem;
+  if (id == -1) {
+    for (int a = 0; a < 7; ++a)
+      COFFEE_CUDA_TRY(
+          cudaMemcpy((char*)host + a * bytes, f->d[a], bytes, cudaMemcpyDeviceToHost));
+  } else {
+    int rc = ensure_field(f, id);
+    if (rc) return rc;
+    COFFEE_CUDA_TRY(cudaMemcpy(host, f->d[id], bytes, cudaMemcpyDeviceToHost));
+  }
+  return COFFEE_OK;
+}
+
+template <typename T>
+static int fill_guards_t(coffee_fields* f, cudaStream_t stream) {
+  EzConst<T> c;
+  build_const<T>(f->env, SEM_CPU_REF, &c);
+  const int threads = 256;
+  const long long n = (long long)f->n;
+  const int blocks = (int)std::min<long long>((n + threads - 1) / threads, 148LL * 32);
+  fill_guards_kernel<T><<<blocks, threads, 0, stream>>>(c.g, f7<T>(f->d), n);
+  COFFEE_CUDA_TRY(cudaGetLastError());
+  return COFFEE_OK;
+}
+
+namespace {
+struct FourierModes {
+  int nb, nv;
+  const double *kb, *bamp, *phib, *kv, *vamp, *phiv;  // device pointers
+};
+
+template <typename T>
+__global__ void init_fourier_kernel(const EzConst<T> c, const F7<T> u, const long long n,
+                                    const double b0x, const double b0y, const double b0z,
+                                    const FourierModes m) {
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx % c.g.dims[0]);
+    const int j = (int)((idx / c.g.dims[0]) % c.g.dims[1]);
+    const int k = (int)(idx / c.g.sz);
+    // coordinates of the vertex, as the host generator computes them (FP64)
+    const double x = (double)c.lower[0] + (double)c.delta[0] * (double)(i - c.g.guard[0]);
+    const double y = (double)c.lower[1] + (double)c.delta[1] * (double)(j - c.g.guard[1]);
+    const double z = (double)c.lower[2] + (double)c.delta[2] * (double)(k - c.g.guard[2]);
+    double B[3] = {b0x, b0y, b0z}, v[3] = {0, 0, 0};
+    for (int q = 0; q < m.nb; ++q) {
+      const double s = sin(m.kb[3 * q] * x + m.kb[3 * q + 1] * y + m.kb[3 * q + 2] * z + m.phib[q]);
+      for (int a = 0; a < 3; ++a) B[a] += m.bamp[3 * q + a] * s;
+    }
+    for (int q = 0; q < m.nv; ++q) {
+      const double s = sin(m.kv[3 * q] * x + m.kv[3 * q + 1] * y + m.kv[3 * q + 2] * z + m.phiv[q]);
+      for (int a = 0; a < 3; ++a) v[a] += m.vamp[3 * q + a] * s;
+    }
+    u.p[0][idx] = (T)(-(v[1] * B[2] - v[2] * B[1]));
+    u.p[1][idx] = (T)(-(v[2] * B[0] - v[0] * B[2]));
+    u.p[2][idx] = (T)(-(v[0] * B[1] - v[1] * B[0]));
+    u.p[3][idx] = (T)B[0];
+    u.p[4][idx] = (T)B[1];
+    u.p[5][idx] = (T)B[2];
+    u.p[6][idx] = (T)0;
+  }
+}
+}  // namespace
+
+extern "C" int coffee_fields_init_fourier(coffee_fields* f, const double b0[3], int nb,
+                                          const double* kb, const double* bamp,
+                                          const double* phib, int nv, const double* kv,
+                                          const double* vamp, const double* phiv) {
+  clear_error();
+  if (!f || !b0 || nb < 0 || nv < 0 || (nb > 0 && (!kb || !bamp || !phib)) ||
+      (nv > 0 && (!kv || !vamp || !phiv)))
+    return fail(COFFEE_E_INVALID, "coffee_fields_init_fourier: bad argument");
+  COFFEE_CUDA_TRY(cudaSetDevice(f->env->device));
+  const size_t nd = (size_t)7 * (nb + nv) + 1;
+  std::vector<double> h(nd, 0.0);
+  double* p = h.data();
+  std::memcpy(p, kb, sizeof(double) * 3 * nb);
+  std::memcpy(p + 3 * nb, bamp, sizeof(double) * 3 * nb);
+  std::memcpy(p + 6 * nb, phib, sizeof(double) * nb);
+  double* q = p + 7 * nb;
+  std::memcpy(q, kv, sizeof(double) * 3 * nv);
+  std::memcpy(q + 3 * nv, vamp, sizeof(double) * 3 * nv);
+  std::memcpy(q + 6 * nv, phiv, sizeof(double) * nv);
+  double* d = nullptr;
+  COFFEE_CUDA_TRY(cudaMalloc(&d, sizeof(double) * nd));
+  cudaError_t err = cudaMemcpy(d, h.data(), sizeof(double) * nd, cudaMemcpyHostToDevice);
+  if (err != cudaSuccess) {
+    cudaFree(d);
+    return fail(COFFEE_E_CUDA, "init_fourier upload: %s", cudaGetErrorString(err));
+  }
+  FourierModes m{nb, nv, d, d + 3 * nb, d + 6 * nb, d + 7 * nb, d + 7 * nb + 3 * nv,
+                 d + 7 * nb + 6 * nv};
+  const long long n = (long long)f->n;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 64);
+  if (f->elem == 4) {
+    EzConst<float> c;
+    build_const<float>(f->env, SEM_CPU_REF, &c);
+    init_fourier_kernel<float><<<blocks, 256>>>(c, f7<float>(f->d), n, b0[0], b0[1], b0[2], m);
+  } else {
+    EzConst<double> c;
+    build_const<double>(f->env, SEM_CPU_REF, &c);
+    init_fourier_kernel<double><<<blocks, 256>>>(c, f7<double>(f->d), n, b0[0], b0[1], b0[2], m);
+  }
+  err = cudaGetLastError();
+  if (err == cudaSuccess) err = cudaDeviceSynchronize();
+  cudaFree(d);
+  if (err != cudaSuccess) return fail(COFFEE_E_CUDA, "init_fourier: %s", cudaGetErrorString(err));
+  ++f->generation;
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_fields_fill_guards(coffee_fields* f) {
+  clear_error();
+  if (!f) return fail(COFFEE_E_INVALID, "coffee_fields_fill_guards: null argument");
+  COFFEE_CUDA_TRY(cudaSetDevice(f->env->device));
+  int rc = (f->elem == 4) ? fill_guards_t<float>(f, 0) : fill_guards_t<double>(f, 0);
+  if (rc) return rc;
+  COFFEE_CUDA_TRY(cudaDeviceSynchronize());
+  ++f->generation;
+  return COFFEE_OK;
+}
+
+// ------------------------------------------------------------------ solver
+
+template <typename T>
+static int configure_solver(coffee_solver* s) {
+  using S = Shape<T>;
+  auto k_first = ez_stage_kernel<T, S::STX, S::STY, S::SPF, true>;
+  auto k_rest = ez_stage_kernel<T, S::STX, S::STY, S::SPF, false>;
+  auto k_ko = ez_ko_kernel<T, S::KTX, S::KTY, S::KPF>;
+  COFFEE_CUDA_TRY(cudaFuncSetAttribute(k_first, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)stage_smem<T>(true)));
+  COFFEE_CUDA_TRY(cudaFuncSetAttribute(k_rest, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)stage_smem<T>(false)));
+  COFFEE_CUDA_TRY(cudaFuncSetAttribute(k_ko, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)ko_smem<T>()));
+  int per_sm_stage = 1, per_sm_ko = 1;
+  COFFEE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm_stage, k_rest, S::STX * S::STY, stage_smem<T>(false)));
+  COFFEE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm_ko, k_ko, S::KTX * S::KTY, ko_smem<T>()));
+  if (per_sm_stage < 1 || per_sm_ko < 1)
+    return fail(COFFEE_E_CUDA, "stage/KO kernels cannot be resident (occupancy 0)");
+  const int sms = num_sms(s->env->device);
+  const coffee_params& p = s->env->p;
+  int box[3];
+  for (int a = 0; a < 3; ++a) box[a] = p.N[a] + 2 * p.shift_ghost;
+  const int sx = (box[0] + S::STX - 1) / S::STX, sy = (box[1] + S::STY - 1) / S::STY;
+  s->kchunk_stage = pick_kchunk(box[2], sx * sy, sms * per_sm_stage, 4);
+  s->grid_stage = dim3(sx, sy, (box[2] + s->kchunk_stage - 1) / s->kchunk_stage);
+  const int kx = (box[0] + S::KTX - 1) / S::KTX, ky = (box[1] + S::KTY - 1) / S::KTY;
+  s->kchunk_ko = pick_kchunk(box[2], kx * ky, sms * per_sm_ko, 6);
+  s->grid_ko = dim3(kx, ky, (box[2] + s->kchunk_ko - 1) / s->kchunk_ko);
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int variant,
+                                    int semantics, void* stream, coffee_solver** out) {
+  clear_error();
+  if (!env || !f || !out) return fail(COFFEE_E_INVALID, "coffee_solver_create: null argument");
+  *out = nullptr;
+  if (f->env != env) return fail(COFFEE_E_INVALID, "fields belong to another environment");
+  if (variant != COFFEE_VARIANT_FLAT)
+    return fail(COFFEE_E_INVALID, "solver variant %d is not available", variant);
+  if (semantics != COFFEE_SEM_CPU_REF && semantics != COFFEE_SEM_GPU_REF)
+    return fail(COFFEE_E_INVALID, "unknown semantics %d", semantics);
+  if (env->p.problem < 0 || env->p.problem > 2)
+    return fail(COFFEE_E_CONFIG, "problem %d is not supported by the flat EZ solver",
+                env->p.problem);
+  COFFEE_CUDA_TRY(cudaSetDevice(env->device));
+  coffee_solver* s = new (std::nothrow) coffee_solver();
+  if (!s) return fail(COFFEE_E_NOMEM, "out of host memory");
+  s->env = env;
+  s->f = f;
+  s->variant = variant;
+  s->semantics = semantics;
+  s->stream = static_cast<cudaStream_t>(stream);
+  s->aux = 0;
+  s->timing = 0;
+  s->events_used = 0;
+  s->synced_generation = 0;
+  bool abs_any = env->p.shift_ghost > 0;
+  for (int a = 0; a < 3; ++a) abs_any = abs_any || env->p.pml[a] > 0;
+  s->absorbing = abs_any;
+  const size_t bytes = f->n * f->elem;
+  auto cleanup = [&]() {
+    for (int a = 0; a < 7; ++a) {
+      if (s->B[a]) cudaFree(s->B[a]);
+      if (s->dU[a]) cudaFree(s->dU[a]);
+      if (s->Un[a]) cudaFree(s->Un[a]);
+    }
+    delete s;
+  };
+  for (int a = 0; a < 7; ++a) {
+    cudaError_t err = cudaMalloc(&s->B[a], bytes);
+    if (err == cudaSuccess) err = cudaMalloc(&s->dU[a], bytes);
+    if (err == cudaSuccess) err = cudaMemset(s->dU[a], 0, bytes);
+    if (err == cudaSuccess && abs_any) err = cudaMalloc(&s->Un[a], bytes);
+    if (err == cudaSuccess && abs_any) err = cudaMemset(s->Un[a], 0, bytes);
+    if (err != cudaSuccess) {
+      cleanup();
+      return fail(COFFEE_E_NOMEM, "solver scratch allocation failed: %s", cudaGetErrorString(err));
+    }
+  }
+  int rc = (f->elem == 4) ? configure_solver<float>(s) : configure_solver<double>(s);
+  if (rc) {
+    cleanup();
+    return rc;
+  }
+  s->partial_blocks = num_sms(env->device) * 4;
+  cudaError_t err = cudaMalloc(&s->d_partials, sizeof(double) * s->partial_blocks);
+  if (err == cudaSuccess) err = cudaMalloc(&s->d_count, sizeof(int));
+  if (err == cudaSuccess) err = cudaEventCreate(&s->ev_begin);
+  if (err == cudaSuccess) err = cudaEventCreate(&s->ev_end);
+  if (err != cudaSuccess) {
+    cleanup();
+    return fail(COFFEE_E_NOMEM, "solver setup failed: %s", cudaGetErrorString(err));
+  }
+  *out = s;
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_solver_destroy(coffee_solver* s) {
+  if (!s) return COFFEE_OK;
+  cudaSetDevice(s->env->device);
+  cudaStreamSynchronize(s->stream);
+  for (int a = 0; a < 7; ++a) {
+    if (s->B[a]) cudaFree(s->B[a]);
+    if (s->dU[a]) cudaFree(s->dU[a]);
+    if (s->Un[a]) cudaFree(s->Un[a]);
+  }
+  for (auto e : s->events) cudaEventDestroy(e);
+  cudaEventDestroy(s->ev_begin);
+  cudaEventDestroy(s->ev_end);
+  cudaFree(s->d_partials);
+  cudaFree(s->d_count);
+  delete s;
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_solver_set_aux(coffee_solver* s, int enable) {
+  clear_error();
+  if (!s) return fail(COFFEE_E_INVALID, "coffee_solver_set_aux: null argument");
+  if (enable)
+    for (int id = COFFEE_JX; id <= COFFEE_DIVB; ++id) {
+      int rc = ensure_field(s->f, id);
+      if (rc) return rc;
+    }
+  s->aux = enable ? 1 : 0;
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_solver_set_timing(coffee_solver* s, int enable) {
+  if (!s) return fail(COFFEE_E_INVALID, "coffee_solver_set_timing: null argument");
+  s->timing = enable ? 1 : 0;
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_solver_launches_per_step(coffee_solver* s) {
+  (void)s;
+  return 6;  // 5 stage kernels + 1 KO kernel
+}
+
+static int next_event_pair(coffee_solver* s, int kind, cudaEvent_t* a, cudaEvent_t* b) {
+  const size_t need = (size_t)(s->events_used + 1) * 2;
+  while (s->events.size() < need) {
+    cudaEvent_t e;
+    COFFEE_CUDA_TRY(cudaEventCreate(&e));
+    s->events.push_back(e);
+  }
+  if (s->event_kind.size() < (size_t)(s->events_used + 1)) s->event_kind.resize(s->events_used + 1);
+  s->event_kind[s->events_used] = kind;
+  *a = s->events[2 * s->events_used];
+  *b = s->events[2 * s->events_used + 1];
+  ++s->events_used;
+  return COFFEE_OK;
+}
+
+template <typename T>
+static int run_steps(coffee_solver* s, double time, int nsteps) {
+  using S = Shape<T>;
+  EzConst<T> c;
+  build_const<T>(s->env, s->semantics, &c);
+  coffee_fields* f = s->f;
+  cudaStream_t st = s->stream;
+  const size_t bytes = f->n * f->elem;
+  if (s->synced_generation != f->generation) {
+    // the second buffer must carry the same guard values (non-periodic
+    // guards are never written by the kernels)
+    for (int a = 0; a < 7; ++a)
+      COFFEE_CUDA_TRY(cudaMemcpyAsync(s->B[a], f->d[a], bytes, cudaMemcpyDeviceToDevice, st));
+    s->synced_generation = f->generation;
+  }
+  F7<T> A = f7<T>(f->d), Bb = f7<T>(s->B), dU = f7<T>(s->dU), Un = f7<T>(s->Un);
+  F5<T> aux;
+  for (int a = 0; a < 5; ++a) aux.p[a] = static_cast<T*>(f->d[COFFEE_JX + a]);
+  const T dt = c.dt;
+  T t = (T)time;
+  const dim3 bs(S::STX, S::STY), bk(S::KTX, S::KTY);
+  s->events_used = 0;
+  if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(s->ev_begin, st));
+  for (int step = 0; step < nsteps; ++step) {
+    for (int i = 0; i < 5; ++i) {
+      const F7<T>& src = (i % 2 == 0) ? A : Bb;
+      const F7<T>& dst = (i % 2 == 0) ? Bb : A;
+      F7<const T> srcc;
+      for (int a = 0; a < 7; ++a) srcc.p[a] = src.p[a];
+      int flags = 0;
+      if (i == 4) flags |= ST_LAST;
+      if (i == 4 && s->aux) flags |= ST_AUX;
+      if (i == 0 && s->absorbing) flags |= ST_WRITE_UN;
+      const T tst = t + (T)kCs[i] * dt;
+      cudaEvent_t e0 = nullptr, e1 = nullptr;
+      if (s->timing) {
+        int rc = next_event_pair(s, i == 0 ? COFFEE_KERNEL_STAGE_FIRST : COFFEE_KERNEL_STAGE,
+                                 &e0, &e1);
+        if (rc) return rc;
+        COFFEE_CUDA_TRY(cudaEventRecord(e0, st));
+      }
+      if (i == 0)
+        ez_stage_kernel<T, S::STX, S::STY, S::SPF, true>
+            <<<s->grid_stage, bs, stage_smem<T>(true), st>>>(c, srcc, dst, dU, Un, aux,
+                                                             (T)kAs[i], (T)kBs[i], tst,
+                                                             s->kchunk_stage, flags);
+      else
+        ez_stage_kernel<T, S::STX, S::STY, S::SPF, false>
+            <<<s->grid_stage, bs, stage_smem<T>(false), st>>>(c, srcc, dst, dU, Un, aux,
+                                                              (T)kAs[i], (T)kBs[i], tst,
+                                                              s->kchunk_stage, flags);
+      COFFEE_CUDA_TRY(cudaGetLastError());
+      if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(e1, st));
+    }
+    F7<const T> srcc;
+    for (int a = 0; a < 7; ++a) srcc.p[a] = Bb.p[a];
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (s->timing) {
+      int rc = next_event_pair(s, COFFEE_KERNEL_KO, &e0, &e1);
+      if (rc) return rc;
+      COFFEE_CUDA_TRY(cudaEventRecord(e0, st));
+    }
+    ez_ko_kernel<T, S::KTX, S::KTY, S::KPF>
+        <<<s->grid_ko, bk, ko_smem<T>(), st>>>(c, srcc, A, t + dt, s->kchunk_ko);
+    COFFEE_CUDA_TRY(cudaGetLastError());
+    if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(e1, st));
+    t = t + dt;
+  }
+  if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(s->ev_end, st));
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_solver_step(coffee_solver* s, double time, int nsteps) {
+  clear_error();
+  if (!s) return fail(COFFEE_E_INVALID, "coffee_solver_step: null argument");
+  if (nsteps < 0) return fail(COFFEE_E_INVALID, "nsteps must be >= 0");
+  COFFEE_CUDA_TRY(cudaSetDevice(s->env->device));
+  return (s->f->elem == 4) ? run_steps<float>(s, time, nsteps) : run_steps<double>(s, time, nsteps);
+}
+
+extern "C" int coffee_solver_last_timing(coffee_solver* s, double ms[3], int launches[3],
+                                         double* total_ms) {
+  clear_error();
+  if (!s) return fail(COFFEE_E_INVALID, "coffee_solver_last_timing: null argument");
+  if (!s->timing) return fail(COFFEE_E_INVALID, "timing is off (coffee_solver_set_timing)");
+  COFFEE_CUDA_TRY(cudaEventSynchronize(s->ev_end));
+  double sum[3] = {0, 0, 0};
+  int cnt[3] = {0, 0, 0};
+  for (int q = 0; q < s->events_used; ++q) {
+    float t = 0;
+    COFFEE_CUDA_TRY(cudaEventElapsedTime(&t, s->events[2 * q], s->events[2 * q + 1]));
+    sum[s->event_kind[q]] += t;
+    cnt[s->event_kind[q]] += 1;
+  }
+  float tot = 0;
+  COFFEE_CUDA_TRY(cudaEventElapsedTime(&tot, s->ev_begin, s->ev_end));
+  for (int k = 0; k < 3; ++k) {
+    if (ms) ms[k] = sum[k];
+    if (launches) launches[k] = cnt[k];
+  }
+  if (total_ms) *total_ms = tot;
+  return COFFEE_OK;
+}
+
+template <typename T>
+static int diag_t(coffee_solver* s, int what, double* out) {
+  EzConst<T> c;
+  build_const<T>(s->env, s->semantics, &c);
+  const coffee_params& p = s->env->p;
+  T xl[3], xh[3];
+  for (int a = 0; a < 3; ++a) {
+    // region of total_energy (field_solver_EZ.cu:759-770)
+    xh[a] = (T)p.lower[a] + (T)p.size[a] - (T)p.pml[a] * c.delta[a];
+    xl[a] = (T)p.lower[a] + (T)p.pml[a] * c.delta[a];
+  }
+  diag_kernel<T><<<s->partial_blocks, 256, 0, s->stream>>>(c, f7c<T>(s->f->d), what, xl[0],
+                                                           xl[1], xl[2], xh[0], xh[1], xh[2],
+                                                           s->d_partials);
+  COFFEE_CUDA_TRY(cudaGetLastError());
+  std::vector<double> h(s->partial_blocks);
+  COFFEE_CUDA_TRY(cudaMemcpyAsync(h.data(), s->d_partials, sizeof(double) * h.size(),
+                                  cudaMemcpyDeviceToHost, s->stream));
+  COFFEE_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  const bool is_max = (what == COFFEE_DIAG_MAX_EDOTB || what == COFFEE_DIAG_MAX_EOVERB);
+  double acc = 0;
+  for (double v : h) acc = is_max ? std::max(acc, v) : acc + v;
+  if (what == COFFEE_DIAG_DIVB_L2) acc = std::sqrt(acc);
+  *out = acc;
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_diag_reduce(coffee_solver* s, int what, double* out) {
+  clear_error();
+  if (!s || !out) return fail(COFFEE_E_INVALID, "coffee_diag_reduce: null argument");
+  if (what < COFFEE_DIAG_ENERGY_E || what > COFFEE_DIAG_MAX_EOVERB)
+    return fail(COFFEE_E_INVALID, "unknown diagnostic %d", what);
+  COFFEE_CUDA_TRY(cudaSetDevice(s->env->device));
+  return (s->f->elem == 4) ? diag_t<float>(s, what, out) : diag_t<double>(s, what, out);
+}
+
+extern "C" int coffee_solver_check_finite(coffee_solver* s) {
+  clear_error();
+  if (!s) return fail(COFFEE_E_INVALID, "coffee_solver_check_finite: null argument");
+  COFFEE_CUDA_TRY(cudaSetDevice(s->env->device));
+  COFFEE_CUDA_TRY(cudaMemsetAsync(s->d_count, 0, sizeof(int), s->stream));
+  const long long n = (long long)s->f->n;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)s->partial_blocks * 8);
+  if (s->f->elem == 4)
+    count_nonfinite_kernel<float><<<blocks, 256, 0, s->stream>>>(f7c<float>(s->f->d), n, s->d_count);
+  else
+    count_nonfinite_kernel<double><<<blocks, 256, 0, s->stream>>>(f7c<double>(s->f->d), n, s->d_count);
+  COFFEE_CUDA_TRY(cudaGetLastError());
+  int h = 0;
+  COFFEE_CUDA_TRY(cudaMemcpyAsync(&h, s->d_count, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  COFFEE_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  if (h != 0) return fail(COFFEE_E_NONFINITE, "%d field values are NaN or Inf", h);
+  return COFFEE_OK;
+}
+
+// ------------------------------------------------------------- snapshots
+
+extern "C" int coffee_solver_save_snapshot(coffee_solver* s, const char* path, double time,
+                                           int64_t step) {
+  clear_error();
+  if (!s || !path) return fail(COFFEE_E_INVALID, "coffee_solver_save_snapshot: null argument");
+  COFFEE_CUDA_TRY(cudaSetDevice(s->env->device));
+  COFFEE_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  coffee_fields* f = s->f;
+  const size_t bytes = f->n * f->elem;
+  std::vector<char> host;
+  try {
+    host.resize(bytes * 7);
+  } catch (...) {
+    return fail(COFFEE_E_NOMEM, "snapshot: cannot allocate %zu host bytes", bytes * 7);
+  }
+  for (int a = 0; a < 7; ++a)
+    COFFEE_CUDA_TRY(cudaMemcpy(host.data() + a * bytes, f->d[a], bytes, cudaMemcpyDeviceToHost));
+  fld_header h;
+  fld_header_init(&h, f->elem, 7, s->env->grid.dims, s->env->grid.guard);
+  h.time = time;
+  h.step = step;
+  const void* arrays[7];
+  for (int a = 0; a < 7; ++a) arrays[a] = host.data() + a * bytes;
+  if (!fld_write(path, &h, arrays, f->n)) return fail(COFFEE_E_IO, "cannot write %s", path);
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_solver_load_snapshot(coffee_solver* s, const char* path, double* time,
+                                           int64_t* step) {
+  clear_error();
+  if (!s || !path) return fail(COFFEE_E_INVALID, "coffee_solver_load_snapshot: null argument");
+  fld_header h;
+  std::vector<char> payload;
+  if (!fld_read(path, &h, &payload)) return fail(COFFEE_E_IO, "cannot read %s", path);
+  coffee_fields* f = s->f;
+  for (int a = 0; a < 3; ++a)
+    if (h.dims[a] != s->env->grid.dims[a])
+      return fail(COFFEE_E_IO, "%s: dims do not match the grid", path);
+  if (h.elem_size != f->elem || h.nfields < 7)
+    return fail(COFFEE_E_IO, "%s: precision or field count does not match", path);
+  const size_t bytes = f->n * f->elem;
+  if (h.crc32 != 0) {
+    uint32_t crc = fld_crc32_update(0, payload.data(), bytes * (size_t)h.nfields);
+    if (crc != h.crc32) return fail(COFFEE_E_IO, "%s: CRC mismatch", path);
+  }
+  COFFEE_CUDA_TRY(cudaSetDevice(s->env->device));
+  COFFEE_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  for (int a = 0; a < 7; ++a)
+    COFFEE_CUDA_TRY(cudaMemcpy(f->d[a], payload.data() + a * bytes, bytes, cudaMemcpyHostToDevice));
+  ++f->generation;
+  if (time) *time = h.time;
+  if (step) *step = h.step;
+  return COFFEE_OK;
+}

@@ -1,0 +1,211 @@
+"""Initial conditions for the benchmark and test problems (host side, numpy).
+
+These play the role of the reference's ``user_*.hpp`` snippets (e.g.
+``src/user_alfven.hpp``, ``src/user_pulsar3d_EZ.hpp``): they fill E, B, P
+on every grid point, guard cells included, at the collocated EZ vertex
+positions ``lower + delta*(n - guard)`` (``Grid::pos`` with stagger bit 1,
+``src/data/grid.h:116-134``).  Values are computed in float64 and returned
+in the requested dtype, as 7 arrays of shape ``(d2, d1, d0)``.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .config import Grid, SimParams
+
+# ---------------------------------------------------------------- Alfven wave
+
+
+def alfven_params(N: int = 128, guard: int = 3) -> SimParams:
+    """Periodic unit box, dx = 1/N, dt = 0.5*dx, no absorbing layer,
+    no star (problem 0), E.B damping on (the reference default)."""
+    p = SimParams()
+    p.N = [N, N, N]
+    p.guard = [guard] * 3
+    p.lower = [0.0, 0.0, 0.0]
+    p.size = [1.0, 1.0, 1.0]
+    p.periodic_boundary = [True, True, True]
+    p.pml = [0, 0, 0]
+    p.problem = 0
+    p.dt = 0.5 / N
+    p.use_edotb_damping = True
+    return p
+
+
+def alfven_fields(p: SimParams, dtype=np.float32, amp=0.1, width2=0.02, vz=0.1):
+    """B = (1, amp*sin(2 pi x)*exp(-((y-1/2)^2+(z-1/2)^2)/width2), 0),
+    E = -v x B with v = vz zhat, so E = (vz*By, -vz*Bx, 0) and E.B = 0; P = 0."""
+    g = Grid.from_params(p, dtype)
+    ft = np.dtype(dtype)
+    x = g.coords(0, np.float64)
+    y = g.coords(1, np.float64)
+    z = g.coords(2, np.float64)
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    Bx = np.ones_like(X)
+    By = amp * np.sin(2 * np.pi * X) * np.exp(-((Y - 0.5) ** 2 + (Z - 0.5) ** 2) / width2)
+    Bz = np.zeros_like(X)
+    Ex = vz * By
+    Ey = -vz * Bx
+    Ez = np.zeros_like(X)
+    P = np.zeros_like(X)
+    return [a.astype(ft) for a in (Ex, Ey, Ez, Bx, By, Bz, P)]
+
+
+# ------------------------------------------------------------- turbulence
+
+TURB_SEED = 20261203
+
+
+def turbulence_params(N: int = 512, guard: int = 3, cfl: float = 0.5) -> SimParams:
+    p = alfven_params(N, guard)
+    p.dt = cfl / N
+    return p
+
+
+def turbulence_modes(seed: int = TURB_SEED, nmodes: int = 32, nmin: float = 2.0,
+                     nmax: float = 8.0, db_rms: float = 0.3, nv: int = 8,
+                     vmax_bound: float = 0.45):
+    """Mode tables for the random force-free turbulence problem.
+
+    A = sum_m a_m e_m cos(k_m.x + phi_m) with integer wave vectors n_m,
+    |n_m| in [nmin, nmax], k = 2 pi n, e_m a random unit vector normal to k_m,
+    so dB_m = curl A_m = -a_m (k_m x e_m) sin(k_m.x + phi_m).  Amplitudes
+    follow |dB_m|^2 ~ |k_m|^-2 and are scaled so rms(dB) = db_rms (the modes
+    are distinct and not opposite, so rms^2 = sum |dB_m|^2 / 2).
+
+    v = sum_n c_n u_n sin(q_n.x + psi_n) with 1 <= |n| <= 2, unit u_n, and
+    sum |c_n| = vmax_bound, which bounds |v| <= vmax_bound < 0.5.
+
+    Returns float64 arrays: (kb[m,3], bamp[m,3], phib[m]), (kv, vamp, phiv),
+    with bamp the vector amplitude of sin(k.x + phi) in dB.
+    """
+    rng = np.random.default_rng(seed)
+    seen = set()
+    ks, dirs = [], []
+    while len(ks) < nmodes:
+        n = rng.integers(-int(nmax), int(nmax) + 1, size=3)
+        nn = float(np.linalg.norm(n))
+        key = tuple(int(v) for v in n)
+        neg = tuple(-v for v in key)
+        if nn < nmin or nn > nmax or key in seen or neg in seen:
+            continue
+        seen.add(key)
+        ks.append(n.astype(np.float64))
+    kb = 2 * np.pi * np.array(ks)
+    bamp = np.zeros((nmodes, 3))
+    for m in range(nmodes):
+        k = kb[m]
+        e = rng.normal(size=3)
+        e -= k * (e @ k) / (k @ k)
+        e /= np.linalg.norm(e)
+        kmag = np.linalg.norm(k)
+        # a_m ~ |k|^-2  =>  |dB_m| = a_m |k| ~ |k|^-1
+        a = kmag ** -2
+        bamp[m] = -a * np.cross(k, e)
+    phib = rng.uniform(0, 2 * np.pi, size=nmodes)
+    rms = math.sqrt(0.5 * float(np.sum(bamp ** 2)))
+    bamp *= db_rms / rms
+
+    kvs = []
+    seen = set()
+    while len(kvs) < nv:
+        n = rng.integers(-2, 3, size=3)
+        nn = float(np.linalg.norm(n))
+        key = tuple(int(v) for v in n)
+        if nn < 1 or nn > 2 or key in seen:
+            continue
+        seen.add(key)
+        kvs.append(n.astype(np.float64))
+    kv = 2 * np.pi * np.array(kvs)
+    u = rng.normal(size=(nv, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    c = rng.uniform(0.5, 1.0, size=nv)
+    c *= vmax_bound / c.sum()
+    vamp = u * c[:, None]
+    phiv = rng.uniform(0, 2 * np.pi, size=nv)
+    return (kb, bamp, phib), (kv, vamp, phiv)
+
+
+def turbulence_fields(p: SimParams, dtype=np.float32, seed: int = TURB_SEED, b0=1.0):
+    """B = b0 xhat + sum dB_m, E = -v x B, P = 0, evaluated per z-plane."""
+    g = Grid.from_params(p, dtype)
+    (kb, bamp, phib), (kv, vamp, phiv) = turbulence_modes(seed)
+    x = g.coords(0, np.float64)
+    y = g.coords(1, np.float64)
+    z = g.coords(2, np.float64)
+    d0, d1, d2 = g.dims
+    out = [np.empty((d2, d1, d0), dtype=dtype) for _ in range(7)]
+    Y, X = np.meshgrid(y, x, indexing="ij")
+    for kk in range(d2):
+        B = np.zeros((3, d1, d0))
+        B[0] += b0
+        for m in range(len(phib)):
+            ph = np.sin(kb[m, 0] * X + kb[m, 1] * Y + kb[m, 2] * z[kk] + phib[m])
+            B += bamp[m][:, None, None] * ph
+        v = np.zeros((3, d1, d0))
+        for m in range(len(phiv)):
+            ph = np.sin(kv[m, 0] * X + kv[m, 1] * Y + kv[m, 2] * z[kk] + phiv[m])
+            v += vamp[m][:, None, None] * ph
+        E = -np.cross(v, B, axis=0)
+        for c in range(3):
+            out[c][kk] = E[c]
+            out[3 + c][kk] = B[c]
+        out[6][kk] = 0
+    return out
+
+
+# ---------------------------------------------------------------- pulsar
+
+
+def pulsar_params(N: int = 64, guard: int = 3, half_size: float = 16.0, radius: float = 3.0,
+                  omega: float = 0.05, b0: float = 1.0, pml: int = 8,
+                  offset: float = 0.5) -> SimParams:
+    """Star at the origin of a non-periodic box with an absorbing layer
+    (problem 1, as ``src/main-pulsar3d.cpp`` + ``user_pulsar3d_EZ.hpp``).
+
+    The box is shifted by ``offset`` cells so that no grid point sits at
+    r = 0, where the dipole is singular (the reference evaluates it there as
+    b0 / TINY, a value that differs between its float and FP64 builds)."""
+    p = SimParams()
+    p.N = [N, N, N]
+    p.guard = [guard] * 3
+    d = 2 * half_size / N
+    p.lower = [-half_size - offset * d] * 3
+    p.size = [2 * half_size] * 3
+    p.periodic_boundary = [False, False, False]
+    p.pml = [pml] * 3
+    p.pmllen = max(1, pml // 2)
+    p.sigpml = 0.1
+    p.problem = 1
+    p.radius = radius
+    p.omega = omega
+    p.b0 = b0
+    p.dt = 0.4 * (2 * half_size / N)
+    return p
+
+
+def _dipole2(x, y, z, p1, p2, p3, phase, tiny):
+    """b0-less dipole2 of pulsar_impl.hpp:57-78, float64."""
+    c, s = math.cos(phase), math.sin(phase)
+    p1t, p2t, p3t = p1 * c - p2 * s, p1 * s + p2 * c, p3
+    r2 = x * x + y * y + z * z
+    pr = p1t * x + p2t * y + p3t * z
+    den = np.sqrt(r2 ** 3) + tiny
+    return [(3.0 * q * pr / (r2 + tiny) - pq) / den for q, pq in ((x, p1t), (y, p2t), (z, p3t))]
+
+
+def pulsar_fields(p: SimParams, dtype=np.float32):
+    """B = b0 * dipole(p1, p2, p3), E = 0, P = 0 at every point
+    (``src/user_pulsar3d_EZ.hpp``; the quadrupole terms are zero unless set)."""
+    g = Grid.from_params(p, dtype)
+    tiny = 1e-7 if np.dtype(dtype) == np.float32 else 1e-11
+    x = g.coords(0, np.float64)
+    y = g.coords(1, np.float64)
+    z = g.coords(2, np.float64)
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    b = _dipole2(X, Y, Z, p.p1, p.p2, p.p3, 0.0, tiny)
+    zeros = np.zeros_like(X)
+    arrs = [zeros, zeros, zeros, p.b0 * b[0], p.b0 * b[1], p.b0 * b[2], zeros]
+    return [np.asarray(a, dtype=dtype).copy() for a in arrs]

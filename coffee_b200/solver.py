@@ -1,0 +1,264 @@
+"""Python mirror of the reference's objects on the field-update path.
+
+``SimEnvironment``, ``SimData`` and ``FieldSolverEZ`` carry the names and
+meaning of ``Coffee::sim_environment`` (reference src/sim_env.h:17-87),
+``Coffee::sim_data`` (src/data/sim_data.h:11-24) and
+``Coffee::field_solver_EZ`` (src/algorithms/field_solver_EZ.h:6-33).  Each is
+a thin owner of a C-ABI handle of libcoffee_b200.so; all computation runs in
+the library's CUDA kernels.  Host arrays are numpy arrays of shape
+``(dims[2], dims[1], dims[0])`` in the reference layout (x fastest).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .config import SimParams
+from ._lib import CoffeeGrid, CoffeeParams, check
+
+FIELD_NAMES = ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "P")
+
+
+def to_coffee_params(p: SimParams) -> CoffeeParams:
+    """SimParams -> coffee_params, field by field."""
+    lib = _lib.load()
+    cp = CoffeeParams()
+    lib.coffee_params_default(ctypes.byref(cp))
+    for name, ctype in CoffeeParams._fields_:
+        if not hasattr(p, name):
+            continue
+        v = getattr(p, name)
+        if isinstance(v, list):
+            arr = getattr(cp, name)
+            for i in range(3):
+                arr[i] = int(v[i]) if isinstance(arr[i], int) else float(v[i])
+        elif isinstance(v, bool):
+            setattr(cp, name, int(v))
+        else:
+            setattr(cp, name, v)
+    return cp
+
+
+class SimEnvironment:
+    """One rank of ``sim_environment`` on one GPU."""
+
+    def __init__(self, params: SimParams, device: int = 0):
+        self.lib = _lib.load()
+        self.sim_params = params
+        self._cp = to_coffee_params(params)
+        h = ctypes.c_void_p()
+        check(self.lib.coffee_env_create(ctypes.byref(self._cp), device, ctypes.byref(h)))
+        self.handle = h
+        g = CoffeeGrid()
+        check(self.lib.coffee_env_grid(self.handle, ctypes.byref(g)))
+        self._grid = g
+
+    @classmethod
+    def from_toml(cls, text: str, device: int = 0) -> "SimEnvironment":
+        """Build from config.toml text parsed by the library (parse_config)."""
+        lib = _lib.load()
+        cp = CoffeeParams()
+        check(lib.coffee_params_parse_toml(text.encode(), ctypes.byref(cp)))
+        env = cls.__new__(cls)
+        env.lib = lib
+        env.sim_params = SimParams.from_toml(text, is_text=True)
+        env._cp = cp
+        h = ctypes.c_void_p()
+        check(lib.coffee_env_create(ctypes.byref(cp), device, ctypes.byref(h)))
+        env.handle = h
+        g = CoffeeGrid()
+        check(lib.coffee_env_grid(h, ctypes.byref(g)))
+        env._grid = g
+        return env
+
+    def grid(self) -> CoffeeGrid:
+        return self._grid
+
+    def params(self) -> CoffeeParams:
+        return self._cp
+
+    @property
+    def dims(self):
+        return tuple(self._grid.dims)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.coffee_env_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SimData:
+    """Device-resident E, B, P (+ J, divE, divB on request)."""
+
+    def __init__(self, env: SimEnvironment, dtype=np.float32):
+        self.env = env
+        self.lib = env.lib
+        self.dtype = np.dtype(dtype)
+        h = ctypes.c_void_p()
+        check(self.lib.coffee_fields_create(env.handle, self.dtype.itemsize, ctypes.byref(h)))
+        self.handle = h
+        d0, d1, d2 = env.dims
+        self.shape = (d2, d1, d0)
+
+    def upload(self, arrays):
+        """sync_to_device of E, B, P from 7 host arrays."""
+        if len(arrays) != 7:
+            raise ValueError("need 7 arrays (Ex Ey Ez Bx By Bz P)")
+        for fid, a in enumerate(arrays):
+            self.upload_field(fid, a)
+
+    def upload_field(self, fid, a):
+        a = np.ascontiguousarray(a, dtype=self.dtype)
+        if a.shape != self.shape:
+            raise ValueError(f"array shape {a.shape} != grid {self.shape}")
+        check(self.lib.coffee_fields_upload(self.handle, int(fid), a.ctypes.data_as(ctypes.c_void_p)))
+
+    def upload_packed(self, buf: np.ndarray):
+        """Upload 7 arrays stored back to back in one (pinned or pageable) buffer."""
+        check(self.lib.coffee_fields_upload(self.handle, -1, buf.ctypes.data_as(ctypes.c_void_p)))
+
+    def download_packed(self, buf: np.ndarray):
+        check(self.lib.coffee_fields_download(self.handle, -1, buf.ctypes.data_as(ctypes.c_void_p)))
+
+    def download(self, names=FIELD_NAMES):
+        """sync_to_host; returns a list of arrays."""
+        out = []
+        for n in names:
+            fid = _lib.FIELD_IDS[n] if isinstance(n, str) else int(n)
+            a = np.empty(self.shape, dtype=self.dtype)
+            check(self.lib.coffee_fields_download(self.handle, fid, a.ctypes.data_as(ctypes.c_void_p)))
+            out.append(a)
+        return out
+
+    def init_fourier(self, b0, bmodes, vmodes):
+        """Device-side problem set-up: B = b0 + sum bamp sin(kb.x + phib),
+        E = -v x B with v = sum vamp sin(kv.x + phiv), P = 0."""
+        (kb, bamp, phib), (kv, vamp, phiv) = bmodes, vmodes
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (kb, bamp, phib, kv, vamp, phiv)]
+        P = ctypes.POINTER(ctypes.c_double)
+        b0a = (ctypes.c_double * 3)(*[float(x) for x in b0])
+        check(self.lib.coffee_fields_init_fourier(
+            self.handle, b0a, len(arrs[2]), arrs[0].ctypes.data_as(P), arrs[1].ctypes.data_as(P),
+            arrs[2].ctypes.data_as(P), len(arrs[5]), arrs[3].ctypes.data_as(P),
+            arrs[4].ctypes.data_as(P), arrs[5].ctypes.data_as(P)))
+
+    def dev_ptr(self, name) -> int:
+        fid = _lib.FIELD_IDS[name] if isinstance(name, str) else int(name)
+        p = ctypes.c_void_p()
+        check(self.lib.coffee_fields_ptr(self.handle, fid, ctypes.byref(p)))
+        return p.value
+
+    def fill_guards(self):
+        check(self.lib.coffee_fields_fill_guards(self.handle))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.coffee_fields_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FieldSolverEZ:
+    """``field_solver_EZ(sim_data&, sim_environment&)`` on the GPU."""
+
+    def __init__(self, data: SimData, env: SimEnvironment, semantics: str = "cpu",
+                 stream: int | None = None):
+        self.data = data
+        self.env = env
+        self.lib = env.lib
+        sem = {"cpu": _lib.SEM_CPU_REF, "gpu": _lib.SEM_GPU_REF}[semantics]
+        h = ctypes.c_void_p()
+        check(self.lib.coffee_solver_create(env.handle, data.handle, _lib.VARIANT_FLAT, sem,
+                                            ctypes.c_void_p(stream or 0), ctypes.byref(h)))
+        self.handle = h
+
+    def evolve_fields(self, time: float):
+        """One full step (5 LSRK stages + KO), as the reference's evolve_fields."""
+        check(self.lib.coffee_solver_step(self.handle, float(time), 1))
+
+    def step(self, time: float, nsteps: int):
+        check(self.lib.coffee_solver_step(self.handle, float(time), int(nsteps)))
+
+    def set_aux(self, enable: bool):
+        check(self.lib.coffee_solver_set_aux(self.handle, int(bool(enable))))
+
+    def set_timing(self, enable: bool):
+        check(self.lib.coffee_solver_set_timing(self.handle, int(bool(enable))))
+
+    def last_timing(self):
+        """Per-kind device milliseconds and launch counts of the last step call."""
+        ms = (ctypes.c_double * 3)()
+        n = (ctypes.c_int * 3)()
+        tot = ctypes.c_double()
+        check(self.lib.coffee_solver_last_timing(self.handle, ms, n, ctypes.byref(tot)))
+        kinds = ("stage_first", "stage", "ko")
+        return {"ms": dict(zip(kinds, list(ms))), "launches": dict(zip(kinds, list(n))),
+                "total_ms": tot.value}
+
+    def launches_per_step(self) -> int:
+        return int(self.lib.coffee_solver_launches_per_step(self.handle))
+
+    def diag(self, what: str) -> float:
+        out = ctypes.c_double()
+        check(self.lib.coffee_diag_reduce(self.handle, _lib.DIAG[what], ctypes.byref(out)))
+        return out.value
+
+    def total_energy(self, which: str = "B") -> float:
+        """field_solver_EZ::total_energy of E or B, accumulated in FP64."""
+        return self.diag("energy_" + which)
+
+    def check_finite(self):
+        check(self.lib.coffee_solver_check_finite(self.handle))
+
+    def save_snapshot(self, path: str, time: float, step: int):
+        check(self.lib.coffee_solver_save_snapshot(self.handle, path.encode(), float(time), int(step)))
+
+    def load_snapshot(self, path: str):
+        t = ctypes.c_double()
+        s = ctypes.c_int64()
+        check(self.lib.coffee_solver_load_snapshot(self.handle, path.encode(), ctypes.byref(t),
+                                                   ctypes.byref(s)))
+        return t.value, s.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.coffee_solver_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run_flat(params: SimParams, fields, nsteps: int, time0: float = 0.0, semantics: str = "cpu",
+             aux: bool = False, device: int = 0):
+    """Upload ``fields``, advance ``nsteps`` on the GPU, return the 7 fields
+    (and J, divE, divB when ``aux``)."""
+    env = SimEnvironment(params, device)
+    data = SimData(env, fields[0].dtype)
+    data.upload(fields)
+    solver = FieldSolverEZ(data, env, semantics)
+    if aux:
+        solver.set_aux(True)
+    solver.step(time0, nsteps)
+    out = data.download()
+    auxa = data.download(("Jx", "Jy", "Jz", "divE", "divB")) if aux else None
+    solver.close()
+    data.close()
+    env.close()
+    return out, auxa

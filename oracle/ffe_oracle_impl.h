@@ -1,0 +1,559 @@
+/* Body of the oracle restatement, instantiated for REAL = float and double
+ * by ffe_oracle.c (test infrastructure only; see ffe_oracle.h).
+ *
+ * Expressions keep the reference's operand order and its mixed float/double
+ * promotions (double literals such as 3.0 promote float operands to double
+ * in the pulsar helpers, src/algorithms/pulsar_impl.hpp:10-139).  The
+ * restatement runs plain scalar loops where the reference CPU build runs
+ * AVX-512 vectors; the results agree to rounding. */
+
+#define CAT2(a, b) a##b
+#define CAT(a, b) CAT2(a, b)
+#define FN(name) CAT(name, SFX)
+
+typedef struct {
+  int d0, d1, d2;
+  int g[3];
+  REAL delta[3], inv_delta[3], lower[3];
+  size_t n;
+} FN(grid_t);
+
+static inline REAL FN(pos)(const FN(grid_t) * g, int axis, int n) {
+  /* Grid::pos(axis, n, 1) = lower + delta*(n - guard + 0)  (grid.h:116-134) */
+  return g->lower[axis] + g->delta[axis] * ((REAL)(n - g->g[axis]) + (REAL)0.0);
+}
+
+/* diff1_4 (finite_diff_simd.h:15-25): (f-2 - 8 f-1 + 8 f+1 - f+2) / 12 */
+static inline REAL FN(df1)(const REAL* f, size_t ijk, size_t s, REAL inv) {
+  REAL v = (f[ijk - 2 * s] - f[ijk - s] * (REAL)8.0 + f[ijk + s] * (REAL)8.0 -
+            f[ijk + 2 * s]) / (REAL)12.0;
+  return v * inv;
+}
+
+/* diff6_2 (finite_diff_simd.h:41-58) */
+static inline REAL FN(d6)(const REAL* f, size_t ijk, size_t s) {
+  return (f[ijk - 3 * s] - (REAL)6.0 * f[ijk - 2 * s] + (REAL)15.0 * f[ijk - s] -
+          (REAL)20.0 * f[ijk] + (REAL)15.0 * f[ijk + s] - (REAL)6.0 * f[ijk + 2 * s] +
+          f[ijk + 3 * s]);
+}
+
+/* shape() (pulsar_impl.hpp:52-55): evaluated in double, returned as Scalar */
+static inline REAL FN(shape)(REAL r, REAL r0, REAL del) {
+  return (REAL)(0.5 * (1.0 - tanh((double)((r - r0) / del))));
+}
+
+static inline REAL FN(cube)(REAL x) { return x * x * x; }
+
+/* dipole2 (pulsar_impl.hpp:57-78) */
+static REAL FN(dipole2)(REAL x, REAL y, REAL z, REAL p1, REAL p2, REAL p3,
+                        REAL phase, int n) {
+  REAL cosph = (REAL)cos((double)phase);
+  REAL sinph = (REAL)sin((double)phase);
+  REAL p1t = p1 * cosph - p2 * sinph;
+  REAL p2t = p1 * sinph + p2 * cosph;
+  REAL p3t = p3;
+  REAL r2 = x * x + y * y + z * z;
+  REAL pr = p1t * x + p2t * y + p3t * z;
+  REAL den = (REAL)sqrt((double)FN(cube)(r2)) + TINYR;
+  REAL c = (n == 0) ? x : (n == 1) ? y : z;
+  REAL pc = (n == 0) ? p1t : (n == 1) ? p2t : p3t;
+  if (n < 0 || n > 2) return 0;
+  return (REAL)((3.0 * (double)c * (double)pr / (double)(r2 + TINYR) - (double)pc) /
+                (double)den);
+}
+
+/* quadrupole (pulsar_impl.hpp:80-118) */
+static REAL FN(quadrupole)(REAL x, REAL y, REAL z, REAL q11, REAL q12, REAL q13,
+                           REAL q22, REAL q23, REAL qox, REAL qoy, REAL qoz,
+                           REAL phase, int n) {
+  REAL cosph = (REAL)cos((double)phase);
+  REAL sinph = (REAL)sin((double)phase);
+  REAL q11t = (REAL)((double)q11 * (double)(cosph * cosph) -
+                     2.0 * (double)q12 * (double)cosph * (double)sinph +
+                     (double)q22 * (double)(sinph * sinph));
+  REAL q12t = (REAL)((double)q12 * cos(2.0 * (double)phase) +
+                     (double)((q11 - q22) * cosph * sinph));
+  REAL q22t = (REAL)((double)q22 * (double)(cosph * cosph) +
+                     (double)q11 * (double)(sinph * sinph) +
+                     2.0 * (double)q12 * (double)cosph * (double)sinph);
+  REAL q13t = q13 * cosph - q23 * sinph;
+  REAL q23t = q23 * cosph + q13 * sinph;
+  REAL q33t = -q11 - q22;
+  REAL qox1 = qox * cosph - qoy * sinph;
+  REAL qoy1 = qox * sinph + qoy * cosph;
+  REAL x1 = x - qox1, y1 = y - qoy1, z1 = z - qoz;
+  REAL r2 = x1 * x1 + y1 * y1 + z1 * z1;
+  REAL r7 = FN(cube)(r2) * (REAL)sqrt((double)r2);
+  REAL xqx = (REAL)((double)(q11t * x1 * x1) + 2.0 * (double)q12t * (double)x1 * (double)y1 +
+                    (double)(q22t * y1 * y1) +
+                    2.0 * (double)(q13t * x1 + q23t * y1) * (double)z1 +
+                    (double)(q33t * z1 * z1));
+  REAL a, c;
+  if (n == 0) { a = q11t * x1 + q12t * y1 + q13t * z1; c = x1; }
+  else if (n == 1) { a = q12t * x1 + q22t * y1 + q23t * z1; c = y1; }
+  else if (n == 2) { a = q13t * x1 + q23t * y1 + q33t * z1; c = z1; }
+  else return 0;
+  return (REAL)((-2.0 * (double)a * (double)r2 + 5.0 * (double)c * (double)xqx) /
+                (double)(r7 + TINYR));
+}
+
+static REAL FN(quadru_dipole)(const oracle_params* p, REAL x, REAL y, REAL z,
+                              REAL phase, int n) {
+  return FN(dipole2)(x, y, z, (REAL)p->p1, (REAL)p->p2, (REAL)p->p3, phase, n) +
+         FN(quadrupole)(x, y, z, (REAL)p->q11, (REAL)p->q12, (REAL)p->q13,
+                        (REAL)p->q22, (REAL)p->q23, (REAL)p->q_offset_x,
+                        (REAL)p->q_offset_y, (REAL)p->q_offset_z, phase, n);
+}
+
+/* Periodic guard fill of one array along `dir` (single-rank send_guard_cells,
+ * sim_env_impl.hpp:179-228 + sim_env.cpp:42-115). */
+static void FN(periodic_fill)(REAL* a, const FN(grid_t) * g, int dir) {
+  const int ext[3] = {g->d0, g->d1, g->d2};
+  const size_t stride[3] = {1, (size_t)g->d0, (size_t)g->d0 * g->d1};
+  const int gd = g->g[dir];
+  const int n = ext[dir] - 2 * gd;
+  const int a1 = (dir == 0) ? 1 : 0, a2 = (dir == 2) ? 1 : 2;
+  for (int q = 0; q < ext[a2]; ++q)
+    for (int pp = 0; pp < ext[a1]; ++pp) {
+      size_t base = pp * stride[a1] + q * stride[a2];
+      for (int s = 0; s < gd; ++s) {
+        a[base + (size_t)(n + gd + s) * stride[dir]] = a[base + (size_t)(gd + s) * stride[dir]];
+        a[base + (size_t)s * stride[dir]] = a[base + (size_t)(n + s) * stride[dir]];
+      }
+    }
+}
+
+static void FN(guard_fill)(REAL* const* U, const FN(grid_t) * g, const oracle_params* p) {
+  for (int dir = 0; dir < 3; ++dir) {
+    if (!p->periodic[dir] || g->g[dir] == 0) continue;
+    for (int f = 0; f < 7; ++f) FN(periodic_fill)(U[f], g, dir);
+  }
+}
+
+#define LOOP_BOX(g, sh)                                                        \
+  _Pragma("omp parallel for schedule(static)")                                 \
+  for (int k = (g)->g[2] - (sh); k < (g)->d2 - (g)->g[2] + (sh); ++k)          \
+    for (int j = (g)->g[1] - (sh); j < (g)->d1 - (g)->g[1] + (sh); ++j)        \
+      for (int i = (g)->g[0] - (sh); i < (g)->d0 - (g)->g[0] + (sh); ++i)
+
+/* rk_step (CPU field_solver_EZ.cpp:105-322, GPU field_solver_EZ.cu:36-211):
+ * dU = As dU + dt RHS(U) over the update box, then U += Bs dU. */
+static void FN(rk_step)(const oracle_params* p, const FN(grid_t) * g, REAL* const* U,
+                        REAL* const* dU, REAL* const* aux, REAL As, REAL Bs) {
+  const int sh = p->shift_ghost;
+  const size_t s0 = 1, s1 = (size_t)g->d0, s2 = (size_t)g->d0 * g->d1;
+  REAL *Ex = U[0], *Ey = U[1], *Ez = U[2], *Bx = U[3], *By = U[4], *Bz = U[5], *P = U[6];
+  const REAL dt = (REAL)p->dt, ch2 = (REAL)p->ch2, tau = (REAL)p->tau;
+  const REAL gam_dt = (REAL)p->damp_gamma / dt;
+  const int cpu = p->semantics == ORACLE_SEM_CPU_REF;
+  const int lanes = p->taper_lanes > 0 ? p->taper_lanes : 1;
+  LOOP_BOX(g, sh) {
+    size_t ijk = (size_t)i + ((size_t)j + (size_t)k * g->d1) * g->d0;
+    REAL ix = g->inv_delta[0], iy = g->inv_delta[1], iz = g->inv_delta[2];
+    REAL rotBx = FN(df1)(Bz, ijk, s1, iy) - FN(df1)(By, ijk, s2, iz);
+    REAL rotBy = FN(df1)(Bx, ijk, s2, iz) - FN(df1)(Bz, ijk, s0, ix);
+    REAL rotBz = FN(df1)(By, ijk, s0, ix) - FN(df1)(Bx, ijk, s1, iy);
+    REAL rotEx = FN(df1)(Ez, ijk, s1, iy) - FN(df1)(Ey, ijk, s2, iz);
+    REAL rotEy = FN(df1)(Ex, ijk, s2, iz) - FN(df1)(Ez, ijk, s0, ix);
+    REAL rotEz = FN(df1)(Ey, ijk, s0, ix) - FN(df1)(Ex, ijk, s1, iy);
+    REAL divE = FN(df1)(Ex, ijk, s0, ix) + FN(df1)(Ey, ijk, s1, iy) + FN(df1)(Ez, ijk, s2, iz);
+    REAL divB = FN(df1)(Bx, ijk, s0, ix) + FN(df1)(By, ijk, s1, iy) + FN(df1)(Bz, ijk, s2, iz);
+    REAL ex = Ex[ijk], ey = Ey[ijk], ez = Ez[ijk], bx = Bx[ijk], by = By[ijk], bz = Bz[ijk];
+    REAL B2 = bx * bx + by * by + bz * bz;
+    if (B2 < TINYR) B2 = TINYR;
+    REAL Jx, Jy, Jz;
+    if (p->use_edotb_damping) {
+      REAL E2 = ex * ex + ey * ey + ez * ez;
+      REAL chi2 = B2 - E2;
+      REAL EdotB = ex * bx + ey * by + ez * bz;
+      REAL E02 = (REAL)0.5 * ((REAL)sqrt((double)(chi2 * chi2 + (REAL)4.0 * EdotB * EdotB)) - chi2) + B2;
+      REAL Jp = (bx * rotBx + by * rotBy + bz * rotBz) - (ex * rotEx + ey * rotEy + ez * rotEz) +
+                EdotB * gam_dt;
+      Jx = divE * (ey * bz - ez * by) / E02 + Jp * bx / B2;
+      Jy = divE * (ez * bx - ex * bz) / E02 + Jp * by / B2;
+      Jz = divE * (ex * by - ey * bx) / E02 + Jp * bz / B2;
+    } else {
+      REAL Jp = (bx * rotBx + by * rotBy + bz * rotBz) - (ex * rotEx + ey * rotEy + ez * rotEz);
+      Jx = (divE * (ey * bz - ez * by) + Jp * bx) / B2;
+      Jy = (divE * (ez * bx - ex * bz) + Jp * by) / B2;
+      Jz = (divE * (ex * by - ey * bx) + Jp * bz) / B2;
+    }
+    if (aux) {
+      aux[0][ijk] = Jx; aux[1][ijk] = Jy; aux[2][ijk] = Jz;
+      aux[3][ijk] = divE; aux[4][ijk] = divB;
+    }
+    REAL Px = 0, Py = 0, Pz = 0;
+    if (p->divB_clean) {
+      Px = FN(df1)(P, ijk, s0, ix);
+      Py = FN(df1)(P, ijk, s1, iy);
+      Pz = FN(df1)(P, ijk, s2, iz);
+    }
+    REAL s = 1;
+    if (cpu) {
+      /* taper with the reference's lane offsets in y and z */
+      int lane = (i - (g->g[0] - sh)) % lanes;
+      int ibase = i - lane;
+      REAL x = (REAL)lane * g->delta[0] + FN(pos)(g, 0, ibase);
+      REAL y = (REAL)lane * g->delta[1] + FN(pos)(g, 1, j);
+      REAL z = (REAL)lane * g->delta[2] + FN(pos)(g, 2, k);
+      REAL r = (REAL)sqrt((double)(x * x + y * y + z * z));
+      s = (REAL)0.5 * ((REAL)1.0 - TANHR((r - (REAL)3.0) / (REAL)0.5));
+      dU[3][ijk] = dU[3][ijk] * As - (rotEx + Px * s) * dt;
+      dU[4][ijk] = dU[4][ijk] * As - (rotEy + Py * s) * dt;
+      dU[5][ijk] = dU[5][ijk] * As - (rotEz + Pz * s) * dt;
+      dU[0][ijk] = dU[0][ijk] * As + (rotBx - Jx) * dt;
+      dU[1][ijk] = dU[1][ijk] * As + (rotBy - Jy) * dt;
+      dU[2][ijk] = dU[2][ijk] * As + (rotBz - Jz) * dt;
+      dU[6][ijk] = dU[6][ijk] * As - P[ijk] / tau - divB * ch2 * dt;
+    } else {
+      dU[3][ijk] = As * dU[3][ijk] - dt * (rotEx + Px);
+      dU[4][ijk] = As * dU[4][ijk] - dt * (rotEy + Py);
+      dU[5][ijk] = As * dU[5][ijk] - dt * (rotEz + Pz);
+      dU[0][ijk] = As * dU[0][ijk] + dt * (rotBx - Jx);
+      dU[1][ijk] = As * dU[1][ijk] + dt * (rotBy - Jy);
+      dU[2][ijk] = As * dU[2][ijk] + dt * (rotBz - Jz);
+      dU[6][ijk] = As * dU[6][ijk] - dt * ch2 * divB - P[ijk] / tau;
+    }
+  }
+  LOOP_BOX(g, sh) {
+    size_t ijk = (size_t)i + ((size_t)j + (size_t)k * g->d1) * g->d0;
+    for (int f = 0; f < 7; ++f) U[f][ijk] = U[f][ijk] + Bs * dU[f][ijk];
+  }
+}
+
+/* Clamps.  CPU build: clean_epar_check_eGTb always (field_solver_EZ.cpp:552-634).
+ * GPU build: kernel_Epar if clean_ep, kernel_EgtB if check_egb (.cu:213-270). */
+static void FN(clamps)(const oracle_params* p, const FN(grid_t) * g, REAL* const* U) {
+  const int sh = p->shift_ghost;
+  const int cpu = p->semantics == ORACLE_SEM_CPU_REF;
+  REAL *Ex = U[0], *Ey = U[1], *Ez = U[2], *Bx = U[3], *By = U[4], *Bz = U[5];
+  if (cpu || p->clean_ep) {
+    LOOP_BOX(g, sh) {
+      size_t ijk = (size_t)i + ((size_t)j + (size_t)k * g->d1) * g->d0;
+      REAL bx = Bx[ijk], by = By[ijk], bz = Bz[ijk];
+      REAL B2 = bx * bx + by * by + bz * bz;
+      if (B2 < TINYR) B2 = TINYR;
+      REAL EB = cpu ? (bx * Ex[ijk] + by * Ey[ijk] + bz * Ez[ijk])
+                    : (Ex[ijk] * bx + Ey[ijk] * by + Ez[ijk] * bz);
+      if (cpu) {
+        Ex[ijk] = Ex[ijk] - EB * bx / B2;
+        Ey[ijk] = Ey[ijk] - EB * by / B2;
+        Ez[ijk] = Ez[ijk] - EB * bz / B2;
+      } else {
+        Ex[ijk] = Ex[ijk] - EB / B2 * bx;
+        Ey[ijk] = Ey[ijk] - EB / B2 * by;
+        Ez[ijk] = Ez[ijk] - EB / B2 * bz;
+      }
+    }
+  }
+  if (cpu || p->check_egb) {
+    LOOP_BOX(g, sh) {
+      size_t ijk = (size_t)i + ((size_t)j + (size_t)k * g->d1) * g->d0;
+      REAL bx = Bx[ijk], by = By[ijk], bz = Bz[ijk];
+      REAL B2 = bx * bx + by * by + bz * bz;
+      if (B2 < TINYR) B2 = TINYR;
+      REAL ex = Ex[ijk], ey = Ey[ijk], ez = Ez[ijk];
+      REAL E2 = ex * ex + ey * ey + ez * ez;
+      if (E2 > B2) {
+        REAL s = (REAL)sqrt((double)(B2 / E2));
+        Ex[ijk] = ex * s;
+        Ey[ijk] = ey * s;
+        Ez[ijk] = ez * s;
+      }
+    }
+  }
+}
+
+/* boundary_pulsar: CPU field_solver_EZ.cpp:711-839 (rl = 1.5 R), GPU
+ * field_solver_EZ.cu:394-528 (rl = 2 R).  With wpert != NULL it is the CPU
+ * build's boundary_alfven (.cpp:841-1005): the star uses dipole2 and the
+ * rotation velocity carries the Alfven perturbation. */
+static REAL FN(wpert)(REAL t, REAL th, REAL tp_start, REAL tp_end, REAL dw0, REAL nT,
+                      REAL rpert1, REAL rpert2) {
+  /* field_solver_EZ.cpp:644-661 */
+  REAL th1 = (REAL)acos(sqrt(1.0 - 1.0 / (double)rpert1));
+  REAL th2 = (REAL)acos(sqrt(1.0 - 1.0 / (double)rpert2));
+  if (th1 > th2) { REAL tmp = th1; th1 = th2; th2 = tmp; }
+  REAL mu = (REAL)((double)(th1 + th2) / 2.0);
+  REAL s = (REAL)((double)(mu - th1) / 3.0);
+  if (t >= tp_start && t <= tp_end && th >= th1 && th <= th2) {
+    REAL q = (th - mu) / s;
+    return (REAL)((double)dw0 * exp(-0.5 * (double)(q * q)) *
+                  sin((double)(t - tp_start) * 2.0 * M_PI * (double)nT / (double)(tp_end - tp_start)));
+  }
+  return 0;
+}
+
+static REAL FN(wpert3d)(REAL t, REAL th, REAL ph, REAL tp_start, REAL tp_end, REAL dw0,
+                        REAL nT, REAL rpert1, REAL rpert2, REAL ph1, REAL ph2, REAL dph) {
+  /* field_solver_EZ.cpp:663-684 */
+  REAL th1 = (REAL)acos(sqrt(1.0 - 1.0 / (double)rpert1));
+  REAL th2 = (REAL)acos(sqrt(1.0 - 1.0 / (double)rpert2));
+  if (th1 > th2) { REAL tmp = th1; th1 = th2; th2 = tmp; }
+  REAL mu = (REAL)((double)(th1 + th2) / 2.0);
+  REAL s = (REAL)((double)(mu - th1) / 3.0);
+  if (t >= tp_start && t <= tp_end && th >= th1 && th <= th2) {
+    REAL q = (th - mu) / s;
+    double v = (double)dw0 * exp(-0.5 * (double)(q * q)) *
+               sin((double)(t - tp_start) * 2.0 * M_PI * (double)nT / (double)(tp_end - tp_start)) *
+               (double)FN(shape)(ph, (REAL)((double)ph2 * M_PI), (REAL)((double)dph * M_PI)) *
+               (1.0 - (double)FN(shape)(ph, (REAL)((double)ph1 * M_PI), (REAL)((double)dph * M_PI)));
+    return (REAL)v;
+  }
+  return 0;
+}
+
+static void FN(twistv)(REAL t, REAL x, REAL y, REAL z, REAL tp_start, REAL tp_end,
+                       REAL dw0, REAL nT, REAL theta0, REAL drpert, REAL ri, REAL v[3]) {
+  /* field_solver_EZ.cpp:686-709 */
+  REAL costh0 = (REAL)cos((double)theta0), sinth0 = (REAL)sin((double)theta0);
+  REAL x1 = -x * costh0 + z * sinth0, y1 = y, z1 = x * sinth0 + z * costh0;
+  REAL r = (REAL)sqrt((double)(x * x + y * y + z * z));
+  REAL R1 = (REAL)sqrt((double)(x1 * x1 + y1 * y1));
+  REAL costh = x1 / (R1 + TINYR), sinth = y1 / (R1 + TINYR);
+  REAL dw = 0;
+  if (r > ri && z1 >= 0 && R1 <= drpert && t >= tp_start && t <= tp_end) {
+    double c = cos((double)(R1 / drpert) * M_PI / 2.0);
+    double s2 = sin((double)(t - tp_start) * M_PI / (double)(tp_end - tp_start));
+    dw = (REAL)((double)dw0 * (c * c) *
+                sin((double)(t - tp_start) * 2.0 * M_PI * (double)nT / (double)(tp_end - tp_start)) *
+                (s2 * s2));
+  }
+  v[0] = dw * R1 * sinth * costh0;
+  v[1] = dw * R1 * costh;
+  v[2] = -dw * R1 * sinth * sinth0;
+}
+
+static void FN(boundary_star)(const oracle_params* p, const FN(grid_t) * g, REAL* const* U,
+                              REAL t, int alfven) {
+  const int sh = p->shift_ghost;
+  const int cpu = p->semantics == ORACLE_SEM_CPU_REF;
+  REAL *Ex = U[0], *Ey = U[1], *Ez = U[2], *Bx = U[3], *By = U[4], *Bz = U[5];
+  const REAL R = (REAL)p->radius;
+  const REAL rl = cpu ? (REAL)(1.5 * (double)R) : (REAL)(2.0 * (double)R);
+  const REAL ri = (REAL)(0.5 * (double)R);
+  const REAL scaleEpar = (REAL)(0.5 * (double)g->delta[0]);
+  const REAL scaleEperp = (REAL)(0.25 * (double)g->delta[0]);
+  const REAL scaleBperp = scaleEpar, scaleBpar = scaleBperp;
+  const REAL d1 = (REAL)(4.0 * (double)g->delta[0]);
+  const REAL d0 = 0;
+  const REAL phase = (REAL)p->omega * t;
+  const REAL b0 = (REAL)p->b0;
+  LOOP_BOX(g, sh) {
+    size_t ijk = (size_t)i + ((size_t)j + (size_t)k * g->d1) * g->d0;
+    REAL x = FN(pos)(g, 0, i), y = FN(pos)(g, 1, j), z = FN(pos)(g, 2, k);
+    REAL r2 = x * x + y * y + z * z;
+    if (r2 < TINYR) r2 = TINYR;
+    REAL r = (REAL)sqrt((double)r2);
+    if (!(r < rl)) continue;
+    REAL vx, vy, vz;
+    REAL bxn, byn, bzn;
+    if (alfven) {
+      REAL th = (REAL)acos((double)(z / r));
+      REAL ph = (REAL)atan2((double)y, (double)x);
+      if (p->pert_type == 0 || p->pert_type == 1) {
+        REAL w0 = 0, w1 = 0;
+        if (p->pert_type == 0) {
+          w0 = FN(wpert)(t, th, (REAL)p->tp_start, (REAL)p->tp_end, (REAL)p->dw0, (REAL)p->nT,
+                         (REAL)p->rpert1, (REAL)p->rpert2);
+          w1 = FN(wpert)(t, th, (REAL)p->tp_start1, (REAL)p->tp_end1, (REAL)p->dw1,
+                         (REAL)p->nT1, (REAL)p->rpert11, (REAL)p->rpert21);
+        } else {
+          w0 = FN(wpert3d)(t, th, ph, (REAL)p->tp_start, (REAL)p->tp_end, (REAL)p->dw0,
+                           (REAL)p->nT, (REAL)p->rpert1, (REAL)p->rpert2, (REAL)p->ph1,
+                           (REAL)p->ph2, (REAL)p->dph);
+          w1 = FN(wpert3d)(t, th, ph, (REAL)p->tp_start1, (REAL)p->tp_end1, (REAL)p->dw1,
+                           (REAL)p->nT1, (REAL)p->rpert11, (REAL)p->rpert21, (REAL)p->ph11,
+                           (REAL)p->ph21, (REAL)p->dph1);
+        }
+        REAL w = (REAL)p->omega + w0 + w1;
+        vx = -w * y; vy = w * x; vz = 0;
+      } else {
+        REAL v[3] = {0, 0, 0};
+        FN(twistv)(t, x, y, z, (REAL)p->tp_start, (REAL)p->tp_end, (REAL)p->dw0, (REAL)p->nT,
+                   (REAL)p->theta0, (REAL)p->drpert, ri, v);
+        vx = v[0]; vy = v[1]; vz = v[2];
+      }
+      bxn = b0 * FN(dipole2)(x, y, z, (REAL)p->p1, (REAL)p->p2, (REAL)p->p3, phase, 0);
+      byn = b0 * FN(dipole2)(x, y, z, (REAL)p->p1, (REAL)p->p2, (REAL)p->p3, phase, 1);
+      bzn = b0 * FN(dipole2)(x, y, z, (REAL)p->p1, (REAL)p->p2, (REAL)p->p3, phase, 2);
+    } else {
+      REAL w = (REAL)p->omega;
+      vx = -w * y; vy = w * x; vz = 0;
+      bxn = b0 * FN(quadru_dipole)(p, x, y, z, phase, 0);
+      byn = b0 * FN(quadru_dipole)(p, x, y, z, phase, 1);
+      bzn = b0 * FN(quadru_dipole)(p, x, y, z, phase, 2);
+    }
+    REAL s = FN(shape)(r, R - d1, scaleBperp);
+    REAL bn_dot_r = bxn * x + byn * y + bzn * z;
+    REAL B_dot_r = Bx[ijk] * x + By[ijk] * y + Bz[ijk] * z;
+    REAL Bxnew = bn_dot_r * x / r2 * s + B_dot_r * x / r2 * (1 - s);
+    REAL Bynew = bn_dot_r * y / r2 * s + B_dot_r * y / r2 * (1 - s);
+    REAL Bznew = bn_dot_r * z / r2 * s + B_dot_r * z / r2 * (1 - s);
+    s = FN(shape)(r, R - d1, scaleBpar);
+    Bxnew += (bxn - bn_dot_r * x / r2) * s + (Bx[ijk] - B_dot_r * x / r2) * (1 - s);
+    Bynew += (byn - bn_dot_r * y / r2) * s + (By[ijk] - B_dot_r * y / r2) * (1 - s);
+    Bznew += (bzn - bn_dot_r * z / r2) * s + (Bz[ijk] - B_dot_r * z / r2) * (1 - s);
+    Bx[ijk] = Bxnew; By[ijk] = Bynew; Bz[ijk] = Bznew;
+    REAL exn = -vy * Bz[ijk] + vz * By[ijk];
+    REAL eyn = vx * Bz[ijk] - vz * Bx[ijk];
+    REAL ezn = -vx * By[ijk] + vy * Bx[ijk];
+    REAL en_dot_r = (exn * x + eyn * y + ezn * z);
+    REAL E_dot_r = (Ex[ijk] * x + Ey[ijk] * y + Ez[ijk] * z);
+    s = FN(shape)(r, R - d0, scaleEperp);
+    REAL Exnew = en_dot_r * x / r2 * s + E_dot_r * x / r2 * (1 - s);
+    REAL Eynew = en_dot_r * y / r2 * s + E_dot_r * y / r2 * (1 - s);
+    REAL Eznew = en_dot_r * z / r2 * s + E_dot_r * z / r2 * (1 - s);
+    s = FN(shape)(r, R - d0, scaleEpar);
+    Exnew += (exn - en_dot_r * x / r2) * s + (Ex[ijk] - E_dot_r * x / r2) * (1 - s);
+    Eynew += (eyn - en_dot_r * y / r2) * s + (Ey[ijk] - E_dot_r * y / r2) * (1 - s);
+    Eznew += (ezn - en_dot_r * z / r2) * s + (Ez[ijk] - E_dot_r * z / r2) * (1 - s);
+    Ex[ijk] = Exnew; Ey[ijk] = Eynew; Ez[ijk] = Eznew;
+    if (r < ri) {
+      Bx[ijk] = bxn; By[ijk] = byn; Bz[ijk] = bzn;
+      Ex[ijk] = exn; Ey[ijk] = eyn; Ez[ijk] = ezn;
+    }
+  }
+}
+
+/* pmlsigma (damping_boundary.h:14-22) */
+static inline REAL FN(pmlsigma)(REAL x, REAL xl, REAL xh, REAL scale, REAL sig0) {
+  if (x > xh) return sig0 * FN(cube)((x - xh) / scale);
+  if (x < xl) return sig0 * FN(cube)((xl - x) / scale);
+  return 0;
+}
+
+/* Absorbing layer at the last stage.  CPU: damping_boundary.cpp:5-83 (B relaxes
+ * toward the background dipole Bbg, P untouched, per-axis scale).  GPU:
+ * boundary.cu:81-145 (B toward 0, P toward Pn, delta[0] scale on all axes). */
+static void FN(absorbing)(const oracle_params* p, const FN(grid_t) * g, REAL* const* U,
+                          REAL* const* Un, REAL* const* Bbg) {
+  const int sh = p->shift_ghost;
+  const int cpu = p->semantics == ORACLE_SEM_CPU_REF;
+  REAL lo[3], hi[3], sc[3];
+  for (int a = 0; a < 3; ++a) {
+    REAL L = (REAL)p->lower[a], S = (REAL)p->size[a];
+    REAL pm = (REAL)p->pml[a] * g->delta[a];
+    hi[a] = L + S - pm;
+    lo[a] = L + pm;
+    sc[a] = (REAL)p->pmllen * (cpu ? g->delta[a] : g->delta[0]);
+  }
+  const REAL sig0 = (REAL)p->sigpml;
+  LOOP_BOX(g, sh) {
+    size_t ijk = (size_t)i + ((size_t)j + (size_t)k * g->d1) * g->d0;
+    REAL x = FN(pos)(g, 0, i), y = FN(pos)(g, 1, j), z = FN(pos)(g, 2, k);
+    if (!(x > hi[0] || x < lo[0] || y > hi[1] || y < lo[1] || z > hi[2] || z < lo[2])) continue;
+    REAL sig = FN(pmlsigma)(x, lo[0], hi[0], sc[0], sig0) + FN(pmlsigma)(y, lo[1], hi[1], sc[1], sig0) +
+               FN(pmlsigma)(z, lo[2], hi[2], sc[2], sig0);
+    if (!(sig > TINYR)) continue;
+    /* the reference mixes a double (1.0 - exp) / sig with float fields */
+    const double ed = exp(-(double)sig);
+    const double fd = (1.0 - ed) / (double)sig;
+    for (int c = 0; c < 3; ++c)
+      U[c][ijk] = (REAL)(ed * (double)Un[c][ijk] + fd * (double)(U[c][ijk] - Un[c][ijk]));
+    for (int c = 3; c < 6; ++c) {
+      if (cpu) {
+        REAL bg = Bbg[c - 3][ijk];
+        U[c][ijk] = (REAL)((double)bg + ed * (double)(Un[c][ijk] - bg) +
+                           fd * (double)(U[c][ijk] - Un[c][ijk]));
+      } else {
+        U[c][ijk] = (REAL)(ed * (double)Un[c][ijk] + fd * (double)(U[c][ijk] - Un[c][ijk]));
+      }
+    }
+    if (!cpu) U[6][ijk] = (REAL)(ed * (double)Un[6][ijk] + fd * (double)(U[6][ijk] - Un[6][ijk]));
+  }
+}
+
+/* Kreiss-Oliger (CPU .cpp:324-457 on E, B; GPU .cu:272-392 on E, B, P). */
+static void FN(kreiss_oliger)(const oracle_params* p, const FN(grid_t) * g, REAL* const* U,
+                              REAL* const* tmp) {
+  const int sh = p->shift_ghost;
+  const int nf = (p->semantics == ORACLE_SEM_CPU_REF) ? 6 : 7;
+  const size_t s1 = (size_t)g->d0, s2 = (size_t)g->d0 * g->d1;
+  LOOP_BOX(g, sh) {
+    size_t ijk = (size_t)i + ((size_t)j + (size_t)k * g->d1) * g->d0;
+    for (int f = 0; f < nf; ++f)
+      tmp[f][ijk] = FN(d6)(U[f], ijk, 1) + FN(d6)(U[f], ijk, s1) + FN(d6)(U[f], ijk, s2);
+  }
+  const REAL KO_const = (REAL)(-1.0 / 64.0);
+  const REAL c = -(REAL)p->KOeps * KO_const;
+  LOOP_BOX(g, sh) {
+    size_t ijk = (size_t)i + ((size_t)j + (size_t)k * g->d1) * g->d0;
+    for (int f = 0; f < nf; ++f) U[f][ijk] = U[f][ijk] + tmp[f][ijk] * c;
+  }
+}
+
+int FN(oracle_evolve)(const oracle_params* p, REAL* const* U, REAL* const* aux, int nsteps,
+                      double time0) {
+  FN(grid_t) g;
+  g.d0 = p->N[0] + 2 * p->guard[0];
+  g.d1 = p->N[1] + 2 * p->guard[1];
+  g.d2 = p->N[2] + 2 * p->guard[2];
+  for (int a = 0; a < 3; ++a) {
+    g.g[a] = p->guard[a];
+    if (p->N[a] <= 0) return -1;
+    g.delta[a] = (REAL)p->size[a] / (REAL)p->N[a];
+    g.inv_delta[a] = (REAL)1.0 / g.delta[a];
+    g.lower[a] = (REAL)p->lower[a];
+    if (p->guard[a] < p->shift_ghost + 3) return -2; /* KO needs radius 3 */
+  }
+  g.n = (size_t)g.d0 * g.d1 * g.d2;
+  REAL* buf = (REAL*)calloc(g.n * 16, sizeof(REAL));
+  if (!buf) return -3;
+  REAL* dU[7];
+  REAL* Un[7];
+  REAL* Bbg[3];
+  for (int f = 0; f < 7; ++f) { dU[f] = buf + f * g.n; Un[f] = buf + (7 + f) * g.n; }
+  for (int c = 0; c < 2; ++c) Bbg[c] = buf + (14 + c) * g.n;
+  REAL* Bbg2 = (REAL*)calloc(g.n, sizeof(REAL));
+  if (!Bbg2) { free(buf); return -3; }
+  Bbg[2] = Bbg2;
+  /* Bbg = b0 * quadru_dipole at phase 0, every point incl. guards
+   * (field_solver_EZ.cpp:66-85) */
+  if (p->semantics == ORACLE_SEM_CPU_REF) {
+    for (int k = 0; k < g.d2; ++k)
+      for (int j = 0; j < g.d1; ++j)
+        for (int i = 0; i < g.d0; ++i) {
+          size_t ijk = (size_t)i + ((size_t)j + (size_t)k * g.d1) * g.d0;
+          REAL x = FN(pos)(&g, 0, i), y = FN(pos)(&g, 1, j), z = FN(pos)(&g, 2, k);
+          for (int c = 0; c < 3; ++c) Bbg[c][ijk] = (REAL)p->b0 * FN(quadru_dipole)(p, x, y, z, 0, c);
+        }
+  }
+  static const double As_d[5] = {0, -0.4178904745, -1.192151694643, -1.697784692471,
+                                 -1.514183444257};
+  static const double Bs_d[5] = {0.1496590219993, 0.3792103129999, 0.8229550293869,
+                                 0.6994504559488, 0.1530572479681};
+  static const double cs_d[5] = {0, 0.1496590219993, 0.3704009573644, 0.6222557631345,
+                                 0.9582821306784};
+  REAL time = (REAL)time0;
+  const REAL dt = (REAL)p->dt;
+  const int cpu = p->semantics == ORACLE_SEM_CPU_REF;
+  const int absorbing = 1; /* both builds call it at the last stage */
+  for (int step = 0; step < nsteps; ++step) {
+    for (int f = 0; f < 7; ++f) memcpy(Un[f], U[f], g.n * sizeof(REAL));
+    for (int st = 0; st < 5; ++st) {
+      FN(rk_step)(p, &g, U, dU, aux, (REAL)As_d[st], (REAL)Bs_d[st]);
+      FN(clamps)(p, &g, U);
+      REAL ts = time + (REAL)cs_d[st] * dt;
+      if (p->problem == 1) FN(boundary_star)(p, &g, U, ts, 0);
+      else if (p->problem == 2 && cpu) FN(boundary_star)(p, &g, U, ts, 1);
+      if (st == 4 && absorbing) FN(absorbing)(p, &g, U, Un, Bbg);
+      FN(guard_fill)(U, &g, p);
+    }
+    /* the KO scratch reuses the start-of-step copies, as the reference does */
+    FN(kreiss_oliger)(p, &g, U, Un);
+    FN(clamps)(p, &g, U);
+    if (p->problem == 1) FN(boundary_star)(p, &g, U, time + dt, 0);
+    else if (p->problem == 2 && cpu) FN(boundary_star)(p, &g, U, time + dt, 1);
+    FN(guard_fill)(U, &g, p);
+    time += dt;
+  }
+  free(Bbg2);
+  free(buf);
+  return 0;
+}
+
+#undef LOOP_BOX
+#undef FN
+#undef CAT
+#undef CAT2

@@ -1,0 +1,115 @@
+"""Parity of the CUDA field update (through the C ABI) with the oracle.
+
+FP32 results are held to the bar of helpers.fp32_parity: within
+max(2e-5, 4 x noise) relative L2 of the reference float build, per field,
+where `noise` is the float build's own distance from the same algorithm in
+FP64, and no less accurate than the float build against that FP64 run (up to
+2x + 2e-5).  FP64 results must match the reference FP64 build to 1e-10.
+"""
+import numpy as np
+import pytest
+
+from coffee_b200 import problems
+from coffee_b200.solver import run_flat
+from helpers import fp32_parity, golden_cases, interior, load_golden, rel_l2
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_golden_fp32(name):
+    p, d = load_golden(name)
+    aux = "aux_f32" in d
+    out, auxo = run_flat(p, list(d["in_f32"]), int(d["steps"]), time0=float(d["time0"]),
+                         semantics="cpu", aux=aux)
+    ok, rep = fp32_parity(out, d["out_f32"], d["out_f64_l16"])
+    assert ok, rep
+    if aux:
+        sl = interior(p)
+        for f in range(5):
+            assert rel_l2(auxo[f][sl], d["aux_f32"][f][sl]) < 2e-4, (name, f)
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_golden_fp64(name):
+    p, d = load_golden(name)
+    f64 = [a.astype(np.float64) for a in d["in_f32"]]
+    out, _ = run_flat(p, f64, int(d["steps"]), time0=float(d["time0"]), semantics="cpu")
+    for f in range(7):
+        assert rel_l2(out[f], d["out_f64"][f]) < 1e-10, (name, f, rel_l2(out[f], d["out_f64"][f]))
+
+
+def _check_vs_port(p, f32, steps, semantics, t0=0.0):
+    sem = oracle.SEM_CPU_REF if semantics == "cpu" else oracle.SEM_GPU_REF
+    ref32, _ = oracle.run_port(p, f32, steps, time0=t0, semantics=sem, taper_lanes=16)
+    ref64, _ = oracle.run_port(p, [a.astype(np.float64) for a in f32], steps, time0=t0,
+                               semantics=sem, taper_lanes=16)
+    out, _ = run_flat(p, f32, steps, time0=t0, semantics=semantics)
+    ok, rep = fp32_parity(out, ref32, ref64)
+    assert ok, rep
+    # guard points hold exactly what the kernels wrote: compare them too
+    for f in range(7):
+        assert rel_l2(out[f], ref32[f]) <= max(1e-4, 8 * rel_l2(ref32[f], ref64[f])), f
+
+
+@pytest.mark.parametrize("semantics", ["cpu", "gpu"])
+def test_alfven_both_semantics(semantics):
+    p = problems.alfven_params(32)
+    _check_vs_port(p, problems.alfven_fields(p, np.float32), 6, semantics)
+
+
+@pytest.mark.parametrize("semantics", ["cpu", "gpu"])
+def test_pulsar_absorbing_both_semantics(semantics):
+    p = problems.pulsar_params(N=32, half_size=8.0, radius=2.0, omega=0.1, b0=1.0, pml=6)
+    p.q11 = 0.05
+    p.q12 = 0.02
+    p.p1 = 0.3
+    _check_vs_port(p, problems.pulsar_fields(p, np.float32), 4, semantics, t0=0.3)
+
+
+def test_mixed_boundaries_noncubic():
+    p = problems.turbulence_params(16)
+    p.N = [48, 16, 32]
+    p.size = [3.0, 1.0, 2.0]
+    p.periodic_boundary = [True, False, True]
+    p.pml = [0, 3, 0]
+    p.pmllen = 2
+    _check_vs_port(p, problems.turbulence_fields(p, np.float32), 5, "cpu")
+
+
+def test_shift_ghost():
+    p = problems.alfven_params(16)
+    p.guard = [5, 5, 5]
+    p.shift_ghost = 2
+    p.periodic_boundary = [True, False, True]
+    _check_vs_port(p, problems.alfven_fields(p, np.float32), 3, "gpu")
+
+
+def test_no_cleaning_no_damping():
+    p = problems.turbulence_params(32)
+    p.divB_clean = False
+    p.use_edotb_damping = False
+    p.KOeps = 0.1
+    p.clean_ep = False
+    p.check_egb = False
+    for sem in ("cpu", "gpu"):
+        _check_vs_port(p, problems.turbulence_fields(p, np.float32), 4, sem)
+
+
+def test_config1_alfven128_100_steps():
+    """The Alfven-wave configuration at full size and length: 128^3 + 3
+    guards, periodic, dt = dx/2, 100 steps, all 7 fields, against the
+    reference float build when it is built here (else the restatement), with
+    the FP32 noise floor from the restatement in FP64."""
+    p = problems.alfven_params(128)
+    f32 = problems.alfven_fields(p, np.float32)
+    if oracle.reference_available(np.float32):
+        ref32, _, _ = oracle.run_reference(p, f32, 100)
+    else:
+        ref32, _ = oracle.run_port(p, f32, 100, taper_lanes=16)
+    ref64, _ = oracle.run_port(p, [a.astype(np.float64) for a in f32], 100, taper_lanes=16)
+    out, _ = run_flat(p, f32, 100)
+    ok, rep = fp32_parity(out, ref32, ref64)
+    print(rep)
+    assert ok, rep
