@@ -158,7 +158,7 @@ def cpu_reference_run(steps: int, warmup: int, nproc: int | None = None):
     from oracle import oracle
 
     cores = nproc or len(os.sched_getaffinity(0))
-    cores = max(1, min(cores, 128))
+    cores = max(1, min(cores, 64))
     tmp = tempfile.mkdtemp(prefix="coffee_cpu_")
     try:
         p, fin, cfg = _slab_input(tmp)

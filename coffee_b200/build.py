@@ -35,25 +35,30 @@ def _newest_input() -> float:
     return max(os.path.getmtime(p) for p in paths if os.path.isfile(p))
 
 
-def build(force: bool = False, ptxas_verbose: bool = False, log=None) -> str:
-    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _newest_input():
-        return LIB
+def build(force: bool = False, ptxas_verbose: bool = False, log=None, defines=(),
+          out: str | None = None) -> str:
+    """Compile the library; `defines` (e.g. ["COFFEE_F32_STY=4"]) override
+    tile-shape macros, `out` writes the library elsewhere than LIB."""
+    target = out or LIB
+    if not force and not defines and os.path.exists(target) and \
+            os.path.getmtime(target) >= _newest_input():
+        return target
     cmd = [nvcc_path(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "--shared",
            "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
            "-I", INCLUDE, "-I", CSRC, "-DCOFFEE_BUILDING_LIBRARY",
-           "-o", LIB + ".tmp"]
+           "-o", target + ".tmp"] + [f"-D{d}" for d in defines]
     if ptxas_verbose:
         cmd += ["-Xptxas", "-v"]
     cmd += [os.path.join(CSRC, s) for s in SOURCES]
     cmd += ["-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
-    out = r.stdout + r.stderr
+    text = r.stdout + r.stderr
     if log is not None:
-        log.write(out)
+        log.write(text)
     if r.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({r.returncode}):\n{out[-6000:]}")
-    os.replace(LIB + ".tmp", LIB)
-    return LIB
+        raise RuntimeError(f"nvcc failed ({r.returncode}):\n{text[-6000:]}")
+    os.replace(target + ".tmp", target)
+    return target
 
 
 if __name__ == "__main__":

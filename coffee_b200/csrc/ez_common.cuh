@@ -47,6 +47,9 @@ struct EzConst {
 };
 
 template <typename T> struct F7 { T* p[7]; };
+// Seven values of one point, passed by value to the out-of-line boundary
+// functions so that the caller's registers never need an address.
+template <typename T> struct V7 { T v[7]; };
 template <typename T> struct F5 { T* p[5]; };
 
 // ---- cp.async helpers (sm_80+ asynchronous global->shared copies) --------

@@ -170,11 +170,11 @@ __device__ inline void twistv_dev(const EzConst<T>& c, T t, T x, T y, T z, T ri,
 // The blend itself, kept out of line: only points near the star reach it,
 // so its registers do not weigh on the streaming loop.
 template <typename T>
-__device__ __noinline__ void star_blend(const EzConst<T>& c, T x, T y, T z, T r2, T r, T t,
-                                        T u[6]) {
+__device__ __noinline__ V7<T> star_blend(const EzConst<T>& c, T x, T y, T z, T r2, T r, T t,
+                                         V7<T> u) {
   const bool cpu = c.semantics == SEM_CPU_REF;
   const bool alfven = (c.problem == 2);
-  T ex = u[0], ey = u[1], ez = u[2], bx = u[3], by = u[4], bz = u[5];
+  T ex = u.v[0], ey = u.v[1], ez = u.v[2], bx = u.v[3], by = u.v[4], bz = u.v[5];
   const T R = c.radius;
   const T ri = (T)(0.5 * (double)R);
   const T scaleEpar = (T)(0.5 * (double)c.delta[0]);
@@ -239,7 +239,8 @@ __device__ __noinline__ void star_blend(const EzConst<T>& c, T x, T y, T z, T r2
     bx = bn[0]; by = bn[1]; bz = bn[2];
     ex = exn; ey = eyn; ez = ezn;
   }
-  u[0] = ex; u[1] = ey; u[2] = ez; u[3] = bx; u[4] = by; u[5] = bz;
+  u.v[0] = ex; u.v[1] = ey; u.v[2] = ez; u.v[3] = bx; u.v[4] = by; u.v[5] = bz;
+  return u;
 }
 
 template <typename T>
@@ -252,7 +253,14 @@ __device__ __forceinline__ void star_boundary(const EzConst<T>& c, int i, int j,
   if (r2 < Tiny<T>::v) r2 = Tiny<T>::v;
   const T r = sqrt(r2);
   const T rl = cpu ? (T)(1.5 * (double)c.radius) : (T)(2.0 * (double)c.radius);
-  if (r < rl) star_blend(c, x, y, z, r2, r, t, u);
+  if (r < rl) {
+    V7<T> in;
+#pragma unroll
+    for (int f = 0; f < 7; ++f) in.v[f] = u[f];
+    const V7<T> out = star_blend(c, x, y, z, r2, r, t, in);
+#pragma unroll
+    for (int f = 0; f < 6; ++f) u[f] = out.v[f];
+  }
 }
 
 // ---------------------------------------------------------- absorbing layer
@@ -286,20 +294,23 @@ __device__ __forceinline__ T absorbing_sigma(const EzConst<T>& c, int i, int j, 
 // P is left alone, the length scale uses each axis' delta.  GPU build
 // (boundary.cu:127-142): B toward zero, P toward Pn, delta[0] on every axis.
 template <typename T>
-__device__ __noinline__ void absorbing_apply(const EzConst<T>& c, int i, int j, int k, T sig, T u[7],
-                                       const T un[7]) {
+__device__ __noinline__ V7<T> absorbing_apply(const EzConst<T>& c, int i, int j, int k, T sig,
+                                              V7<T> u, const V7<T> un) {
   const double ed = exp(-(double)sig);
   const double fd = (1.0 - ed) / (double)sig;
-  for (int a = 0; a < 3; ++a) u[a] = (T)(ed * (double)un[a] + fd * (double)(u[a] - un[a]));
+  for (int a = 0; a < 3; ++a)
+    u.v[a] = (T)(ed * (double)un.v[a] + fd * (double)(u.v[a] - un.v[a]));
   if (c.semantics == SEM_CPU_REF) {
     T bg[3];
     star_field(c, grid_pos(c, 0, i), grid_pos(c, 1, j), grid_pos(c, 2, k), (T)0, bg);
     for (int a = 0; a < 3; ++a)
-      u[3 + a] = (T)((double)bg[a] + ed * (double)(un[3 + a] - bg[a]) +
-                     fd * (double)(u[3 + a] - un[3 + a]));
+      u.v[3 + a] = (T)((double)bg[a] + ed * (double)(un.v[3 + a] - bg[a]) +
+                       fd * (double)(u.v[3 + a] - un.v[3 + a]));
   } else {
-    for (int a = 3; a < 7; ++a) u[a] = (T)(ed * (double)un[a] + fd * (double)(u[a] - un[a]));
+    for (int a = 3; a < 7; ++a)
+      u.v[a] = (T)(ed * (double)un.v[a] + fd * (double)(u.v[a] - un.v[a]));
   }
+  return u;
 }
 
 // The P-gradient taper of the CPU build's rk_step
