@@ -67,7 +67,6 @@ struct coffee_solver {
   int aux;
   int timing;
   uint64_t synced_generation;
-  int stage_variant;
   int kchunk_stage, kchunk_ko;
   dim3 grid_stage, grid_ko;
   std::vector<cudaEvent_t> events;   // pairs around each launch (timing mode)
@@ -90,48 +89,32 @@ template <typename T> struct Shape;
 #define COFFEE_F32_STY 8
 #endif
 #ifndef COFFEE_F32_SPF
-#define COFFEE_F32_SPF 2
-#endif
-#ifndef COFFEE_F32_RPF
-#define COFFEE_F32_RPF 3
+#define COFFEE_F32_SPF 1
 #endif
 #ifndef COFFEE_F32_KTY
-#define COFFEE_F32_KTY 4
+#define COFFEE_F32_KTY 8
 #endif
 #ifndef COFFEE_F32_KPF
-#define COFFEE_F32_KPF 3
+#define COFFEE_F32_KPF 1
 #endif
 template <> struct Shape<float> {
   static constexpr int STX = 32, STY = COFFEE_F32_STY, SPF = COFFEE_F32_SPF;  // stage tile, prefetch
-  static constexpr int RPF = COFFEE_F32_RPF;  // prefetch of the register-window stage
   static constexpr int KTX = 32, KTY = COFFEE_F32_KTY, KPF = COFFEE_F32_KPF;  // KO tile, prefetch
 };
 template <> struct Shape<double> {
   static constexpr int STX = 32, STY = 4, SPF = 1;
-  static constexpr int RPF = 1;
   static constexpr int KTX = 32, KTY = 4, KPF = 1;
 };
-
-// Stage kernel variants: all operands from shared memory, or the z stencil
-// in a register window (COFFEE_STAGE_KERNEL=smem|regwin at solver creation).
-enum StageVariant { STAGE_SMEM = 0, STAGE_REGWIN = 1 };
-
-template <typename T>
-size_t stage_rw_smem() {
-  using S = Shape<T>;
-  return stage_rw_smem_bytes<T, S::STX, S::STY, S::RPF>();
-}
 
 template <typename T>
 size_t stage_smem(bool first) {
   using S = Shape<T>;
-  return first ? TileCfg<T, S::STX, S::STY, 2, S::SPF, false>::smem_bytes
-               : TileCfg<T, S::STX, S::STY, 2, S::SPF, true>::smem_bytes;
+  return stage_smem_bytes<T, S::STX, S::STY, S::SPF>(first);
 }
 template <typename T>
 size_t ko_smem() {
   using S = Shape<T>;
-  return TileCfg<T, S::KTX, S::KTY, 3, S::KPF, false>::smem_bytes;
+  return ko_smem_bytes<T, S::KTX, S::KTY, S::KPF>();
 }
 
 // LSRK(5,4) coefficients of the reference (field_solver_EZ.cpp:1009-1014)
@@ -181,6 +164,7 @@ void build_const(const coffee_env* env, int semantics, EzConst<T>* c) {
   c->dt = (T)p.dt;
   c->ch2 = (T)p.ch2;
   c->tau = (T)p.tau;
+  c->inv_tau = (T)(1.0 / (double)c->tau);
   // -KOeps * KO_const with KO_const = -1/64 (FFE_DISSIPATION_ORDER 6)
   c->ko_c = -(T)p.KOeps * (T)(-1.0 / 64.0);
   c->gam_dt = (T)p.damp_gamma / (T)p.dt;
@@ -624,26 +608,16 @@ static int configure_solver(coffee_solver* s) {
   using S = Shape<T>;
   auto k_first = ez_stage_kernel<T, S::STX, S::STY, S::SPF, true>;
   auto k_rest = ez_stage_kernel<T, S::STX, S::STY, S::SPF, false>;
-  auto r_first = ez_stage_rw_kernel<T, S::STX, S::STY, S::RPF, true>;
-  auto r_rest = ez_stage_rw_kernel<T, S::STX, S::STY, S::RPF, false>;
   auto k_ko = ez_ko_kernel<T, S::KTX, S::KTY, S::KPF>;
   COFFEE_CUDA_TRY(cudaFuncSetAttribute(k_first, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)stage_smem<T>(true)));
   COFFEE_CUDA_TRY(cudaFuncSetAttribute(k_rest, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)stage_smem<T>(false)));
-  COFFEE_CUDA_TRY(cudaFuncSetAttribute(r_first, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)stage_rw_smem<T>()));
-  COFFEE_CUDA_TRY(cudaFuncSetAttribute(r_rest, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)stage_rw_smem<T>()));
   COFFEE_CUDA_TRY(cudaFuncSetAttribute(k_ko, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)ko_smem<T>()));
   int per_sm_stage = 1, per_sm_ko = 1;
-  if (s->stage_variant == STAGE_REGWIN)
-    COFFEE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm_stage, r_rest, S::STX * S::STY, stage_rw_smem<T>()));
-  else
-    COFFEE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm_stage, k_rest, S::STX * S::STY, stage_smem<T>(false)));
+  COFFEE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm_stage, k_rest, S::STX * S::STY, stage_smem<T>(false)));
   COFFEE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &per_sm_ko, k_ko, S::KTX * S::KTY, ko_smem<T>()));
   if (per_sm_stage < 1 || per_sm_ko < 1)
@@ -689,14 +663,6 @@ extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int varia
   bool abs_any = env->p.shift_ghost > 0;
   for (int a = 0; a < 3; ++a) abs_any = abs_any || env->p.pml[a] > 0;
   s->absorbing = abs_any;
-  s->stage_variant = STAGE_SMEM;
-  if (const char* v = std::getenv("COFFEE_STAGE_KERNEL")) {
-    if (std::strcmp(v, "regwin") == 0) s->stage_variant = STAGE_REGWIN;
-    else if (std::strcmp(v, "smem") != 0) {
-      delete s;
-      return fail(COFFEE_E_INVALID, "COFFEE_STAGE_KERNEL must be smem or regwin, got %s", v);
-    }
-  }
   const size_t bytes = f->n * f->elem;
   auto cleanup = [&]() {
     for (int a = 0; a < 7; ++a) {
@@ -833,24 +799,14 @@ static int run_steps(coffee_solver* s, double time, int nsteps) {
         COFFEE_CUDA_TRY(cudaEventRecord(e0, st));
       }
       const T As = (T)kAs[i], Bs = (T)kBs[i];
-      if (s->stage_variant == STAGE_REGWIN) {
-        if (i == 0)
-          ez_stage_rw_kernel<T, S::STX, S::STY, S::RPF, true>
-              <<<s->grid_stage, bs, stage_rw_smem<T>(), st>>>(c, srcc, dst, dU, Un, aux, As, Bs,
-                                                              tst, s->kchunk_stage, flags);
-        else
-          ez_stage_rw_kernel<T, S::STX, S::STY, S::RPF, false>
-              <<<s->grid_stage, bs, stage_rw_smem<T>(), st>>>(c, srcc, dst, dU, Un, aux, As, Bs,
-                                                              tst, s->kchunk_stage, flags);
-      } else if (i == 0) {
+      if (i == 0)
         ez_stage_kernel<T, S::STX, S::STY, S::SPF, true>
             <<<s->grid_stage, bs, stage_smem<T>(true), st>>>(c, srcc, dst, dU, Un, aux, As, Bs,
                                                              tst, s->kchunk_stage, flags);
-      } else {
+      else
         ez_stage_kernel<T, S::STX, S::STY, S::SPF, false>
             <<<s->grid_stage, bs, stage_smem<T>(false), st>>>(c, srcc, dst, dU, Un, aux, As,
                                                               Bs, tst, s->kchunk_stage, flags);
-      }
       COFFEE_CUDA_TRY(cudaGetLastError());
       if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(e1, st));
     }

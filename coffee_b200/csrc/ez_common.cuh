@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace coffee {
 
 // TINY of the reference (src/data/typedefs.h:6-12)
@@ -30,7 +32,7 @@ template <typename T>
 struct EzConst {
   GridGeom g;
   T delta[3], inv_delta[3], lower[3];
-  T dt, ch2, tau;
+  T dt, ch2, tau, inv_tau;
   T ko_c;           // -KOeps * KO_const, KO_const = -1/64
   T gam_dt;         // damp_gamma / dt
   int use_edotb, divB_clean, clean_ep, check_egb;
@@ -69,5 +71,44 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
+
+// ---- shared-memory loads at a 32-bit address plus a compile-time offset --
+// (one instruction per operand: no address arithmetic in the stencil loop)
+template <typename T, int OFF>
+__device__ __forceinline__ T lds(uint32_t a) {
+  static_assert(OFF >= 0, "offsets are measured from the tile corner");
+  T v;
+  if constexpr (sizeof(T) == 4)
+    asm volatile("ld.shared.f32 %0, [%1+%2];\n" : "=f"(v) : "r"(a), "n"(OFF));
+  else
+    asm volatile("ld.shared.f64 %0, [%1+%2];\n" : "=d"(v) : "r"(a), "n"(OFF));
+  return v;
+}
+
+// static_for<N>(fn) calls fn(std::integral_constant<int, 0..N-1>) in order,
+// so the index can feed template arguments (compile-time offsets).
+template <int I, int N>
+struct StaticFor {
+  template <class Fn>
+  __device__ __forceinline__ static void run(Fn& fn) {
+    fn(std::integral_constant<int, I>{});
+    StaticFor<I + 1, N>::run(fn);
+  }
+};
+template <int N>
+struct StaticFor<N, N> {
+  template <class Fn>
+  __device__ __forceinline__ static void run(Fn&) {}
+};
+template <int N, class Fn>
+__device__ __forceinline__ void static_for(Fn&& fn) {
+  StaticFor<0, N>::run(fn);
+}
+
+// ---- field-precision arithmetic helpers ---------------------------------
+// FP32: hardware reciprocal-based division (max 2 ulp for the operand
+// ranges here: divisors are floored at TINY); FP64: IEEE division.
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
 
 }  // namespace coffee

@@ -4,34 +4,33 @@
 // Both kernels stream along z.  A CTA owns a TX x TY column of points and a
 // chunk of z planes.  Each z plane of the 7 fields (E, B, P), with a halo of
 // H points in x and y, is copied global -> shared memory by cp.async into a
-// ring of 2H+1+PF planes, PF planes ahead of the plane being computed, so the
-// HBM reads of the next planes overlap the arithmetic of this one.  Every
-// stencil operand (x, y and z neighbours) is then read from shared memory.
-// The LSRK accumulators dU are read in the same copy groups (no halo) and
-// written back in place; the new E, B, P go to a second buffer (stencil
-// reads of other points still need the old values), together with their
-// periodic guard images, so no separate halo-exchange pass is needed.
+// ring of planes, PF planes ahead of the plane being computed, so the HBM
+// reads of the next planes overlap the arithmetic of this one.  The new
+// E, B, P go to a second buffer (stencil reads of other points still need
+// the old values), together with their periodic guard images, so no separate
+// halo-exchange pass is needed.
+//
+// The kernels are bound by instruction issue more than by anything else, so
+// the stencil loops are written to cost one instruction per operand: shared
+// memory is addressed by 32-bit addresses with the field / neighbour offsets
+// as compile-time immediates (lds<T, OFF>), loops over the 7 fields are
+// unrolled at compile time (static_for), and the guard-image bookkeeping is
+// skipped for points that have no image.
 #pragma once
 
 #include "ez_physics.cuh"
 
 namespace coffee {
 
-template <typename T, int TX, int TY, int H, int PF, bool WITH_DU>
-struct TileCfg {
-  static constexpr int R = 2 * H + 1 + PF;  // ring depth in planes
-  static constexpr int SX = TX + 2 * H;     // shared row pitch
-  static constexpr int SY = TY + 2 * H;
-  static constexpr int PLANE = SX * SY;     // one field, one plane
-  static constexpr int NT = TX * TY;
-  static constexpr int NLOAD = (PLANE + NT - 1) / NT;
-  static constexpr int DU_SLOTS = WITH_DU ? PF + 1 : 0;
-  static constexpr size_t smem_bytes =
-      ((size_t)R * 7 * PLANE + (size_t)DU_SLOTS * 7 * NT) * sizeof(T);
-};
-
 // Flags of the stage kernel.
 enum StageFlags { ST_LAST = 1, ST_AUX = 2, ST_WRITE_UN = 4 };
+
+// Minimum resident CTAs for __launch_bounds__: two 256-thread CTAs (or the
+// equivalent) per SM in FP32, which caps registers at 128 per thread.
+template <typename T, int NT>
+constexpr int min_blocks() {
+  return (sizeof(T) == 4) ? ((512 / NT) > 0 ? 512 / NT : 1) : 1;
+}
 
 // 4th-order first derivative (reference diff1_4, finite_diff.h:13-18):
 // ((f-2 - f+2) + 8 (f+1 - f-1)) * inv_delta / 12.
@@ -47,22 +46,36 @@ __device__ __forceinline__ T d6_2(T m3, T m2, T m1, T c, T p1, T p2, T p3) {
   return ((m3 + p3) - (T)6 * (m2 + p2)) + ((T)15 * (m1 + p1) - (T)20 * c);
 }
 
-// Write the 7 new values of point (i, j, k) to `out` at the point and at
-// its periodic guard images.
+// Write the 7 new values of point (i, j, k) (linear index o) to `out` at the
+// point and at its periodic guard images.
 template <typename T>
-__device__ __forceinline__ void store_with_images(const GridGeom& g, const F7<T>& out, int i,
-                                                  int j, int k, const T u[7]) {
-  int xs[2], ys[2], zs[2];
-  const int nx = periodic_targets(g, 0, i, xs);
-  const int ny = periodic_targets(g, 1, j, ys);
-  const int nz = periodic_targets(g, 2, k, zs);
-  for (int c = 0; c < nz; ++c)
-    for (int b = 0; b < ny; ++b)
-      for (int a = 0; a < nx; ++a) {
-        const long long o = (long long)zs[c] * g.sz + (long long)ys[b] * g.sy + xs[a];
+__device__ __forceinline__ void store_with_images(const GridGeom& g, const ColumnCtx<T>& col,
+                                                  const F7<T>& out, int k, long long o,
+                                                  const T u[7]) {
+  if (col.xy_simple && only_self(g, 2, k)) {
 #pragma unroll
-        for (int f = 0; f < 7; ++f) out.p[f][o] = u[f];
+    for (int f = 0; f < 7; ++f) out.p[f][o] = u[f];
+    return;
+  }
+  int xs[2], ys[2], zs[2];
+  const int nx = periodic_targets(g, 0, col.i, xs);
+  const int ny = periodic_targets(g, 1, col.j, ys);
+  const int nz = periodic_targets(g, 2, k, zs);
+#pragma unroll
+  for (int cz = 0; cz < 2; ++cz) {
+    if (cz >= nz) break;
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      if (b >= ny) break;
+#pragma unroll
+      for (int a = 0; a < 2; ++a) {
+        if (a >= nx) break;
+        const long long q = (long long)zs[cz] * g.sz + (long long)ys[b] * g.sy + xs[a];
+#pragma unroll
+        for (int f = 0; f < 7; ++f) out.p[f][q] = u[f];
       }
+    }
+  }
 }
 
 // Everything a stage does at one point once its derivatives are known:
@@ -75,7 +88,7 @@ template <typename T, bool FIRST>
 __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7], const T dx[7],
                                             const T dy[7], const T dz[7], const T dold[7],
                                             const T As, const T Bs, const T tst,
-                                            const int flags, const int i, const int j,
+                                            const int flags, const ColumnCtx<T>& col,
                                             const int k, const long long o, const F7<T>& du,
                                             const F7<T>& un, const F5<T>& aux,
                                             const F7<T>& uout) {
@@ -98,13 +111,13 @@ __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7], c
     const T EdotB = ex * bx + ey * by + ez * bz;
     const T E02 = (T)0.5 * (sqrt(chi2 * chi2 + (T)4 * EdotB * EdotB) - chi2) + B2;
     const T Jp = BrotB - ErotE + EdotB * c.gam_dt;
-    const T a = divE / E02, b = Jp / B2;
+    const T a = fdiv(divE, E02), b = fdiv(Jp, B2);
     Jx = a * cx + b * bx;
     Jy = a * cy + b * by;
     Jz = a * cz + b * bz;
   } else {
     const T Jp = BrotB - ErotE;
-    const T rB2 = (T)1 / B2;
+    const T rB2 = fdiv((T)1, B2);
     Jx = (divE * cx + Jp * bx) * rB2;
     Jy = (divE * cy + Jp * by) * rB2;
     Jz = (divE * cz + Jp * bz) * rB2;
@@ -115,7 +128,7 @@ __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7], c
     Py = dy[6];
     Pz = dz[6];
     if (cpu) {
-      const T s = p_taper(c, i, j, k);
+      const T s = p_taper(c, col, k);
       Px *= s;
       Py *= s;
       Pz *= s;
@@ -130,13 +143,13 @@ __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7], c
   d[3] = -(rotEx + Px) * dt;
   d[4] = -(rotEy + Py) * dt;
   d[5] = -(rotEz + Pz) * dt;
-  d[6] = -P / c.tau - divB * c.ch2 * dt;
+  d[6] = -P * c.inv_tau - divB * c.ch2 * dt;
   if constexpr (!FIRST) {
 #pragma unroll
     for (int f = 0; f < 7; ++f) d[f] = fma(dold[f], As, d[f]);
   }
   // the start-of-step copy is only read inside the absorbing layer
-  const T sig = c.absorbing ? absorbing_sigma(c, i, j, k) : (T)0;
+  const T sig = c.absorbing ? absorbing_sigma(c, col.i, col.j, k) : (T)0;
   if ((flags & ST_WRITE_UN) != 0 && sig > (T)0) {
 #pragma unroll
     for (int f = 0; f < 7; ++f) un.p[f][o] = u[f];
@@ -154,7 +167,7 @@ __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7], c
 #pragma unroll
   for (int f = 0; f < 7; ++f) nu[f] = fma(d[f], Bs, u[f]);
   apply_clamps(c, nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
-  star_boundary(c, i, j, k, tst, nu);
+  star_boundary(c, col.i, col.j, k, tst, nu);
   if ((flags & ST_LAST) != 0 && sig > (T)0) {
     V7<T> uv, unv;
 #pragma unroll
@@ -162,12 +175,50 @@ __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7], c
       uv.v[f] = nu[f];
       unv.v[f] = un.p[f][o];
     }
-    uv = absorbing_apply(c, i, j, k, sig, uv, unv);
+    uv = absorbing_apply(c, col.i, col.j, k, sig, uv, unv);
 #pragma unroll
     for (int f = 0; f < 7; ++f) nu[f] = uv.v[f];
   }
-  store_with_images(c.g, uout, i, j, k, nu);
+  store_with_images(c.g, col, uout, k, o, nu);
 }
+
+// Per-thread table of the shared-memory slots and global offsets that a
+// CTA's threads copy for one (TX + 2H) x (TY + 2H) tile of one field plane.
+template <typename T, int TX, int TY, int H>
+struct TileLoader {
+  static constexpr int SX = TX + 2 * H, SY = TY + 2 * H, PLANE = SX * SY, NT = TX * TY;
+  static constexpr int NLOAD = (PLANE + NT - 1) / NT;
+  static constexpr int FB = PLANE * (int)sizeof(T);  // bytes of one field plane
+  uint32_t sadd[NLOAD];   // shared byte address within slot 0, field 0
+  long long goff[NLOAD];  // byte offset within a global plane
+  bool lv[NLOAD];
+
+  __device__ __forceinline__ TileLoader(const GridGeom& g, uint32_t sbase, int tid, int gx0,
+                                        int gy0) {
+#pragma unroll
+    for (int m = 0; m < NLOAD; ++m) {
+      const int e = tid + m * NT;
+      const int r = e / SX, cl = e - r * SX;
+      const int gx = gx0 + cl, gy = gy0 + r;
+      lv[m] = (e < PLANE) && gx < g.dims[0] && gy < g.dims[1];
+      sadd[m] = sbase + (uint32_t)(e * (int)sizeof(T));
+      goff[m] = ((long long)gy * g.sy + gx) * (long long)sizeof(T);
+    }
+  }
+
+  // Copy one plane (byte offset pb into each field array) of the 7 fields
+  // into the ring slot at byte offset `slot`.
+  __device__ __forceinline__ void copy(const F7<const T>& uin, long long pb,
+                                       uint32_t slot) const {
+    static_for<7>([&](auto fc) {
+      constexpr int f = decltype(fc)::value;
+      const char* gb = reinterpret_cast<const char*>(uin.p[f]) + pb;
+#pragma unroll
+      for (int m = 0; m < NLOAD; ++m)
+        if (lv[m]) cp_async<sizeof(T)>(sadd[m] + slot + (uint32_t)(f * FB), gb + goff[m]);
+    });
+  }
+};
 
 // ---------------------------------------------------------------------------
 // One LSRK stage (reference rk_step + clamps + star boundary + absorbing
@@ -177,16 +228,29 @@ __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7], c
 //   U'  <- U + Bs dU
 //   U'  <- clamps, star boundary at tst, absorbing layer (ST_LAST)
 // reading U from `uin` and writing U' (with guard images) to `uout`.
+// Shared memory: a ring of 5 + PF planes of the 7 fields with a 2-point x/y
+// halo (z neighbours are read from the ring too), then PF + 1 planes of dU.
 // ---------------------------------------------------------------------------
+template <typename T, int TX, int TY, int PF>
+constexpr size_t stage_smem_bytes(bool first) {
+  return (size_t)(5 + PF) * 7 * (TX + 4) * (TY + 4) * sizeof(T) +
+         (first ? 0 : (size_t)(PF + 1) * 7 * TX * TY * sizeof(T));
+}
+
 template <typename T, int TX, int TY, int PF, bool FIRST>
-__global__ void __launch_bounds__(TX * TY, (sizeof(T) == 4) ? (512 / (TX * TY) > 0 ? 512 / (TX * TY) : 1) : 1)
-    ez_stage_kernel(const __grid_constant__ EzConst<T> c, const F7<const T> uin, const F7<T> uout,
-                    const F7<T> du, const F7<T> un, const F5<T> aux, const T As, const T Bs,
-                    const T tst, const int kchunk, const int flags) {
-  using C = TileCfg<T, TX, TY, 2, PF, !FIRST>;
+__global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
+    ez_stage_kernel(const __grid_constant__ EzConst<T> c, const F7<const T> uin,
+                    const F7<T> uout, const F7<T> du, const F7<T> un, const F5<T> aux,
+                    const T As, const T Bs, const T tst, const int kchunk, const int flags) {
+  using L = TileLoader<T, TX, TY, 2>;
+  constexpr int R = 5 + PF;
+  constexpr int ES = (int)sizeof(T);
+  constexpr int SX = L::SX, FB = L::FB, SB = 7 * FB;
+  constexpr int NT = TX * TY, DFB = NT * ES, DSB = 7 * DFB;
+  constexpr int CEN = (2 * SX + 2) * ES;  // own point, from the corner of its 5x5 patch
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sU = reinterpret_cast<T*>(smem_raw);
-  T* sD = sU + (size_t)C::R * 7 * C::PLANE;
+  const uint32_t sbase = smem_u32(smem_raw);
+  const uint32_t dbase = sbase + (uint32_t)(R * SB);
 
   const GridGeom& g = c.g;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -195,83 +259,67 @@ __global__ void __launch_bounds__(TX * TY, (sizeof(T) == 4) ? (512 / (TX * TY) >
   const int k0 = g.lo[2] + blockIdx.z * kchunk;
   const int k1 = min(k0 + kchunk, g.hi[2]);
   const bool active = (i < g.hi[0]) && (j < g.hi[1]);
-  const int gx0 = g.lo[0] + blockIdx.x * TX - 2;
-  const int gy0 = g.lo[1] + blockIdx.y * TY - 2;
   const long long own = (long long)j * g.sy + i;
-
-  int soff[C::NLOAD];
-  long long goff[C::NLOAD];
-  bool lv[C::NLOAD];
-#pragma unroll
-  for (int m = 0; m < C::NLOAD; ++m) {
-    const int e = tid + m * C::NT;
-    const int r = e / C::SX, col = e - r * C::SX;
-    const int gx = gx0 + col, gy = gy0 + r;
-    lv[m] = (e < C::PLANE) && gx < g.dims[0] && gy < g.dims[1];
-    soff[m] = e;
-    goff[m] = (long long)gy * g.sy + gx;
-  }
+  const ColumnCtx<T> col = make_column(c, i, j);
+  const L loader(g, sbase, tid, g.lo[0] + (int)blockIdx.x * TX - 2,
+                 g.lo[1] + (int)blockIdx.y * TY - 2);
+  const long long pbytes = g.sz * ES;
+  const uint32_t dme = dbase + (uint32_t)(tid * ES);
+  const long long own_b = own * ES;
   const int kend = k1 + 2;  // planes [k0-2, k1+2) are read
 
   auto issue = [&](int kp) {
-    if (kp < kend) {
-      const int slot = kp % C::R;
-#pragma unroll
-      for (int f = 0; f < 7; ++f) {
-        T* base = sU + (size_t)(slot * 7 + f) * C::PLANE;
-        const T* gb = uin.p[f] + (long long)kp * g.sz;
-#pragma unroll
-        for (int m = 0; m < C::NLOAD; ++m)
-          if (lv[m]) cp_async<sizeof(T)>(smem_u32(base + soff[m]), gb + goff[m]);
-      }
-    }
+    if (kp < kend) loader.copy(uin, kp * pbytes, (uint32_t)((kp % R) * SB));
     if constexpr (!FIRST) {
       const int kd = kp - 2;
       if (kd >= k0 && kd < k1 && active) {
-        const int slot = kd % (PF + 1);
-#pragma unroll
-        for (int f = 0; f < 7; ++f)
-          cp_async<sizeof(T)>(smem_u32(sD + (size_t)(slot * 7 + f) * C::NT + tid),
-                              du.p[f] + (long long)kd * g.sz + own);
+        const uint32_t ds = dme + (uint32_t)((kd % (PF + 1)) * DSB);
+        const long long pb = kd * pbytes + own_b;
+        static_for<7>([&](auto fc) {
+          constexpr int f = decltype(fc)::value;
+          cp_async<sizeof(T)>(ds + f * DFB, reinterpret_cast<const char*>(du.p[f]) + pb);
+        });
       }
     }
     cp_async_commit();
   };
-
 #pragma unroll 1
-  for (int p = 0; p < C::R; ++p) issue(k0 - 2 + p);
+  for (int p = 0; p < R; ++p) issue(k0 - 2 + p);
 
   const T six = c.inv_delta[0] / (T)12, siy = c.inv_delta[1] / (T)12,
           siz = c.inv_delta[2] / (T)12;
+  const uint32_t corner = sbase + (uint32_t)((ty * SX + tx) * ES);
 
 #pragma unroll 1
   for (int k = k0; k < k1; ++k) {
     cp_async_wait<PF>();
     __syncthreads();
     if (active) {
-      const int sl[5] = {(k - 2) % C::R, (k - 1) % C::R, k % C::R, (k + 1) % C::R,
-                         (k + 2) % C::R};
-      const int rc = (ty + 2) * C::SX + tx + 2;  // own point within a plane
-      T u[7], dx[7], dy[7], dz[7];
-#pragma unroll
-      for (int f = 0; f < 7; ++f) {
-        const T* pc = sU + (size_t)(sl[2] * 7 + f) * C::PLANE + rc;
-        u[f] = pc[0];
-        dx[f] = d1_4(pc[-2], pc[-1], pc[1], pc[2], six);
-        dy[f] = d1_4(pc[-2 * C::SX], pc[-C::SX], pc[C::SX], pc[2 * C::SX], siy);
-        const T zm2 = sU[(size_t)(sl[0] * 7 + f) * C::PLANE + rc];
-        const T zm1 = sU[(size_t)(sl[1] * 7 + f) * C::PLANE + rc];
-        const T zp1 = sU[(size_t)(sl[3] * 7 + f) * C::PLANE + rc];
-        const T zp2 = sU[(size_t)(sl[4] * 7 + f) * C::PLANE + rc];
-        dz[f] = d1_4(zm2, zm1, zp1, zp2, siz);
-      }
-      T dold[7];
+      const uint32_t a0 = corner + (uint32_t)((k % R) * SB);
+      const uint32_t am2 = corner + (uint32_t)(((k - 2) % R) * SB);
+      const uint32_t am1 = corner + (uint32_t)(((k - 1) % R) * SB);
+      const uint32_t ap1 = corner + (uint32_t)(((k + 1) % R) * SB);
+      const uint32_t ap2 = corner + (uint32_t)(((k + 2) % R) * SB);
+      T u[7], dx[7], dy[7], dz[7], dold[7];
+      static_for<7>([&](auto fc) {
+        constexpr int f = decltype(fc)::value;
+        constexpr int o = f * FB;
+        u[f] = lds<T, o + CEN>(a0);
+        dx[f] = d1_4(lds<T, o + CEN - 2 * ES>(a0), lds<T, o + CEN - ES>(a0),
+                     lds<T, o + CEN + ES>(a0), lds<T, o + CEN + 2 * ES>(a0), six);
+        dy[f] = d1_4(lds<T, o + 2 * ES>(a0), lds<T, o + (SX + 2) * ES>(a0),
+                     lds<T, o + (3 * SX + 2) * ES>(a0), lds<T, o + (4 * SX + 2) * ES>(a0), siy);
+        dz[f] = d1_4(lds<T, o + CEN>(am2), lds<T, o + CEN>(am1), lds<T, o + CEN>(ap1),
+                     lds<T, o + CEN>(ap2), siz);
+      });
       if constexpr (!FIRST) {
-        const int sd = k % (PF + 1);
-#pragma unroll
-        for (int f = 0; f < 7; ++f) dold[f] = sD[(size_t)(sd * 7 + f) * C::NT + tid];
+        const uint32_t ad = dme + (uint32_t)((k % (PF + 1)) * DSB);
+        static_for<7>([&](auto fc) {
+          constexpr int f = decltype(fc)::value;
+          dold[f] = lds<T, f * DFB>(ad);
+        });
       }
-      stage_point<T, FIRST>(c, u, dx, dy, dz, dold, As, Bs, tst, flags, i, j, k,
+      stage_point<T, FIRST>(c, u, dx, dy, dz, dold, As, Bs, tst, flags, col, k,
                             (long long)k * g.sz + own, du, un, aux, uout);
     }
     __syncthreads();
@@ -281,26 +329,31 @@ __global__ void __launch_bounds__(TX * TY, (sizeof(T) == 4) ? (512 / (TX * TY) >
 }
 
 // ---------------------------------------------------------------------------
-// The same LSRK stage with the z stencil in registers.  Each thread keeps,
-// for its own column, the values of planes k-2..k+2 of the 7 fields in a
-// sliding register window; shared memory holds only the planes still needed
-// for x/y neighbours (k) or arriving (k+1..k+2+PF), so the ring is 3 + PF
-// planes deep and a point costs 9 shared loads per field instead of 13.
-// The accumulators dU of plane k+1 are loaded straight into registers while
-// plane k is computed (they have no stencil), which takes them off the
-// shared-memory path entirely.  Results are bit-identical to
-// ez_stage_kernel: only where the operands are fetched from changes.
+// Kreiss-Oliger dissipation + clamps + star boundary at t + dt + guard fill
+// (reference Kreiss_Oliger and the tail of evolve_fields,
+// field_solver_EZ.cpp:324-457, 1057-1072; .cu:272-392, 696-706):
+//   f' = f + (-KOeps * KO_const) * sum_axes diff6_2(f)
+// for E and B (CPU build) or E, B and P (GPU build).  The operator has 18
+// neighbours per field, so the z direction is held in a register window of
+// planes k-3..k+3 per thread; shared memory keeps plane k (x/y neighbours)
+// and the arriving planes k+1..k+3+PF.
 // ---------------------------------------------------------------------------
-template <typename T, int TX, int TY, int PF, bool FIRST>
-__global__ void __launch_bounds__(TX * TY, (sizeof(T) == 4) ? (512 / (TX * TY) > 0 ? 512 / (TX * TY) : 1) : 1)
-    ez_stage_rw_kernel(const __grid_constant__ EzConst<T> c, const F7<const T> uin, const F7<T> uout,
-                       const F7<T> du, const F7<T> un, const F5<T> aux, const T As,
-                       const T Bs, const T tst, const int kchunk, const int flags) {
-  constexpr int R = 3 + PF;  // planes k .. k+2+PF
-  constexpr int SX = TX + 4, SY = TY + 4, PLANE = SX * SY, NT = TX * TY;
-  constexpr int NLOAD = (PLANE + NT - 1) / NT;
+template <typename T, int TX, int TY, int PF>
+constexpr size_t ko_smem_bytes() {
+  return (size_t)(4 + PF) * 7 * (TX + 6) * (TY + 6) * sizeof(T);
+}
+
+template <typename T, int TX, int TY, int PF>
+__global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
+    ez_ko_kernel(const __grid_constant__ EzConst<T> c, const F7<const T> uin,
+                 const F7<T> uout, const T tko, const int kchunk) {
+  using L = TileLoader<T, TX, TY, 3>;
+  constexpr int R = 4 + PF;
+  constexpr int ES = (int)sizeof(T);
+  constexpr int SX = L::SX, FB = L::FB, SB = 7 * FB;
+  constexpr int CEN = (3 * SX + 3) * ES;  // own point, from the corner of its 7x7 patch
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sU = reinterpret_cast<T*>(smem_raw);
+  const uint32_t sbase = smem_u32(smem_raw);
 
   const GridGeom& g = c.g;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -309,194 +362,66 @@ __global__ void __launch_bounds__(TX * TY, (sizeof(T) == 4) ? (512 / (TX * TY) >
   const int k0 = g.lo[2] + blockIdx.z * kchunk;
   const int k1 = min(k0 + kchunk, g.hi[2]);
   const bool active = (i < g.hi[0]) && (j < g.hi[1]);
-  const int gx0 = g.lo[0] + blockIdx.x * TX - 2;
-  const int gy0 = g.lo[1] + blockIdx.y * TY - 2;
   const long long own = (long long)j * g.sy + i;
-
-  int soff[NLOAD];
-  long long goff[NLOAD];
-  bool lv[NLOAD];
-#pragma unroll
-  for (int m = 0; m < NLOAD; ++m) {
-    const int e = tid + m * NT;
-    const int r = e / SX, col = e - r * SX;
-    const int gx = gx0 + col, gy = gy0 + r;
-    lv[m] = (e < PLANE) && gx < g.dims[0] && gy < g.dims[1];
-    soff[m] = e;
-    goff[m] = (long long)gy * g.sy + gx;
-  }
-  const int kend = k1 + 2;  // planes [k0, k1+2) pass through shared memory
+  const ColumnCtx<T> col = make_column(c, i, j);
+  const L loader(g, sbase, tid, g.lo[0] + (int)blockIdx.x * TX - 3,
+                 g.lo[1] + (int)blockIdx.y * TY - 3);
+  const long long pbytes = g.sz * ES;
+  const int kend = k1 + 3;  // planes [k0, k1+3) pass through shared memory
   auto issue = [&](int kp) {
-    if (kp < kend) {
-      const int slot = kp % R;
-#pragma unroll
-      for (int f = 0; f < 7; ++f) {
-        T* base = sU + (size_t)(slot * 7 + f) * PLANE;
-        const T* gb = uin.p[f] + (long long)kp * g.sz;
-#pragma unroll
-        for (int m = 0; m < NLOAD; ++m)
-          if (lv[m]) cp_async<sizeof(T)>(smem_u32(base + soff[m]), gb + goff[m]);
-      }
-    }
+    if (kp < kend) loader.copy(uin, kp * pbytes, (uint32_t)((kp % R) * SB));
     cp_async_commit();
   };
 #pragma unroll 1
   for (int p = 0; p < R; ++p) issue(k0 + p);
 
-  // register window: w[q][f] = U_f at (i, j, k - 2 + q), q = 0..3 held
-  // across iterations (plane k+2 is read each iteration)
-  T w0[7], w1[7], w2[7], w3[7], dn[7];
+  // w[q][f] = field f at (i, j, k - 3 + q); q = 0..5 carried, 6 read each plane
+  T w[7][7];
   if (active) {
 #pragma unroll
-    for (int f = 0; f < 7; ++f) {
-      const T* col = uin.p[f] + own;
-      w0[f] = col[(long long)(k0 - 2) * g.sz];
-      w1[f] = col[(long long)(k0 - 1) * g.sz];
-      w2[f] = col[(long long)k0 * g.sz];
-      w3[f] = col[(long long)(k0 + 1) * g.sz];
-      if constexpr (!FIRST) dn[f] = du.p[f][(long long)k0 * g.sz + own];
-      else dn[f] = (T)0;
-    }
+    for (int f = 0; f < 7; ++f)
+#pragma unroll
+      for (int q = 0; q < 6; ++q) w[q][f] = uin.p[f][(long long)(k0 - 3 + q) * g.sz + own];
   }
-  const T six = c.inv_delta[0] / (T)12, siy = c.inv_delta[1] / (T)12,
-          siz = c.inv_delta[2] / (T)12;
-  const int rc = (ty + 2) * SX + tx + 2;
-
+  const bool ko_p = (c.semantics != SEM_CPU_REF);
+  const uint32_t corner = sbase + (uint32_t)((ty * SX + tx) * ES);
 #pragma unroll 1
   for (int k = k0; k < k1; ++k) {
-    cp_async_wait<PF>();  // plane k+2 has landed
+    cp_async_wait<PF>();  // plane k+3 has landed
     __syncthreads();
     if (active) {
-      T dcur[7];
-#pragma unroll
-      for (int f = 0; f < 7; ++f) dcur[f] = dn[f];
-      if constexpr (!FIRST) {
-        if (k + 1 < k1) {
-#pragma unroll
-          for (int f = 0; f < 7; ++f) dn[f] = du.p[f][(long long)(k + 1) * g.sz + own];
-        }
-      }
-      const int sc = k % R, s2 = (k + 2) % R;
-      T u[7], dx[7], dy[7], dz[7], w4[7];
-#pragma unroll
-      for (int f = 0; f < 7; ++f) {
-        const T* pc = sU + (size_t)(sc * 7 + f) * PLANE + rc;
-        w4[f] = sU[(size_t)(s2 * 7 + f) * PLANE + rc];
-        u[f] = w2[f];
-        dx[f] = d1_4(pc[-2], pc[-1], pc[1], pc[2], six);
-        dy[f] = d1_4(pc[-2 * SX], pc[-SX], pc[SX], pc[2 * SX], siy);
-        dz[f] = d1_4(w0[f], w1[f], w3[f], w4[f], siz);
-      }
-      stage_point<T, FIRST>(c, u, dx, dy, dz, dcur, As, Bs, tst, flags, i, j, k,
-                            (long long)k * g.sz + own, du, un, aux, uout);
-#pragma unroll
-      for (int f = 0; f < 7; ++f) {
-        w0[f] = w1[f];
-        w1[f] = w2[f];
-        w2[f] = w3[f];
-        w3[f] = w4[f];
-      }
-    }
-    __syncthreads();
-    issue(k + R);
-  }
-  cp_async_wait<0>();
-}
-
-template <typename T, int TX, int TY, int PF>
-constexpr size_t stage_rw_smem_bytes() {
-  return (size_t)(3 + PF) * 7 * (TX + 4) * (TY + 4) * sizeof(T);
-}
-
-// ---------------------------------------------------------------------------
-// Kreiss-Oliger dissipation + clamps + star boundary at t + dt + guard fill
-// (reference Kreiss_Oliger and the tail of evolve_fields,
-// field_solver_EZ.cpp:324-457, 1057-1072; .cu:272-392, 696-706):
-//   f' = f + (-KOeps * KO_const) * sum_axes diff6_2(f)
-// for E and B (CPU build) or E, B and P (GPU build).
-// ---------------------------------------------------------------------------
-template <typename T, int TX, int TY, int PF>
-__global__ void __launch_bounds__(TX * TY, (sizeof(T) == 4) ? (512 / (TX * TY) > 0 ? 512 / (TX * TY) : 1) : 1)
-    ez_ko_kernel(const __grid_constant__ EzConst<T> c, const F7<const T> uin, const F7<T> uout, const T tko,
-                 const int kchunk) {
-  using C = TileCfg<T, TX, TY, 3, PF, false>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sU = reinterpret_cast<T*>(smem_raw);
-
-  const GridGeom& g = c.g;
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int i = g.lo[0] + blockIdx.x * TX + tx;
-  const int j = g.lo[1] + blockIdx.y * TY + ty;
-  const int k0 = g.lo[2] + blockIdx.z * kchunk;
-  const int k1 = min(k0 + kchunk, g.hi[2]);
-  const bool active = (i < g.hi[0]) && (j < g.hi[1]);
-  const int gx0 = g.lo[0] + blockIdx.x * TX - 3;
-  const int gy0 = g.lo[1] + blockIdx.y * TY - 3;
-
-  int soff[C::NLOAD];
-  long long goff[C::NLOAD];
-  bool lv[C::NLOAD];
-#pragma unroll
-  for (int m = 0; m < C::NLOAD; ++m) {
-    const int e = tid + m * C::NT;
-    const int r = e / C::SX, col = e - r * C::SX;
-    const int gx = gx0 + col, gy = gy0 + r;
-    lv[m] = (e < C::PLANE) && gx < g.dims[0] && gy < g.dims[1];
-    soff[m] = e;
-    goff[m] = (long long)gy * g.sy + gx;
-  }
-  const int kend = k1 + 3;
-  auto issue = [&](int kp) {
-    if (kp < kend) {
-      const int slot = kp % C::R;
-#pragma unroll
-      for (int f = 0; f < 7; ++f) {
-        T* base = sU + (size_t)(slot * 7 + f) * C::PLANE;
-        const T* gb = uin.p[f] + (long long)kp * g.sz;
-#pragma unroll
-        for (int m = 0; m < C::NLOAD; ++m)
-          if (lv[m]) cp_async<sizeof(T)>(smem_u32(base + soff[m]), gb + goff[m]);
-      }
-    }
-    cp_async_commit();
-  };
-#pragma unroll 1
-  for (int p = 0; p < C::R; ++p) issue(k0 - 3 + p);
-
-  const int nko = (c.semantics == SEM_CPU_REF) ? 6 : 7;
-#pragma unroll 1
-  for (int k = k0; k < k1; ++k) {
-    cp_async_wait<PF>();
-    __syncthreads();
-    if (active) {
-      int sl[7];
-#pragma unroll
-      for (int q = 0; q < 7; ++q) sl[q] = (k - 3 + q) % C::R;
-      const int rc = (ty + 3) * C::SX + tx + 3;
+      const uint32_t a0 = corner + (uint32_t)((k % R) * SB);
+      const uint32_t a3 = corner + (uint32_t)(((k + 3) % R) * SB);
       T nu[7];
-#pragma unroll
-      for (int f = 0; f < 7; ++f) {
-        const T* pc = sU + (size_t)(sl[3] * 7 + f) * C::PLANE + rc;
-        const T cv = pc[0];
-        if (f < nko) {
-          const T kx = d6_2(pc[-3], pc[-2], pc[-1], cv, pc[1], pc[2], pc[3]);
-          const T ky = d6_2(pc[-3 * C::SX], pc[-2 * C::SX], pc[-C::SX], cv, pc[C::SX],
-                            pc[2 * C::SX], pc[3 * C::SX]);
-          T zv[7];
-#pragma unroll
-          for (int q = 0; q < 7; ++q) zv[q] = sU[(size_t)(sl[q] * 7 + f) * C::PLANE + rc];
-          const T kz = d6_2(zv[0], zv[1], zv[2], cv, zv[4], zv[5], zv[6]);
+      static_for<7>([&](auto fc) {
+        constexpr int f = decltype(fc)::value;
+        constexpr int o = f * FB;
+        w[6][f] = lds<T, o + CEN>(a3);
+        const T cv = w[3][f];
+        if (f < 6 || ko_p) {
+          const T kx = d6_2(lds<T, o + CEN - 3 * ES>(a0), lds<T, o + CEN - 2 * ES>(a0),
+                            lds<T, o + CEN - ES>(a0), cv, lds<T, o + CEN + ES>(a0),
+                            lds<T, o + CEN + 2 * ES>(a0), lds<T, o + CEN + 3 * ES>(a0));
+          const T ky = d6_2(lds<T, o + 3 * ES>(a0), lds<T, o + (SX + 3) * ES>(a0),
+                            lds<T, o + (2 * SX + 3) * ES>(a0), cv,
+                            lds<T, o + (4 * SX + 3) * ES>(a0), lds<T, o + (5 * SX + 3) * ES>(a0),
+                            lds<T, o + (6 * SX + 3) * ES>(a0));
+          const T kz = d6_2(w[0][f], w[1][f], w[2][f], cv, w[4][f], w[5][f], w[6][f]);
           nu[f] = fma(kx + ky + kz, c.ko_c, cv);
         } else {
           nu[f] = cv;
         }
-      }
+      });
       apply_clamps(c, nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
       star_boundary(c, i, j, k, tko, nu);
-      store_with_images(g, uout, i, j, k, nu);
+      store_with_images(g, col, uout, k, (long long)k * g.sz + own, nu);
+#pragma unroll
+      for (int q = 0; q < 6; ++q)
+#pragma unroll
+        for (int f = 0; f < 7; ++f) w[q][f] = w[q + 1][f];
     }
     __syncthreads();
-    issue(k + 4 + PF);
+    issue(k + R);
   }
   cp_async_wait<0>();
 }

@@ -25,17 +25,11 @@ __device__ __forceinline__ void apply_clamps(const EzConst<T>& c, T& ex, T& ey, 
   T B2 = bx * bx + by * by + bz * bz;
   if (B2 < Tiny<T>::v) B2 = Tiny<T>::v;
   if (cpu || c.clean_ep) {
-    const T EB = bx * ex + by * ey + bz * ez;
-    if (cpu) {
-      ex = ex - EB * bx / B2;
-      ey = ey - EB * by / B2;
-      ez = ez - EB * bz / B2;
-    } else {
-      const T q = EB / B2;
-      ex = ex - q * bx;
-      ey = ey - q * by;
-      ez = ez - q * bz;
-    }
+    // E -= (E.B / B^2) B, one division shared by the three components
+    const T q = fdiv(bx * ex + by * ey + bz * ez, B2);
+    ex = ex - q * bx;
+    ey = ey - q * by;
+    ez = ez - q * bz;
   }
   if (cpu || c.check_egb) {
     const T E2 = ex * ex + ey * ey + ez * ez;
@@ -313,19 +307,31 @@ __device__ __noinline__ V7<T> absorbing_apply(const EzConst<T>& c, int i, int j,
   return u;
 }
 
+// Per-thread constants of a column (i, j) of a z-streaming kernel: its
+// indices and the parts of the P-gradient taper that do not depend on k.
+template <typename T>
+struct ColumnCtx {
+  int i, j;
+  bool xy_simple;  // the point writes only itself along x and y (no guard image)
+  T taper_x, taper_y, taper_dz;
+};
+
 // The P-gradient taper of the CPU build's rk_step
 // (field_solver_EZ.cpp:222-230): s = (1 - tanh((r - 3)/0.5)) / 2 with x, y
 // and z each offset by lane*delta, lane = position of i within the
-// reference's SIMD vector.
+// reference's SIMD vector.  x and y are fixed per column (ColumnCtx).
+// In FP32 the taper is evaluated as 1 / (1 + exp(4 (r - 3))), the same
+// function written with one exponential and one reciprocal.
+__device__ __forceinline__ float taper_fn(float r) {
+  return __fdividef(1.0f, 1.0f + __expf(4.0f * (r - 3.0f)));
+}
+__device__ __forceinline__ double taper_fn(double r) { return 0.5 * (1.0 - tanh((r - 3.0) / 0.5)); }
+
 template <typename T>
-__device__ __forceinline__ T p_taper(const EzConst<T>& c, int i, int j, int k) {
-  const int lane = (i - c.g.lo[0]) % c.taper_lanes;
-  const T fl = (T)lane;
-  const T x = fl * c.delta[0] + grid_pos(c, 0, i - lane);
-  const T y = fl * c.delta[1] + grid_pos(c, 1, j);
-  const T z = fl * c.delta[2] + grid_pos(c, 2, k);
-  const T r = sqrt(x * x + y * y + z * z);
-  return (T)0.5 * ((T)1 - tanh((r - (T)3) / (T)0.5));
+__device__ __forceinline__ T p_taper(const EzConst<T>& c, const ColumnCtx<T>& col, int k) {
+  const T z = col.taper_dz + grid_pos(c, 2, k);
+  const T r = sqrt(col.taper_x * col.taper_x + col.taper_y * col.taper_y + z * z);
+  return taper_fn(r);
 }
 
 // Index lists of the points that hold the value computed at (i, j, k):
@@ -334,16 +340,41 @@ __device__ __forceinline__ T p_taper(const EzConst<T>& c, int i, int j, int k) {
 // face.  Composing the three directions reproduces the x -> y -> z order of
 // the reference's exchange, corners included.
 __device__ __forceinline__ int periodic_targets(const GridGeom& g, int axis, int i, int out[2]) {
-  int n = 0;
   const int gd = g.guard[axis], d = g.dims[axis], N = g.N[axis];
-  if (!g.periodic[axis]) {
-    out[n++] = i;
-    return n;
-  }
-  if (i >= gd && i < d - gd) out[n++] = i;
-  if (i >= gd && i < 2 * gd) out[n++] = i + N;
-  if (i >= d - 2 * gd && i < d - gd) out[n++] = i - N;
+  out[0] = i;
+  out[1] = i;
+  if (!g.periodic[axis]) return 1;
+  // at most two of: the point itself (interior), i + N, i - N
+  const bool self = (i >= gd && i < d - gd);
+  const bool up = (i >= gd && i < 2 * gd);
+  const bool down = (i >= d - 2 * gd && i < d - gd);
+  int n = 0;
+  if (self) { out[0] = i; n = 1; }
+  if (up) { if (n == 0) out[0] = i + N; else out[1] = i + N; ++n; }
+  if (down) { if (n == 0) out[0] = i - N; else out[1] = i - N; ++n; }
   return n;
+}
+
+// True when index i along `axis` has no periodic guard image and is not a
+// periodic guard itself, i.e. the value computed there is stored only there.
+__device__ __forceinline__ bool only_self(const GridGeom& g, int axis, int i) {
+  if (!g.periodic[axis]) return true;
+  const int gd = g.guard[axis];
+  return i >= 2 * gd && i < g.dims[axis] - 2 * gd;
+}
+
+template <typename T>
+__device__ __forceinline__ ColumnCtx<T> make_column(const EzConst<T>& c, int i, int j) {
+  ColumnCtx<T> col;
+  col.i = i;
+  col.j = j;
+  col.xy_simple = only_self(c.g, 0, i) && only_self(c.g, 1, j);
+  const int lane = (i - c.g.lo[0]) % c.taper_lanes;
+  const T fl = (T)lane;
+  col.taper_x = fl * c.delta[0] + grid_pos(c, 0, i - lane);
+  col.taper_y = fl * c.delta[1] + grid_pos(c, 1, j);
+  col.taper_dz = fl * c.delta[2];
+  return col;
 }
 
 }  // namespace coffee
