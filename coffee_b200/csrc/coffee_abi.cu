@@ -14,7 +14,7 @@
 #include "coffee_b200.h"
 #include "coffee_fld.h"
 #include "coffee_internal.h"
-#include "ez_kernels.cuh"
+#include "ez_launch.cuh"
 
 #define COFFEE_VERSION_STRING "coffee_b200 0.1 (sm_100a)"
 
@@ -40,11 +40,7 @@ using namespace coffee;
 
 // ------------------------------------------------------------------ handles
 
-struct coffee_env {
-  coffee_params p;
-  coffee_grid grid;
-  int device;
-};
+// coffee_env is defined in ez_launch.cuh
 
 struct coffee_fields {
   coffee_env* env;
@@ -67,8 +63,7 @@ struct coffee_solver {
   int aux;
   int timing;
   uint64_t synced_generation;
-  int kchunk_stage, kchunk_ko;
-  dim3 grid_stage, grid_ko;
+  FlatLaunch launch;
   std::vector<cudaEvent_t> events;   // pairs around each launch (timing mode)
   std::vector<int> event_kind;       // COFFEE_KERNEL_* of each pair
   int events_used;
@@ -81,139 +76,6 @@ struct coffee_solver {
 // ------------------------------------------------------------ kernel shapes
 
 namespace {
-
-template <typename T> struct Shape;
-// FP32 tile shapes; the defaults are the tuned values, the macros exist so
-// that a build can be made with other shapes to measure them.
-#ifndef COFFEE_F32_STY
-#define COFFEE_F32_STY 8
-#endif
-#ifndef COFFEE_F32_SPF
-#define COFFEE_F32_SPF 1
-#endif
-#ifndef COFFEE_F32_KTY
-#define COFFEE_F32_KTY 8
-#endif
-#ifndef COFFEE_F32_KPF
-#define COFFEE_F32_KPF 1
-#endif
-template <> struct Shape<float> {
-  static constexpr int STX = 32, STY = COFFEE_F32_STY, SPF = COFFEE_F32_SPF;  // stage tile, prefetch
-  static constexpr int KTX = 32, KTY = COFFEE_F32_KTY, KPF = COFFEE_F32_KPF;  // KO tile, prefetch
-};
-template <> struct Shape<double> {
-  static constexpr int STX = 32, STY = 4, SPF = 1;
-  static constexpr int KTX = 32, KTY = 4, KPF = 1;
-};
-
-template <typename T>
-size_t stage_smem(bool first) {
-  using S = Shape<T>;
-  return stage_smem_bytes<T, S::STX, S::STY, S::SPF>(first);
-}
-template <typename T>
-size_t ko_smem() {
-  using S = Shape<T>;
-  return ko_smem_bytes<T, S::KTX, S::KTY, S::KPF>();
-}
-
-// LSRK(5,4) coefficients of the reference (field_solver_EZ.cpp:1009-1014)
-const double kAs[5] = {0, -0.4178904745, -1.192151694643, -1.697784692471, -1.514183444257};
-const double kBs[5] = {0.1496590219993, 0.3792103129999, 0.8229550293869, 0.6994504559488,
-                       0.1530572479681};
-const double kCs[5] = {0, 0.1496590219993, 0.3704009573644, 0.6222557631345, 0.9582821306784};
-
-// Choose the z chunk of a CTA: enough CTAs to fill the GPU in whole waves,
-// while the 2H halo planes each chunk re-reads stay a small fraction.
-int pick_kchunk(int nz, int nxy_tiles, int slots, int halo) {
-  int best = nz;
-  double best_cost = 1e300;
-  for (int kc = 4; kc <= nz + 3; kc += 4) {
-    const int kk = std::min(kc, nz);
-    const long long ctas = (long long)nxy_tiles * ((nz + kk - 1) / kk);
-    const double waves = std::ceil((double)ctas / (double)slots);
-    const double cost = waves * (kk + 0.5 * halo);
-    if (cost < best_cost - 1e-9) {
-      best_cost = cost;
-      best = kk;
-    }
-    if (kk == nz) break;
-  }
-  return best;
-}
-
-template <typename T>
-void build_const(const coffee_env* env, int semantics, EzConst<T>* c) {
-  const coffee_params& p = env->p;
-  const coffee_grid& gr = env->grid;
-  std::memset(c, 0, sizeof(*c));
-  GridGeom& g = c->g;
-  for (int a = 0; a < 3; ++a) {
-    g.dims[a] = gr.dims[a];
-    g.guard[a] = gr.guard[a];
-    g.N[a] = gr.dims[a] - 2 * gr.guard[a];
-    g.lo[a] = gr.guard[a] - p.shift_ghost;
-    g.hi[a] = gr.dims[a] - gr.guard[a] + p.shift_ghost;
-    g.periodic[a] = p.periodic_boundary[a] ? 1 : 0;
-    c->delta[a] = (T)(T(p.size[a]) / (T)p.N[a]);
-    c->inv_delta[a] = (T)(1.0 / (double)c->delta[a]);
-    c->lower[a] = (T)p.lower[a];
-  }
-  g.sy = gr.dims[0];
-  g.sz = (long long)gr.dims[0] * gr.dims[1];
-  c->dt = (T)p.dt;
-  c->ch2 = (T)p.ch2;
-  c->tau = (T)p.tau;
-  c->inv_tau = (T)(1.0 / (double)c->tau);
-  // -KOeps * KO_const with KO_const = -1/64 (FFE_DISSIPATION_ORDER 6)
-  c->ko_c = -(T)p.KOeps * (T)(-1.0 / 64.0);
-  c->gam_dt = (T)p.damp_gamma / (T)p.dt;
-  c->use_edotb = p.use_edotb_damping;
-  c->divB_clean = p.divB_clean;
-  c->clean_ep = p.clean_ep;
-  c->check_egb = p.check_egb;
-  c->semantics = semantics;
-  c->taper_lanes = (sizeof(T) == 4) ? 16 : 8;  // AVX-512 width of the reference CPU build
-  c->problem = p.problem;
-  bool abs_any = p.shift_ghost > 0;
-  for (int a = 0; a < 3; ++a) {
-    const T pm = (T)p.pml[a] * c->delta[a];
-    c->pml_hi[a] = (T)p.lower[a] + (T)p.size[a] - pm;
-    c->pml_lo[a] = (T)p.lower[a] + pm;
-    c->pml_scale[a] = (T)p.pmllen * (semantics == SEM_CPU_REF ? c->delta[a] : c->delta[0]);
-    if (p.pml[a] > 0) abs_any = true;
-  }
-  c->absorbing = abs_any ? 1 : 0;
-  c->sigpml = (T)p.sigpml;
-  c->radius = (T)p.radius;
-  c->omega = (T)p.omega;
-  c->b0 = (T)p.b0;
-  c->p1 = (T)p.p1; c->p2 = (T)p.p2; c->p3 = (T)p.p3;
-  c->q11 = (T)p.q11; c->q12 = (T)p.q12; c->q13 = (T)p.q13; c->q22 = (T)p.q22;
-  c->q23 = (T)p.q23;
-  c->qox = (T)p.q_offset_x; c->qoy = (T)p.q_offset_y; c->qoz = (T)p.q_offset_z;
-  c->tp_start = (T)p.tp_start; c->tp_end = (T)p.tp_end; c->rpert1 = (T)p.rpert1;
-  c->rpert2 = (T)p.rpert2; c->dw0 = (T)p.dw0; c->nT = (T)p.nT; c->ph1 = (T)p.ph1;
-  c->ph2 = (T)p.ph2; c->dph = (T)p.dph; c->theta0 = (T)p.theta0; c->drpert = (T)p.drpert;
-  c->tp_start1 = (T)p.tp_start1; c->tp_end1 = (T)p.tp_end1; c->rpert11 = (T)p.rpert11;
-  c->rpert21 = (T)p.rpert21; c->dw1 = (T)p.dw1; c->nT1 = (T)p.nT1; c->ph11 = (T)p.ph11;
-  c->ph21 = (T)p.ph21; c->dph1 = (T)p.dph1;
-  c->pert_type = p.pert_type;
-}
-
-template <typename T>
-F7<T> f7(void* const* a) {
-  F7<T> r;
-  for (int f = 0; f < 7; ++f) r.p[f] = static_cast<T*>(a[f]);
-  return r;
-}
-template <typename T>
-F7<const T> f7c(void* const* a) {
-  F7<const T> r;
-  for (int f = 0; f < 7; ++f) r.p[f] = static_cast<const T*>(a[f]);
-  return r;
-}
-
 // Periodic guard fill of all 7 arrays: every guard point of a periodic axis
 // takes the value of the interior point at the wrapped coordinates.
 template <typename T>
@@ -322,11 +184,6 @@ __global__ void count_nonfinite_kernel(const F7<const T> u, const long long n, i
   if ((threadIdx.x & 31) == 0 && local) atomicAdd(count, local);
 }
 
-int num_sms(int device) {
-  int n = 148;
-  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device);
-  return n;
-}
 
 }  // namespace
 
@@ -605,34 +462,7 @@ extern "C" int coffee_fields_fill_guards(coffee_fields* f) {
 
 template <typename T>
 static int configure_solver(coffee_solver* s) {
-  using S = Shape<T>;
-  auto k_first = ez_stage_kernel<T, S::STX, S::STY, S::SPF, true>;
-  auto k_rest = ez_stage_kernel<T, S::STX, S::STY, S::SPF, false>;
-  auto k_ko = ez_ko_kernel<T, S::KTX, S::KTY, S::KPF>;
-  COFFEE_CUDA_TRY(cudaFuncSetAttribute(k_first, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)stage_smem<T>(true)));
-  COFFEE_CUDA_TRY(cudaFuncSetAttribute(k_rest, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)stage_smem<T>(false)));
-  COFFEE_CUDA_TRY(cudaFuncSetAttribute(k_ko, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)ko_smem<T>()));
-  int per_sm_stage = 1, per_sm_ko = 1;
-  COFFEE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm_stage, k_rest, S::STX * S::STY, stage_smem<T>(false)));
-  COFFEE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm_ko, k_ko, S::KTX * S::KTY, ko_smem<T>()));
-  if (per_sm_stage < 1 || per_sm_ko < 1)
-    return fail(COFFEE_E_CUDA, "stage/KO kernels cannot be resident (occupancy 0)");
-  const int sms = num_sms(s->env->device);
-  const coffee_params& p = s->env->p;
-  int box[3];
-  for (int a = 0; a < 3; ++a) box[a] = p.N[a] + 2 * p.shift_ghost;
-  const int sx = (box[0] + S::STX - 1) / S::STX, sy = (box[1] + S::STY - 1) / S::STY;
-  s->kchunk_stage = pick_kchunk(box[2], sx * sy, sms * per_sm_stage, 4);
-  s->grid_stage = dim3(sx, sy, (box[2] + s->kchunk_stage - 1) / s->kchunk_stage);
-  const int kx = (box[0] + S::KTX - 1) / S::KTX, ky = (box[1] + S::KTY - 1) / S::KTY;
-  s->kchunk_ko = pick_kchunk(box[2], kx * ky, sms * per_sm_ko, 6);
-  s->grid_ko = dim3(kx, ky, (box[2] + s->kchunk_ko - 1) / s->kchunk_ko);
-  return COFFEE_OK;
+  return flat_plan<T>(s->env, s->semantics, &s->launch);
 }
 
 extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int variant,
@@ -757,9 +587,27 @@ static int next_event_pair(coffee_solver* s, int kind, cudaEvent_t* a, cudaEvent
   return COFFEE_OK;
 }
 
+// Timing mode: a pair of events around every launch.
+struct EventHook : LaunchHook {
+  coffee_solver* s;
+  cudaEvent_t pending = nullptr;
+  explicit EventHook(coffee_solver* sv) : s(sv) {}
+  int before(int kind) override {
+    cudaEvent_t a, b;
+    int rc = next_event_pair(s, kind, &a, &b);
+    if (rc) return rc;
+    pending = b;
+    COFFEE_CUDA_TRY(cudaEventRecord(a, s->stream));
+    return COFFEE_OK;
+  }
+  int after(int) override {
+    COFFEE_CUDA_TRY(cudaEventRecord(pending, s->stream));
+    return COFFEE_OK;
+  }
+};
+
 template <typename T>
 static int run_steps(coffee_solver* s, double time, int nsteps) {
-  using S = Shape<T>;
   EzConst<T> c;
   build_const<T>(s->env, s->semantics, &c);
   coffee_fields* f = s->f;
@@ -772,58 +620,14 @@ static int run_steps(coffee_solver* s, double time, int nsteps) {
       COFFEE_CUDA_TRY(cudaMemcpyAsync(s->B[a], f->d[a], bytes, cudaMemcpyDeviceToDevice, st));
     s->synced_generation = f->generation;
   }
-  F7<T> A = f7<T>(f->d), Bb = f7<T>(s->B), dU = f7<T>(s->dU), Un = f7<T>(s->Un);
   F5<T> aux;
   for (int a = 0; a < 5; ++a) aux.p[a] = static_cast<T*>(f->d[COFFEE_JX + a]);
-  const T dt = c.dt;
-  T t = (T)time;
-  const dim3 bs(S::STX, S::STY), bk(S::KTX, S::KTY);
   s->events_used = 0;
+  EventHook hook(s);
   if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(s->ev_begin, st));
-  for (int step = 0; step < nsteps; ++step) {
-    for (int i = 0; i < 5; ++i) {
-      const F7<T>& src = (i % 2 == 0) ? A : Bb;
-      const F7<T>& dst = (i % 2 == 0) ? Bb : A;
-      F7<const T> srcc;
-      for (int a = 0; a < 7; ++a) srcc.p[a] = src.p[a];
-      int flags = 0;
-      if (i == 4) flags |= ST_LAST;
-      if (i == 4 && s->aux) flags |= ST_AUX;
-      if (i == 0 && s->absorbing) flags |= ST_WRITE_UN;
-      const T tst = t + (T)kCs[i] * dt;
-      cudaEvent_t e0 = nullptr, e1 = nullptr;
-      if (s->timing) {
-        int rc = next_event_pair(s, i == 0 ? COFFEE_KERNEL_STAGE_FIRST : COFFEE_KERNEL_STAGE,
-                                 &e0, &e1);
-        if (rc) return rc;
-        COFFEE_CUDA_TRY(cudaEventRecord(e0, st));
-      }
-      const T As = (T)kAs[i], Bs = (T)kBs[i];
-      if (i == 0)
-        ez_stage_kernel<T, S::STX, S::STY, S::SPF, true>
-            <<<s->grid_stage, bs, stage_smem<T>(true), st>>>(c, srcc, dst, dU, Un, aux, As, Bs,
-                                                             tst, s->kchunk_stage, flags);
-      else
-        ez_stage_kernel<T, S::STX, S::STY, S::SPF, false>
-            <<<s->grid_stage, bs, stage_smem<T>(false), st>>>(c, srcc, dst, dU, Un, aux, As,
-                                                              Bs, tst, s->kchunk_stage, flags);
-      COFFEE_CUDA_TRY(cudaGetLastError());
-      if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(e1, st));
-    }
-    F7<const T> srcc;
-    for (int a = 0; a < 7; ++a) srcc.p[a] = Bb.p[a];
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (s->timing) {
-      int rc = next_event_pair(s, COFFEE_KERNEL_KO, &e0, &e1);
-      if (rc) return rc;
-      COFFEE_CUDA_TRY(cudaEventRecord(e0, st));
-    }
-    ez_ko_kernel<T, S::KTX, S::KTY, S::KPF>
-        <<<s->grid_ko, bk, ko_smem<T>(), st>>>(c, srcc, A, t + dt, s->kchunk_ko);
-    COFFEE_CUDA_TRY(cudaGetLastError());
-    if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(e1, st));
-    t = t + dt;
-  }
+  int rc = flat_steps<T>(c, s->launch, f7<T>(f->d), f7<T>(s->B), f7<T>(s->dU), f7<T>(s->Un), aux,
+                         s->aux != 0, time, nsteps, st, s->timing ? &hook : nullptr);
+  if (rc) return rc;
   if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(s->ev_end, st));
   return COFFEE_OK;
 }

@@ -27,9 +27,14 @@ enum StageFlags { ST_LAST = 1, ST_AUX = 2, ST_WRITE_UN = 4 };
 
 // Minimum resident CTAs for __launch_bounds__: two 256-thread CTAs (or the
 // equivalent) per SM in FP32, which caps registers at 128 per thread.
+#ifndef COFFEE_F32_THREADS_PER_SM
+#define COFFEE_F32_THREADS_PER_SM 512
+#endif
 template <typename T, int NT>
 constexpr int min_blocks() {
-  return (sizeof(T) == 4) ? ((512 / NT) > 0 ? 512 / NT : 1) : 1;
+  return (sizeof(T) == 4)
+             ? ((COFFEE_F32_THREADS_PER_SM / NT) > 0 ? COFFEE_F32_THREADS_PER_SM / NT : 1)
+             : 1;
 }
 
 // 4th-order first derivative (reference diff1_4, finite_diff.h:13-18):
@@ -84,9 +89,16 @@ __device__ __forceinline__ void store_with_images(const GridGeom& g, const Colum
 // (ST_LAST) and the stores of dU, J/divE/divB (ST_AUX), Un (ST_WRITE_UN) and
 // of U' with its guard images.  d{x,y,z}[f] are the inv_delta-scaled
 // 4th-order derivatives of field f at the point, u[f] its values.
-template <typename T, bool FIRST>
-__device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7], const T dx[7],
-                                            const T dy[7], const T dz[7], const T dold[7],
+// Curl, divergence and gradient of the fields at one point, as the stage
+// needs them (all inv_delta-scaled 4th-order differences).
+template <typename T>
+struct Derivs {
+  T rotE[3], rotB[3], divE, divB, gradP[3];
+};
+
+template <typename T, bool FIRST, bool BC>
+__device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7],
+                                            const Derivs<T>& dv, const T dold[7],
                                             const T As, const T Bs, const T tst,
                                             const int flags, const ColumnCtx<T>& col,
                                             const int k, const long long o, const F7<T>& du,
@@ -94,10 +106,10 @@ __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7], c
                                             const F7<T>& uout) {
   const bool cpu = c.semantics == SEM_CPU_REF;
   const T ex = u[0], ey = u[1], ez = u[2], bx = u[3], by = u[4], bz = u[5], P = u[6];
-  const T rotBx = dy[5] - dz[4], rotBy = dz[3] - dx[5], rotBz = dx[4] - dy[3];
-  const T rotEx = dy[2] - dz[1], rotEy = dz[0] - dx[2], rotEz = dx[1] - dy[0];
-  const T divE = dx[0] + dy[1] + dz[2];
-  const T divB = dx[3] + dy[4] + dz[5];
+  const T rotBx = dv.rotB[0], rotBy = dv.rotB[1], rotBz = dv.rotB[2];
+  const T rotEx = dv.rotE[0], rotEy = dv.rotE[1], rotEz = dv.rotE[2];
+  const T divE = dv.divE;
+  const T divB = dv.divB;
   T B2 = bx * bx + by * by + bz * bz;
   if (B2 < Tiny<T>::v) B2 = Tiny<T>::v;
   const T BrotB = bx * rotBx + by * rotBy + bz * rotBz;
@@ -124,9 +136,9 @@ __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7], c
   }
   T Px = 0, Py = 0, Pz = 0;
   if (c.divB_clean) {
-    Px = dx[6];
-    Py = dy[6];
-    Pz = dz[6];
+    Px = dv.gradP[0];
+    Py = dv.gradP[1];
+    Pz = dv.gradP[2];
     if (cpu) {
       const T s = p_taper(c, col, k);
       Px *= s;
@@ -149,8 +161,9 @@ __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7], c
     for (int f = 0; f < 7; ++f) d[f] = fma(dold[f], As, d[f]);
   }
   // the start-of-step copy is only read inside the absorbing layer
-  const T sig = c.absorbing ? absorbing_sigma(c, col.i, col.j, k) : (T)0;
-  if ((flags & ST_WRITE_UN) != 0 && sig > (T)0) {
+  T sig = (T)0;
+  if constexpr (BC) sig = c.absorbing ? absorbing_sigma(c, col.i, col.j, k) : (T)0;
+  if (BC && (flags & ST_WRITE_UN) != 0 && sig > (T)0) {
 #pragma unroll
     for (int f = 0; f < 7; ++f) un.p[f][o] = u[f];
   }
@@ -167,8 +180,8 @@ __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7], c
 #pragma unroll
   for (int f = 0; f < 7; ++f) nu[f] = fma(d[f], Bs, u[f]);
   apply_clamps(c, nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
-  star_boundary(c, col.i, col.j, k, tst, nu);
-  if ((flags & ST_LAST) != 0 && sig > (T)0) {
+  if constexpr (BC) star_boundary(c, col.i, col.j, k, tst, nu);
+  if (BC && (flags & ST_LAST) != 0 && sig > (T)0) {
     V7<T> uv, unv;
 #pragma unroll
     for (int f = 0; f < 7; ++f) {
@@ -223,7 +236,9 @@ struct TileLoader {
 // ---------------------------------------------------------------------------
 // One LSRK stage (reference rk_step + clamps + star boundary + absorbing
 // layer + send_guard_cells, src/algorithms/field_solver_EZ.cpp:1024-1055,
-// .cu:669-694):
+// .cu:669-694).  BC = false compiles the kernel without the star and
+// absorbing-layer code, for runs that have neither (their out-of-line calls
+// cost registers even when not taken):
 //   dU  <- As dU + dt RHS(U)        (FIRST: As = 0, so dU is not read)
 //   U'  <- U + Bs dU
 //   U'  <- clamps, star boundary at tst, absorbing layer (ST_LAST)
@@ -237,7 +252,7 @@ constexpr size_t stage_smem_bytes(bool first) {
          (first ? 0 : (size_t)(PF + 1) * 7 * TX * TY * sizeof(T));
 }
 
-template <typename T, int TX, int TY, int PF, bool FIRST>
+template <typename T, int TX, int TY, int PF, bool FIRST, bool BC>
 __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     ez_stage_kernel(const __grid_constant__ EzConst<T> c, const F7<const T> uin,
                     const F7<T> uout, const F7<T> du, const F7<T> un, const F5<T> aux,
@@ -300,18 +315,45 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
       const uint32_t am1 = corner + (uint32_t)(((k - 1) % R) * SB);
       const uint32_t ap1 = corner + (uint32_t)(((k + 1) % R) * SB);
       const uint32_t ap2 = corner + (uint32_t)(((k + 2) % R) * SB);
-      T u[7], dx[7], dy[7], dz[7], dold[7];
-      static_for<7>([&](auto fc) {
+      // The stencil is consumed field group by field group (B, then E, then
+      // P); the warp-level fence between groups keeps the shared loads of the
+      // next group from being hoisted, which bounds the live registers.
+      T u[7], dold[7];
+      Derivs<T> dv;
+      auto d1 = [&](auto fc, T* dxyz) {
         constexpr int f = decltype(fc)::value;
         constexpr int o = f * FB;
         u[f] = lds<T, o + CEN>(a0);
-        dx[f] = d1_4(lds<T, o + CEN - 2 * ES>(a0), lds<T, o + CEN - ES>(a0),
-                     lds<T, o + CEN + ES>(a0), lds<T, o + CEN + 2 * ES>(a0), six);
-        dy[f] = d1_4(lds<T, o + 2 * ES>(a0), lds<T, o + (SX + 2) * ES>(a0),
-                     lds<T, o + (3 * SX + 2) * ES>(a0), lds<T, o + (4 * SX + 2) * ES>(a0), siy);
-        dz[f] = d1_4(lds<T, o + CEN>(am2), lds<T, o + CEN>(am1), lds<T, o + CEN>(ap1),
-                     lds<T, o + CEN>(ap2), siz);
-      });
+        dxyz[0] = d1_4(lds<T, o + CEN - 2 * ES>(a0), lds<T, o + CEN - ES>(a0),
+                       lds<T, o + CEN + ES>(a0), lds<T, o + CEN + 2 * ES>(a0), six);
+        dxyz[1] = d1_4(lds<T, o + 2 * ES>(a0), lds<T, o + (SX + 2) * ES>(a0),
+                       lds<T, o + (3 * SX + 2) * ES>(a0), lds<T, o + (4 * SX + 2) * ES>(a0), siy);
+        dxyz[2] = d1_4(lds<T, o + CEN>(am2), lds<T, o + CEN>(am1), lds<T, o + CEN>(ap1),
+                       lds<T, o + CEN>(ap2), siz);
+      };
+      {
+        T bxd[3], byd[3], bzd[3];
+        d1(std::integral_constant<int, 3>{}, bxd);
+        d1(std::integral_constant<int, 4>{}, byd);
+        d1(std::integral_constant<int, 5>{}, bzd);
+        dv.rotB[0] = bzd[1] - byd[2];
+        dv.rotB[1] = bxd[2] - bzd[0];
+        dv.rotB[2] = byd[0] - bxd[1];
+        dv.divB = bxd[0] + byd[1] + bzd[2];
+      }
+      __syncwarp();
+      {
+        T exd[3], eyd[3], ezd[3];
+        d1(std::integral_constant<int, 0>{}, exd);
+        d1(std::integral_constant<int, 1>{}, eyd);
+        d1(std::integral_constant<int, 2>{}, ezd);
+        dv.rotE[0] = ezd[1] - eyd[2];
+        dv.rotE[1] = exd[2] - ezd[0];
+        dv.rotE[2] = eyd[0] - exd[1];
+        dv.divE = exd[0] + eyd[1] + ezd[2];
+      }
+      __syncwarp();
+      d1(std::integral_constant<int, 6>{}, dv.gradP);
       if constexpr (!FIRST) {
         const uint32_t ad = dme + (uint32_t)((k % (PF + 1)) * DSB);
         static_for<7>([&](auto fc) {
@@ -319,7 +361,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
           dold[f] = lds<T, f * DFB>(ad);
         });
       }
-      stage_point<T, FIRST>(c, u, dx, dy, dz, dold, As, Bs, tst, flags, col, k,
+      stage_point<T, FIRST, BC>(c, u, dv, dold, As, Bs, tst, flags, col, k,
                             (long long)k * g.sz + own, du, un, aux, uout);
     }
     __syncthreads();
@@ -343,7 +385,7 @@ constexpr size_t ko_smem_bytes() {
   return (size_t)(4 + PF) * 7 * (TX + 6) * (TY + 6) * sizeof(T);
 }
 
-template <typename T, int TX, int TY, int PF>
+template <typename T, int TX, int TY, int PF, bool BC>
 __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     ez_ko_kernel(const __grid_constant__ EzConst<T> c, const F7<const T> uin,
                  const F7<T> uout, const T tko, const int kchunk) {
@@ -413,7 +455,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
         }
       });
       apply_clamps(c, nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
-      star_boundary(c, i, j, k, tko, nu);
+      if constexpr (BC) star_boundary(c, i, j, k, tko, nu);
       store_with_images(g, col, uout, k, (long long)k * g.sz + own, nu);
 #pragma unroll
       for (int q = 0; q < 6; ++q)
