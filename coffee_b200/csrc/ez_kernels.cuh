@@ -274,6 +274,10 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
   const int k0 = g.lo[2] + blockIdx.z * kchunk;
   const int k1 = min(k0 + kchunk, g.hi[2]);
   const bool active = (i < g.hi[0]) && (j < g.hi[1]);
+  // lanes of this warp that compute points: the fences between the field
+  // groups below are executed by these lanes only (a tile that overhangs
+  // the grid has idle lanes, which must not be named in the mask)
+  const unsigned amask = __ballot_sync(0xffffffffu, active);
   const long long own = (long long)j * g.sy + i;
   const ColumnCtx<T> col = make_column(c, i, j);
   const L loader(g, sbase, tid, g.lo[0] + (int)blockIdx.x * TX - 2,
@@ -341,7 +345,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
         dv.rotB[2] = byd[0] - bxd[1];
         dv.divB = bxd[0] + byd[1] + bzd[2];
       }
-      __syncwarp();
+      __syncwarp(amask);
       {
         T exd[3], eyd[3], ezd[3];
         d1(std::integral_constant<int, 0>{}, exd);
@@ -352,7 +356,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
         dv.rotE[2] = eyd[0] - exd[1];
         dv.divE = exd[0] + eyd[1] + ezd[2];
       }
-      __syncwarp();
+      __syncwarp(amask);
       d1(std::integral_constant<int, 6>{}, dv.gradP);
       if constexpr (!FIRST) {
         const uint32_t ad = dme + (uint32_t)((k % (PF + 1)) * DSB);
