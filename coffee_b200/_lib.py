@@ -21,6 +21,9 @@ ERRORS = {
 FIELD_IDS = {"Ex": 0, "Ey": 1, "Ez": 2, "Bx": 3, "By": 4, "Bz": 5, "P": 6,
              "Jx": 7, "Jy": 8, "Jz": 9, "divE": 10, "divB": 11}
 VARIANT_FLAT = 0
+VARIANT_LOGSPH = 1
+VARIANT_CYL = 2
+VARIANT_GR = 3
 KERNEL_STAGE_FIRST, KERNEL_STAGE, KERNEL_KO = 0, 1, 2
 SEM_CPU_REF = 0
 SEM_GPU_REF = 1
@@ -100,6 +103,9 @@ SIGNATURES = {
     "coffee_solver_check_finite": (_i, [_vp]),
     "coffee_solver_save_snapshot": (_i, [_vp, ctypes.c_char_p, _d, ctypes.c_int64]),
     "coffee_solver_load_snapshot": (_i, [_vp, ctypes.c_char_p, _P(_d), _P(ctypes.c_int64)]),
+    "coffee_batch_create": (_i, [_P(_vp), _i, _vp, _P(_vp)]),
+    "coffee_batch_step": (_i, [_vp, _P(_d), _i]),
+    "coffee_batch_destroy": (_i, [_vp]),
 }
 
 _lib = None

@@ -15,6 +15,7 @@
 #include "coffee_fld.h"
 #include "coffee_internal.h"
 #include "ez_launch.cuh"
+#include "variants.h"
 
 #define COFFEE_VERSION_STRING "coffee_b200 0.1 (sm_100a)"
 
@@ -64,6 +65,7 @@ struct coffee_solver {
   int timing;
   uint64_t synced_generation;
   FlatLaunch launch;
+  void* vtab;  // tables / scratch of a non-Cartesian variant (device), or null
   std::vector<cudaEvent_t> events;   // pairs around each launch (timing mode)
   std::vector<int> event_kind;       // COFFEE_KERNEL_* of each pair
   int events_used;
@@ -200,7 +202,9 @@ extern "C" int coffee_env_create(const coffee_params* p, int device, coffee_env*
   *out = nullptr;
   for (int a = 0; a < 3; ++a) {
     if (p->N[a] < 1) return fail(COFFEE_E_CONFIG, "N[%d] = %d must be >= 1", a, p->N[a]);
-    if (p->guard[a] < p->shift_ghost + 3)
+    // an axis of one point without guards is the third axis of a 2D run
+    const bool plane_axis = p->N[a] == 1 && p->guard[a] == 0;
+    if (!plane_axis && p->guard[a] < p->shift_ghost + 3)
       return fail(COFFEE_E_CONFIG,
                   "guard[%d] = %d: the KO stencil needs guard >= shift_ghost + 3 = %d", a,
                   p->guard[a], p->shift_ghost + 3);
@@ -471,13 +475,24 @@ extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int varia
   if (!env || !f || !out) return fail(COFFEE_E_INVALID, "coffee_solver_create: null argument");
   *out = nullptr;
   if (f->env != env) return fail(COFFEE_E_INVALID, "fields belong to another environment");
-  if (variant != COFFEE_VARIANT_FLAT)
+  if (variant != COFFEE_VARIANT_FLAT && variant != COFFEE_VARIANT_LOGSPH &&
+      variant != COFFEE_VARIANT_CYL && variant != COFFEE_VARIANT_GR)
     return fail(COFFEE_E_INVALID, "solver variant %d is not available", variant);
   if (semantics != COFFEE_SEM_CPU_REF && semantics != COFFEE_SEM_GPU_REF)
     return fail(COFFEE_E_INVALID, "unknown semantics %d", semantics);
-  if (env->p.problem < 0 || env->p.problem > 2)
-    return fail(COFFEE_E_CONFIG, "problem %d is not supported by the flat EZ solver",
-                env->p.problem);
+  if (variant == COFFEE_VARIANT_FLAT) {
+    if (env->p.problem < 0 || env->p.problem > 2)
+      return fail(COFFEE_E_CONFIG, "problem %d is not supported by the flat EZ solver",
+                  env->p.problem);
+    for (int a = 0; a < 3; ++a)
+      if (env->p.guard[a] < env->p.shift_ghost + 3)
+        return fail(COFFEE_E_CONFIG, "the flat EZ solver needs guard[%d] >= shift_ghost + 3",
+                    a);
+  } else {
+    // the reference has these solvers only in its GPU build
+    int rc = variant == COFFEE_VARIANT_GR ? gr_check(env) : axisym_check(env, variant);
+    if (rc) return rc;
+  }
   COFFEE_CUDA_TRY(cudaSetDevice(env->device));
   coffee_solver* s = new (std::nothrow) coffee_solver();
   if (!s) return fail(COFFEE_E_NOMEM, "out of host memory");
@@ -490,16 +505,19 @@ extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int varia
   s->timing = 0;
   s->events_used = 0;
   s->synced_generation = 0;
-  bool abs_any = env->p.shift_ghost > 0;
+  // the GR solver's inner absorbing region always needs the start-of-step copy
+  bool abs_any = env->p.shift_ghost > 0 || variant == COFFEE_VARIANT_GR;
   for (int a = 0; a < 3; ++a) abs_any = abs_any || env->p.pml[a] > 0;
   s->absorbing = abs_any;
   const size_t bytes = f->n * f->elem;
+  s->vtab = nullptr;
   auto cleanup = [&]() {
     for (int a = 0; a < 7; ++a) {
       if (s->B[a]) cudaFree(s->B[a]);
       if (s->dU[a]) cudaFree(s->dU[a]);
       if (s->Un[a]) cudaFree(s->Un[a]);
     }
+    if (s->vtab) cudaFree(s->vtab);
     delete s;
   };
   for (int a = 0; a < 7; ++a) {
@@ -513,7 +531,10 @@ extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int varia
       return fail(COFFEE_E_NOMEM, "solver scratch allocation failed: %s", cudaGetErrorString(err));
     }
   }
-  int rc = (f->elem == 4) ? configure_solver<float>(s) : configure_solver<double>(s);
+  int rc = variant == COFFEE_VARIANT_GR     ? gr_setup(env, f->elem, &s->vtab)
+           : variant != COFFEE_VARIANT_FLAT ? axisym_setup(env, variant, f->elem, &s->vtab)
+           : (f->elem == 4)               ? configure_solver<float>(s)
+                                          : configure_solver<double>(s);
   if (rc) {
     cleanup();
     return rc;
@@ -540,6 +561,7 @@ extern "C" int coffee_solver_destroy(coffee_solver* s) {
     if (s->dU[a]) cudaFree(s->dU[a]);
     if (s->Un[a]) cudaFree(s->Un[a]);
   }
+  if (s->vtab) cudaFree(s->vtab);
   for (auto e : s->events) cudaEventDestroy(e);
   cudaEventDestroy(s->ev_begin);
   cudaEventDestroy(s->ev_end);
@@ -568,7 +590,8 @@ extern "C" int coffee_solver_set_timing(coffee_solver* s, int enable) {
 }
 
 extern "C" int coffee_solver_launches_per_step(coffee_solver* s) {
-  (void)s;
+  if (s && s->variant == COFFEE_VARIANT_LOGSPH) return 12;  // + axis after each, + 1 per call
+  if (s && s->variant == COFFEE_VARIANT_GR) return 11;      // + an E, H pass before each stage
   return 6;  // 5 stage kernels + 1 KO kernel
 }
 
@@ -625,6 +648,19 @@ static int run_steps(coffee_solver* s, double time, int nsteps) {
   s->events_used = 0;
   EventHook hook(s);
   if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(s->ev_begin, st));
+  if (s->variant != COFFEE_VARIANT_FLAT) {
+    void* auxp[5];
+    for (int a = 0; a < 5; ++a) auxp[a] = f->d[COFFEE_JX + a];
+    LaunchHook* h = s->timing ? &hook : nullptr;
+    int rc = s->variant == COFFEE_VARIANT_GR
+                 ? gr_steps(s->env, f->elem, s->vtab, f->d, s->B, s->dU, s->Un,
+                            s->aux ? auxp : nullptr, nsteps, st, h)
+                 : axisym_steps(s->env, s->variant, f->elem, s->vtab, f->d, s->B, s->dU, s->Un,
+                                s->aux ? auxp : nullptr, time, nsteps, st, h);
+    if (rc) return rc;
+    if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(s->ev_end, st));
+    return COFFEE_OK;
+  }
   int rc = flat_steps<T>(c, s->launch, f7<T>(f->d), f7<T>(s->B), f7<T>(s->dU), f7<T>(s->Un), aux,
                          s->aux != 0, time, nsteps, st, s->timing ? &hook : nullptr);
   if (rc) return rc;
@@ -638,6 +674,92 @@ extern "C" int coffee_solver_step(coffee_solver* s, double time, int nsteps) {
   if (nsteps < 0) return fail(COFFEE_E_INVALID, "nsteps must be >= 0");
   COFFEE_CUDA_TRY(cudaSetDevice(s->env->device));
   return (s->f->elem == 4) ? run_steps<float>(s, time, nsteps) : run_steps<double>(s, time, nsteps);
+}
+
+// ------------------------------------------------------------------ batch
+
+struct coffee_batch {
+  std::vector<coffee_solver*> solvers;
+  std::vector<SphRun> runs;
+  void* table;
+  int nblocks, naxis;
+  int elem;
+  int device;
+  cudaStream_t stream;
+};
+
+extern "C" int coffee_batch_create(coffee_solver* const* solvers, int n, void* stream,
+                                   coffee_batch** out) {
+  clear_error();
+  if (!solvers || !out) return fail(COFFEE_E_INVALID, "coffee_batch_create: null argument");
+  *out = nullptr;
+  if (n < 1 || n > kMaxBatch)
+    return fail(COFFEE_E_INVALID, "a batch holds 1 to %d runs (got %d)", kMaxBatch, n);
+  for (int m = 0; m < n; ++m) {
+    const coffee_solver* s = solvers[m];
+    if (!s) return fail(COFFEE_E_INVALID, "solver %d is null", m);
+    if (s->variant != COFFEE_VARIANT_LOGSPH)
+      return fail(COFFEE_E_INVALID, "solver %d is not a log-spherical solver", m);
+    if (s->f->elem != solvers[0]->f->elem || s->env->device != solvers[0]->env->device)
+      return fail(COFFEE_E_INVALID, "solver %d differs in precision or device from solver 0", m);
+  }
+  COFFEE_CUDA_TRY(cudaSetDevice(solvers[0]->env->device));
+  coffee_batch* b = new (std::nothrow) coffee_batch();
+  if (!b) return fail(COFFEE_E_NOMEM, "out of host memory");
+  b->solvers.assign(solvers, solvers + n);
+  b->runs.resize(n);
+  b->elem = solvers[0]->f->elem;
+  b->device = solvers[0]->env->device;
+  b->stream = static_cast<cudaStream_t>(stream);
+  for (int m = 0; m < n; ++m) {
+    coffee_solver* s = solvers[m];
+    SphRun& r = b->runs[m];
+    r.env = s->env;
+    r.tab = s->vtab;
+    for (int k = 0; k < 7; ++k) {
+      r.A[k] = s->f->d[k];
+      r.B[k] = s->B[k];
+      r.dU[k] = s->dU[k];
+      r.Un[k] = s->Un[k];
+    }
+    for (int k = 0; k < 5; ++k) r.aux[k] = s->f->d[COFFEE_JX + k];
+    r.want_aux = s->aux;
+  }
+  int rc = sph_batch_create(b->runs.data(), n, b->elem, &b->table, &b->nblocks, &b->naxis);
+  if (rc) {
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_batch_step(coffee_batch* b, double* times, int nsteps) {
+  clear_error();
+  if (!b || !times) return fail(COFFEE_E_INVALID, "coffee_batch_step: null argument");
+  if (nsteps < 0) return fail(COFFEE_E_INVALID, "nsteps must be >= 0");
+  COFFEE_CUDA_TRY(cudaSetDevice(b->device));
+  for (coffee_solver* s : b->solvers) {
+    coffee_fields* f = s->f;
+    if (s->synced_generation != f->generation) {
+      // the second buffer carries the same guard values
+      for (int a = 0; a < 7; ++a)
+        COFFEE_CUDA_TRY(cudaMemcpyAsync(s->B[a], f->d[a], f->n * f->elem,
+                                        cudaMemcpyDeviceToDevice, b->stream));
+      s->synced_generation = f->generation;
+    }
+  }
+  return sph_batch_steps(b->table, (int)b->runs.size(), b->elem, b->runs.data(), times, nsteps,
+                         b->nblocks, b->naxis, b->stream);
+}
+
+extern "C" int coffee_batch_destroy(coffee_batch* b) {
+  if (!b) return COFFEE_OK;
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->stream);
+  cudaFree(b->table);
+  delete b;
+  return COFFEE_OK;
 }
 
 extern "C" int coffee_solver_last_timing(coffee_solver* s, double ms[3], int launches[3],

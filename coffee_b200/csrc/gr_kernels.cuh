@@ -1,0 +1,356 @@
+// Kernels of the GR force-free solver in Cartesian Kerr-Schild coordinates
+// (reference src/algorithms/field_solver_gr_EZ.cu, metric
+// src/algorithms/metric_cks_impl.hpp).
+//
+// sim_data's E holds the densitised displacement D; the curl acts on the
+// constitutive fields E = alpha D_i + sqrt(gamma) (beta x B)_i and
+// H = alpha B_i - sqrt(gamma) (beta x D)_i.  A stage is two launches: one
+// writes E and H over the whole grid (the reference's get_Ed / get_Hd), the
+// other does the LSRK update, the clamps and, in the last stage, both
+// absorbing layers in one pass over the update box, reading the current
+// buffer and writing the other one.  The metric is evaluated analytically
+// per point in field precision, as the reference does; unlike the
+// reference, each point evaluates it once per launch (the reference calls
+// get_r inside every metric component, about forty times per point).
+#pragma once
+
+#include "axisym_kernels.cuh"
+#include "ez_common.cuh"
+
+namespace coffee {
+
+template <typename T>
+struct GrConst {
+  int d[3];                 // dims
+  int lo[3], hi[3];         // update box
+  int g[3];                 // guards
+  T lower[3], delta[3], inv_delta[3];
+  T a, dt, tau, ko_c;
+  int calc_current, divB_clean, clean_ep, check_egb;
+  int absorbing;
+  T xl[3], xh[3];           // outer layer edges (boundary.cu:43-54)
+  T pmlscale, sigpml;
+  T r1, r2, dd;             // inner layer: 0.7 r_H, 0.01 r_H, 0.2 r_H (:617-621)
+};
+
+// r of the Kerr-Schild coordinates (metric_cks_impl.hpp:17-24)
+template <typename T>
+__device__ __forceinline__ T cks_r(T a, T x, T y, T z) {
+  const T R2 = x * x + y * y + z * z;
+  const T q = R2 - a * a;
+  T s = q * q + T(4) * (a * z) * (a * z);
+  if (s < Tiny<T>::v) s = Tiny<T>::v;
+  return sqrt((q + sqrt(s)) * T(0.5));
+}
+
+// sqrt(gamma) = sqrt(1 + 2 r^3 / (r^4 + a^2 z^2)) (:77-83)
+template <typename T>
+__device__ __forceinline__ T cks_sqrt_gamma(T a, T x, T y, T z) {
+  const T r = cks_r(a, x, y, z);
+  T den = r * r * r * r + a * a * z * z;
+  if (den < Tiny<T>::v) den = Tiny<T>::v;
+  return sqrt(T(1) + T(2) * r * r * r / den);
+}
+
+// All metric functions at one point (metric_cks_impl.hpp:13-181).
+template <typename T>
+struct Cks {
+  T r, alpha, sg;
+  T bu[3];
+  T gd11, gd12, gd13, gd22, gd23, gd33;
+  T gu11, gu12, gu13, gu22, gu23, gu33;
+
+  __device__ __forceinline__ Cks(T a, T x, T y, T z) {
+    r = cks_r(a, x, y, z);
+    const T r2 = r * r, r3 = r2 * r, r4 = r2 * r2;
+    const T aa = a * a, azz = aa * z * z;
+    T den = r4 + azz;
+    if (den < Tiny<T>::v) den = Tiny<T>::v;
+    T denu = T(2) * r3 + r4 + azz;
+    if (denu < Tiny<T>::v) denu = Tiny<T>::v;
+    T ar = aa + r2;
+    T ar2 = ar * ar;
+    if (ar < Tiny<T>::v) ar = Tiny<T>::v;
+    if (ar2 < Tiny<T>::v) ar2 = Tiny<T>::v;
+    const T lx = r * x + a * y, ly = -a * x + r * y;
+    const T iden = T(1) / den, idenu = T(1) / denu, iar = T(1) / ar, iar2 = T(1) / ar2;
+    const T gam = T(1) + T(2) * r3 * iden;
+    sg = sqrt(gam);
+    alpha = sqrt(T(1) / gam);
+    bu[0] = T(2) * r3 * lx * iar * idenu;
+    bu[1] = T(2) * r3 * ly * iar * idenu;
+    bu[2] = T(2) * r2 * z * idenu;
+    const T hd = T(2) * r3 * iar2 * iden, hu = T(2) * r3 * iar2 * idenu;
+    const T kd = T(2) * r2 * iar * iden, ku = T(2) * r2 * iar * idenu;
+    gd11 = T(1) + hd * lx * lx;
+    gd12 = hd * lx * ly;
+    gd13 = kd * lx * z;
+    gd22 = T(1) + hd * ly * ly;
+    gd23 = kd * ly * z;
+    gd33 = T(1) + T(2) * r * z * z * iden;
+    gu11 = T(1) - hu * lx * lx;
+    gu12 = -hu * lx * ly;
+    gu13 = -ku * lx * z;
+    gu22 = T(1) - hu * ly * ly;
+    gu23 = -ku * ly * z;
+    gu33 = T(1) - T(2) * r * z * z * idenu;
+  }
+  __device__ __forceinline__ void lower(const T* v, T* o) const {
+    o[0] = gd11 * v[0] + gd12 * v[1] + gd13 * v[2];
+    o[1] = gd12 * v[0] + gd22 * v[1] + gd23 * v[2];
+    o[2] = gd13 * v[0] + gd23 * v[1] + gd33 * v[2];
+  }
+  __device__ __forceinline__ void raise(const T* v, T* o) const {
+    o[0] = gu11 * v[0] + gu12 * v[1] + gu13 * v[2];
+    o[1] = gu12 * v[0] + gu22 * v[1] + gu23 * v[2];
+    o[2] = gu13 * v[0] + gu23 * v[1] + gu33 * v[2];
+  }
+};
+
+template <typename T>
+__device__ __forceinline__ T gr_pos(const GrConst<T>& c, int a, int n) {
+  return c.lower[a] + c.delta[a] * (T)(n - c.g[a]);
+}
+
+// E and H over the whole grid (kernel_compute_E_gr / kernel_compute_H_gr,
+// field_solver_gr_EZ.cu:88-186).  eh[0..2] = E, eh[3..5] = H.
+template <typename T>
+__global__ void __launch_bounds__(256) gr_eh_kernel(const __grid_constant__ GrConst<T> c,
+                                                    const F7<T> u, const F7<T> eh) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= c.d[0] || j >= c.d[1] || k >= c.d[2]) return;
+  const long long o = i + (long long)c.d[0] * (j + (long long)c.d[1] * k);
+  const Cks<T> m(c.a, gr_pos(c, 0, i), gr_pos(c, 1, j), gr_pos(c, 2, k));
+  const T D[3] = {__ldg(u.p[0] + o), __ldg(u.p[1] + o), __ldg(u.p[2] + o)};
+  const T B[3] = {__ldg(u.p[3] + o), __ldg(u.p[4] + o), __ldg(u.p[5] + o)};
+  T Dd[3], Bd[3];
+  m.lower(D, Dd);
+  m.lower(B, Bd);
+  eh.p[0][o] = m.alpha * Dd[0] + m.sg * (m.bu[1] * B[2] - m.bu[2] * B[1]);
+  eh.p[1][o] = m.alpha * Dd[1] + m.sg * (m.bu[2] * B[0] - m.bu[0] * B[2]);
+  eh.p[2][o] = m.alpha * Dd[2] + m.sg * (m.bu[0] * B[1] - m.bu[1] * B[0]);
+  eh.p[3][o] = m.alpha * Bd[0] - m.sg * (m.bu[1] * D[2] - m.bu[2] * D[1]);
+  eh.p[4][o] = m.alpha * Bd[1] - m.sg * (m.bu[2] * D[0] - m.bu[0] * D[2]);
+  eh.p[5][o] = m.alpha * Bd[2] - m.sg * (m.bu[0] * D[1] - m.bu[1] * D[0]);
+}
+
+// clean_epar / check_eGTb with the 3-metric (kernel_clean_epar_gr,
+// kernel_check_eGTb_gr, field_solver_gr_EZ.cu:422-521)
+template <typename T>
+__device__ __forceinline__ void gr_clamps(const GrConst<T>& c, const Cks<T>& m, T* v) {
+  if (c.clean_ep) {
+    T Bd[3];
+    m.lower(v + 3, Bd);
+    T B2 = v[3] * Bd[0] + v[4] * Bd[1] + v[5] * Bd[2];
+    if (B2 < Tiny<T>::v) B2 = Tiny<T>::v;
+    const T q = fdiv(v[0] * Bd[0] + v[1] * Bd[1] + v[2] * Bd[2], B2);
+    v[0] -= q * v[3];
+    v[1] -= q * v[4];
+    v[2] -= q * v[5];
+  }
+  if (c.check_egb) {
+    T Dd[3], Bd[3];
+    m.lower(v, Dd);
+    m.lower(v + 3, Bd);
+    T D2 = v[0] * Dd[0] + v[1] * Dd[1] + v[2] * Dd[2];
+    if (D2 < Tiny<T>::v) D2 = Tiny<T>::v;
+    const T B2 = v[3] * Bd[0] + v[4] * Bd[1] + v[5] * Bd[2];
+    if (D2 > B2) {
+      const T s = sqrt(fdiv(B2, D2));
+      v[0] *= s;
+      v[1] *= s;
+      v[2] *= s;
+    }
+  }
+}
+
+// Outer layer at the six faces (kernel_boundary_absorbing_thread,
+// src/algorithms/boundary.cu:17-79), then the inner layer inside 0.7 r_H and
+// the zeroed core inside 0.01 r_H (kernel_absorbing_inner,
+// field_solver_gr_EZ.cu:610-701); both blend towards the start-of-step
+// values n.
+template <typename T>
+__device__ __noinline__ V7<T> gr_absorb(const GrConst<T>& c, V7<T> v, V7<T> n, T x, T y, T z,
+                                        T r) {
+  const T pos[3] = {x, y, z};
+  bool outside = false;
+  T sig = T(0);
+  for (int a = 0; a < 3; ++a) {
+    outside = outside || pos[a] > c.xh[a] || pos[a] < c.xl[a];
+    sig += cyl_pmlsigma(pos[a], c.xl[a], c.xh[a], c.pmlscale, c.sigpml);
+  }
+  if (outside && sig > Tiny<T>::v) {
+    const T e = exp(-sig);
+    const T f = (T(1) - e) / sig;
+    for (int a = 0; a < 6; ++a) v.v[a] = e * n.v[a] + f * (v.v[a] - n.v[a]);
+  }
+  if (r < c.r1) {
+    const T q = (c.r1 - r) / c.dd;
+    const T s = c.sigpml * q * q * q * c.dt;
+    if (s > Tiny<T>::v) {
+      const T e = exp(-s);
+      const T f = (T(1) - e) / s;
+      for (int a = 0; a < 6; ++a) v.v[a] = e * n.v[a] + f * (v.v[a] - n.v[a]);
+    }
+  }
+  if (r < c.r2)
+    for (int a = 0; a < 6; ++a) v.v[a] = T(0);
+  return v;
+}
+
+// One LSRK stage of the GR solver (kernel_rk_step1_gr + kernel_rk_step2_gr,
+// field_solver_gr_EZ.cu:188-420, then the clamps and, in the last stage,
+// the absorbing layers: order of :876-893).  u: D, B, P of the current
+// buffer; eh: E, H of the same buffer.
+template <typename T, bool FIRST>
+__global__ void __launch_bounds__(256) gr_stage_kernel(const __grid_constant__ GrConst<T> c,
+                                                       const F7<T> u, const F7<T> eh,
+                                                       const F7<T> out, const F7<T> du,
+                                                       const F7<T> un, const F5<T> aux,
+                                                       const T As, const T Bs,
+                                                       const int flags) {
+  const int i = c.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = c.lo[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = c.lo[2] + blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= c.hi[0] || j >= c.hi[1] || k >= c.hi[2]) return;
+  const long long sx = 1, sy = c.d[0], sz = (long long)c.d[0] * c.d[1];
+  const long long o = i + sy * j + sz * k;
+  const long long st[3] = {sx, sy, sz};
+  const T x = gr_pos(c, 0, i), y = gr_pos(c, 1, j), z = gr_pos(c, 2, k);
+  const Cks<T> m(c.a, x, y, z);
+  const T igms = T(1) / m.sg;
+
+  auto d1 = [&](const T* f, int ax) {
+    const long long s = st[ax];
+    return d1_4w(__ldg(f + o - 2 * s), __ldg(f + o - s), __ldg(f + o + s), __ldg(f + o + 2 * s)) *
+           c.inv_delta[ax];
+  };
+  const T rotH[3] = {(d1(eh.p[5], 1) - d1(eh.p[4], 2)) * igms,
+                     (d1(eh.p[3], 2) - d1(eh.p[5], 0)) * igms,
+                     (d1(eh.p[4], 0) - d1(eh.p[3], 1)) * igms};
+  const T rotE[3] = {(d1(eh.p[2], 1) - d1(eh.p[1], 2)) * igms,
+                     (d1(eh.p[0], 2) - d1(eh.p[2], 0)) * igms,
+                     (d1(eh.p[1], 0) - d1(eh.p[0], 1)) * igms};
+  // div4 (:44-86): sqrt(gamma) at the coordinates shifted by +-1, 2 delta
+  T divD = T(0), divB = T(0);
+  {
+    const T pos[3] = {x, y, z};
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      T w[4];
+      const T off[4] = {T(-2), T(-1), T(1), T(2)};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        T p3[3] = {pos[0], pos[1], pos[2]};
+        p3[ax] = pos[ax] + off[q] * c.delta[ax];
+        w[q] = cks_sqrt_gamma(c.a, p3[0], p3[1], p3[2]);
+      }
+      const long long s = st[ax];
+      const T* fD = u.p[ax];
+      const T* fB = u.p[3 + ax];
+      divD += d1_4w(__ldg(fD + o - 2 * s) * w[0], __ldg(fD + o - s) * w[1],
+                    __ldg(fD + o + s) * w[2], __ldg(fD + o + 2 * s) * w[3]) * c.inv_delta[ax];
+      divB += d1_4w(__ldg(fB + o - 2 * s) * w[0], __ldg(fB + o - s) * w[1],
+                    __ldg(fB + o + s) * w[2], __ldg(fB + o + 2 * s) * w[3]) * c.inv_delta[ax];
+    }
+    divD *= igms;
+    divB *= igms;
+  }
+  T v[7];
+#pragma unroll
+  for (int a = 0; a < 7; ++a) v[a] = __ldg(u.p[a] + o);
+  T Bd[3], Dd[3];
+  m.lower(v + 3, Bd);
+  m.lower(v, Dd);
+  T J[3] = {T(0), T(0), T(0)};
+  if (c.calc_current) {
+    T B2 = v[3] * Bd[0] + v[4] * Bd[1] + v[5] * Bd[2];
+    if (B2 < Tiny<T>::v) B2 = Tiny<T>::v;
+    const T Jp = (Bd[0] * rotH[0] + Bd[1] * rotH[1] + Bd[2] * rotH[2]) -
+                 (Dd[0] * rotE[0] + Dd[1] * rotE[1] + Dd[2] * rotE[2]);
+    const T e0 = __ldg(eh.p[0] + o), e1 = __ldg(eh.p[1] + o), e2 = __ldg(eh.p[2] + o);
+    const T iB2 = fdiv(T(1), B2);
+    J[0] = (divD * (e1 * Bd[2] - e2 * Bd[1]) * igms + Jp * v[3]) * iB2;
+    J[1] = (divD * (e2 * Bd[0] - e0 * Bd[2]) * igms + Jp * v[4]) * iB2;
+    J[2] = (divD * (e0 * Bd[1] - e1 * Bd[0]) * igms + Jp * v[5]) * iB2;
+  }
+  const T Pd[3] = {d1(u.p[6], 0), d1(u.p[6], 1), d1(u.p[6], 2)};
+  T Pu[3];
+  m.raise(Pd, Pu);
+  const T shape = T(0.5) * (T(1) - tanh((m.r - T(5)) / T(1)));  // r0 = 5, del = 1 (:276-278)
+  const T dt = c.dt;
+  T rhs[7];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    rhs[a] = dt * (rotH[a] - J[a]);
+    rhs[3 + a] = c.divB_clean ? dt * (-rotE[a] + (-m.alpha * Pu[a] + m.bu[a] * divB) * shape)
+                              : -dt * rotE[a];
+  }
+  rhs[6] = dt * (-m.alpha * divB + m.bu[0] * Pd[0] + m.bu[1] * Pd[1] + m.bu[2] * Pd[2]) -
+           m.alpha * v[6] / c.tau;
+  if (flags & AX_WRITE_UN) {
+#pragma unroll
+    for (int a = 0; a < 6; ++a) un.p[a][o] = v[a];
+  }
+#pragma unroll
+  for (int a = 0; a < 7; ++a) {
+    const T dd = FIRST ? rhs[a] : As * du.p[a][o] + rhs[a];
+    du.p[a][o] = dd;
+    v[a] += Bs * dd;
+  }
+  if (flags & AX_AUX) {
+    aux.p[0][o] = J[0];
+    aux.p[1][o] = J[1];
+    aux.p[2][o] = J[2];
+    aux.p[3][o] = divD;
+    aux.p[4][o] = divB;
+  }
+  gr_clamps(c, m, v);
+  V7<T> w;
+#pragma unroll
+  for (int a = 0; a < 7; ++a) w.v[a] = v[a];
+  if ((flags & AX_LAST) && c.absorbing) {
+    V7<T> n;
+#pragma unroll
+    for (int a = 0; a < 6; ++a) n.v[a] = un.p[a][o];
+    n.v[6] = T(0);
+    w = gr_absorb(c, w, n, x, y, z, m.r);
+  }
+#pragma unroll
+  for (int a = 0; a < 7; ++a) out.p[a][o] = w.v[a];
+}
+
+// Kreiss-Oliger pass (kernel_KO_step1_gr / _step2_gr, :523-608, with the
+// 3D 6th difference of finite_diff.h:84-92), then the clamps (:895-900).
+template <typename T>
+__global__ void __launch_bounds__(256) gr_ko_kernel(const __grid_constant__ GrConst<T> c,
+                                                    const F7<T> u, const F7<T> out) {
+  const int i = c.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = c.lo[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = c.lo[2] + blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= c.hi[0] || j >= c.hi[1] || k >= c.hi[2]) return;
+  const long long sy = c.d[0], sz = (long long)c.d[0] * c.d[1];
+  const long long o = i + sy * j + sz * k;
+  constexpr T K6[7] = {T(1), T(-6), T(15), T(-20), T(15), T(-6), T(1)};
+  T v[7];
+#pragma unroll
+  for (int a = 0; a < 7; ++a) {
+    const T* f = u.p[a];
+    T tx = T(0), ty = T(0), tz = T(0);
+#pragma unroll
+    for (int q = 0; q < 7; ++q) {
+      tx += K6[q] * __ldg(f + o + (q - 3));
+      ty += K6[q] * __ldg(f + o + (q - 3) * sy);
+      tz += K6[q] * __ldg(f + o + (q - 3) * sz);
+    }
+    v[a] = __ldg(f + o) + c.ko_c * (tx + ty + tz);
+  }
+  const Cks<T> m(c.a, gr_pos(c, 0, i), gr_pos(c, 1, j), gr_pos(c, 2, k));
+  gr_clamps(c, m, v);
+#pragma unroll
+  for (int a = 0; a < 7; ++a) out.p[a][o] = v[a];
+}
+
+}  // namespace coffee

@@ -209,3 +209,145 @@ def pulsar_fields(p: SimParams, dtype=np.float32):
     zeros = np.zeros_like(X)
     arrs = [zeros, zeros, zeros, p.b0 * b[0], p.b0 * b[1], p.b0 * b[2], zeros]
     return [np.asarray(a, dtype=dtype).copy() for a in arrs]
+
+
+# ------------------------------------------------ 2D log-spherical pulsar
+
+
+def sph_pulsar_params(nr: int = 64, nth: int = 32, guard: int = 4, r_out: float = 100.0,
+                      omega: float = 0.2, b0: float = 1.0, pml: int = 8,
+                      cfl: float = 0.3) -> SimParams:
+    """Aligned dipole star of radius 1 on x = ln r in [0, ln r_out],
+    theta in [0, pi], one z plane (``src/main-pulsar2d-spherical.cpp`` +
+    ``src/user_pulsar_sph.hpp``).  guard[1] >= 4 because the reference's axis
+    boundary writes three rows beyond theta = pi, which is the first guard
+    row.  dt = cfl * d(ln r): the smallest cell is r * d(ln r) at r = 1."""
+    p = SimParams()
+    p.N = [nr, nth, 1]
+    p.guard = [guard, guard, 0]
+    p.lower = [0.0, 0.0, 0.0]
+    p.size = [math.log(r_out), math.pi, 1.0]
+    p.periodic_boundary = [False, False, False]
+    p.pml = [pml, 0, 0]
+    p.pmllen = max(1, pml)
+    p.sigpml = 0.1
+    p.problem = 1
+    p.radius = 1.0
+    p.omega = omega
+    p.b0 = b0
+    p.dt = cfl * math.log(r_out) / nr
+    return p
+
+
+def sph_pulsar_fields(p: SimParams, dtype=np.float32):
+    """B^r = b0 2 cos(th) / r^3 / sqrt(g_11), B^th = b0 sin(th) / r^3 /
+    sqrt(g_22), B^phi = 0, E = 0, P = 0 (``src/user_pulsar_sph.hpp``;
+    dipole_sph_2d, ``pulsar_impl.hpp:131-139``; g_11 = g_22 = r^2), as arrays
+    of shape (1, d1, d0)."""
+    g = Grid.from_params(p, dtype)
+    tiny = 1e-7 if np.dtype(dtype) == np.float32 else 1e-11
+    x = g.coords(0, np.float64)
+    th = g.coords(1, np.float64)
+    TH, X = np.meshgrid(th, x, indexing="ij")
+    r = np.exp(X)
+    gs = np.maximum(r, tiny)
+    zeros = np.zeros_like(X)
+    br = p.b0 * (2.0 * np.cos(TH) / r ** 3) / gs
+    bt = p.b0 * (np.sin(TH) / r ** 3) / gs
+    arrs = [zeros, zeros, zeros, br, bt, zeros, zeros]
+    return [np.asarray(a, dtype=dtype)[None].copy() for a in arrs]
+
+
+# ---------------------------------------------------- 2D cylindrical pulsar
+
+
+def cyl_pulsar_params(nR: int = 64, nz: int = 128, guard: int = 3, R_max: float = 16.0,
+                      radius: float = 2.0, omega: float = 0.1, b0: float = 1.0, pml: int = 8,
+                      cfl: float = 0.4) -> SimParams:
+    """Aligned dipole star at the origin of an R-z box, R in [0, R_max],
+    z in [-R_max, R_max] (``src/main-pulsar2d-cylindrical.cpp`` +
+    ``src/user_pulsar.hpp``); the R = 0 axis is the first interior column.
+    The z grid is shifted by half a cell so that no point is at the origin."""
+    p = SimParams()
+    p.N = [nR, nz, 1]
+    p.guard = [guard, guard, 0]
+    dz = 2 * R_max / nz
+    p.lower = [0.0, -R_max - 0.5 * dz, 0.0]
+    p.size = [R_max, 2 * R_max, 1.0]
+    p.periodic_boundary = [False, False, False]
+    p.pml = [pml, pml, 0]
+    p.pmllen = max(1, pml // 2)
+    p.sigpml = 0.1
+    p.problem = 1
+    p.radius = radius
+    p.omega = omega
+    p.b0 = b0
+    p.dt = cfl * min(R_max / nR, dz)
+    return p
+
+
+def cyl_pulsar_fields(p: SimParams, dtype=np.float32):
+    """B_R, B_z of a dipole of moment b0 R*^3 along z, E = 0, P = 0
+    (``src/user_pulsar.hpp``: dipole_x / dipole_z of ``pulsar_impl.hpp:10-50``
+    with alpha = phase = 0), as arrays of shape (1, d1, d0)."""
+    g = Grid.from_params(p, dtype)
+    tiny = 1e-7 if np.dtype(dtype) == np.float32 else 1e-11
+    R = g.coords(0, np.float64)
+    z = g.coords(1, np.float64)
+    Zz, RR = np.meshgrid(z, R, indexing="ij")
+    r = np.sqrt(RR * RR + Zz * Zz)
+    r = np.where(np.abs(r) < tiny, tiny, r)
+    xn, zn = RR / r, Zz / r
+    m = p.b0 * p.radius ** 3
+    zeros = np.zeros_like(RR)
+    bR = m * (3.0 * xn * zn) / (r ** 3 + tiny)
+    bz = m * (3.0 * zn * zn - 1.0) / (r ** 3 + tiny)
+    arrs = [zeros, zeros, zeros, bR, bz, zeros, zeros]
+    return [np.asarray(a, dtype=dtype)[None].copy() for a in arrs]
+
+
+# ------------------------------------------------ GR Kerr-Schild Wald field
+
+
+def wald_params(N: int = 48, guard: int = 3, half_size: float = 6.0, a: float = 0.9,
+                pml: int = 6, cfl: float = 0.3) -> SimParams:
+    """Kerr black hole of spin a (M = 1) at the centre of [-L, L]^3 in
+    Cartesian Kerr-Schild coordinates, absorbing layer at the box faces and
+    the reference's inner absorbing region inside 0.7 r_H
+    (``src/main-gr.cpp`` + ``src/user_wald2.hpp``).  The grid is shifted by
+    half a cell so that no point sits on the ring singularity's axis."""
+    p = SimParams()
+    p.N = [N, N, N]
+    p.guard = [guard] * 3
+    d = 2 * half_size / N
+    p.lower = [-half_size - 0.5 * d] * 3
+    p.size = [2 * half_size] * 3
+    p.periodic_boundary = [False, False, False]
+    p.pml = [pml] * 3
+    p.pmllen = max(1, pml // 2)
+    p.sigpml = 0.1
+    p.a = a
+    p.problem = 0
+    p.dt = cfl * d
+    return p
+
+
+def cks_sqrt_gamma(a, x, y, z, tiny):
+    """sqrt(gamma) of the Kerr-Schild 3-metric (metric_cks_impl.hpp:17-83), float64."""
+    R2 = x * x + y * y + z * z
+    r = np.sqrt((R2 - a * a + np.sqrt(np.maximum((R2 - a * a) ** 2 + 4.0 * (a * z) ** 2, tiny)))
+                / 2.0)
+    return np.sqrt(1.0 + 2.0 * r ** 3 / np.maximum(r ** 4 + a * a * z * z, tiny))
+
+
+def wald_fields(p: SimParams, dtype=np.float32):
+    """Uniform asymptotic field along the spin axis: B^z = 1 / sqrt(gamma),
+    D = 0, P = 0 (``src/user_wald2.hpp``)."""
+    g = Grid.from_params(p, dtype)
+    tiny = 1e-7 if np.dtype(dtype) == np.float32 else 1e-11
+    x, y, z = (g.coords(a, np.float64) for a in range(3))
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    bz = 1.0 / cks_sqrt_gamma(p.a, X, Y, Z, tiny)
+    zeros = np.zeros_like(X)
+    arrs = [zeros, zeros, zeros, zeros, zeros, bz, zeros]
+    return [np.asarray(a, dtype=dtype).copy() for a in arrs]

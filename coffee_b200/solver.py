@@ -174,6 +174,8 @@ class SimData:
 class FieldSolverEZ:
     """``field_solver_EZ(sim_data&, sim_environment&)`` on the GPU."""
 
+    VARIANT = _lib.VARIANT_FLAT
+
     def __init__(self, data: SimData, env: SimEnvironment, semantics: str = "cpu",
                  stream: int | None = None):
         self.data = data
@@ -181,7 +183,7 @@ class FieldSolverEZ:
         self.lib = env.lib
         sem = {"cpu": _lib.SEM_CPU_REF, "gpu": _lib.SEM_GPU_REF}[semantics]
         h = ctypes.c_void_p()
-        check(self.lib.coffee_solver_create(env.handle, data.handle, _lib.VARIANT_FLAT, sem,
+        check(self.lib.coffee_solver_create(env.handle, data.handle, self.VARIANT, sem,
                                             ctypes.c_void_p(stream or 0), ctypes.byref(h)))
         self.handle = h
 
@@ -262,3 +264,75 @@ def run_flat(params: SimParams, fields, nsteps: int, time0: float = 0.0, semanti
     data.close()
     env.close()
     return out, auxa
+
+
+class FieldSolverEZSpherical(FieldSolverEZ):
+    """``field_solver_EZ_spherical(sim_data&, sim_environment&)``
+    (src/algorithms/field_solver_EZ_spherical.h:6-32): the 2D log-spherical
+    solver, x = ln r, y = theta, one z plane (N[2] = 1, guard[2] = 0).  The
+    reference has it only in its GPU build, which it reproduces."""
+
+    VARIANT = _lib.VARIANT_LOGSPH
+
+    def __init__(self, data: SimData, env: SimEnvironment, stream: int | None = None):
+        super().__init__(data, env, semantics="gpu", stream=stream)
+
+
+class FieldSolverEZCylindrical(FieldSolverEZ):
+    """``field_solver_EZ_cylindrical(sim_data&, sim_environment&)``
+    (src/algorithms/field_solver_EZ_cylindrical.h:6-30): the 2D R-z solver.
+    The reference's solver evolves a P of its own; here P is sim_data's P."""
+
+    VARIANT = _lib.VARIANT_CYL
+
+    def __init__(self, data: SimData, env: SimEnvironment, stream: int | None = None):
+        super().__init__(data, env, semantics="gpu", stream=stream)
+
+
+class FieldSolverGrEZ(FieldSolverEZ):
+    """``field_solver_gr_EZ(sim_data&, sim_environment&)``
+    (src/algorithms/field_solver_gr_EZ.h:6-32): force-free electrodynamics in
+    Cartesian Kerr-Schild coordinates around a black hole of spin
+    ``params.a``.  sim_data's E holds the displacement D; J / divE / divB
+    (set_aux) receive J, div D and div B."""
+
+    VARIANT = _lib.VARIANT_GR
+
+    def __init__(self, data: SimData, env: SimEnvironment, stream: int | None = None):
+        super().__init__(data, env, semantics="gpu", stream=stream)
+
+
+class SphBatch:
+    """Independent log-spherical runs advanced together, one kernel launch
+    per phase for all of them (``coffee_batch_*``; no counterpart in the
+    reference, which runs one grid per process)."""
+
+    def __init__(self, solvers, stream: int | None = None):
+        self.solvers = list(solvers)
+        self.lib = self.solvers[0].lib
+        n = len(self.solvers)
+        arr = (ctypes.c_void_p * n)(*[s.handle.value for s in self.solvers])
+        h = ctypes.c_void_p()
+        check(self.lib.coffee_batch_create(arr, n, ctypes.c_void_p(stream or 0), ctypes.byref(h)))
+        self.handle = h
+        self.times = np.zeros(n, dtype=np.float64)
+
+    def step(self, nsteps: int):
+        """nsteps evolve_fields calls of every run; self.times advances."""
+        t = np.ascontiguousarray(self.times, dtype=np.float64)
+        check(self.lib.coffee_batch_step(self.handle,
+                                         t.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                         int(nsteps)))
+        self.times = t
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.coffee_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

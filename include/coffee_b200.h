@@ -58,7 +58,10 @@ enum { /* field ids for coffee_fields_ptr / upload / download */
   COFFEE_NUM_FIELDS
 };
 enum { /* solver variants */
-  COFFEE_VARIANT_FLAT = 0 /* Cartesian EZ, field_solver_EZ */
+  COFFEE_VARIANT_FLAT = 0,   /* Cartesian EZ, field_solver_EZ */
+  COFFEE_VARIANT_LOGSPH = 1, /* 2D log-spherical EZ, field_solver_EZ_spherical (GPU build) */
+  COFFEE_VARIANT_CYL = 2,    /* 2D cylindrical EZ, field_solver_EZ_cylindrical (GPU build) */
+  COFFEE_VARIANT_GR = 3      /* Kerr-Schild GR EZ, field_solver_gr_EZ (GPU build); E holds D */
 };
 enum { /* which reference build the flat solver reproduces */
   COFFEE_SEM_CPU_REF = 0, /* field_solver_EZ.cpp (the parity oracle build) */
@@ -231,6 +234,21 @@ COFFEE_API int coffee_solver_save_snapshot(coffee_solver* s, const char* path, d
                                 int64_t step);
 COFFEE_API int coffee_solver_load_snapshot(coffee_solver* s, const char* path, double* time,
                                 int64_t* step);
+
+/* ---- batches of log-spherical runs -------------------------------------
+ * No counterpart in the reference (which runs one grid per process).  Many
+ * independent log-spherical runs (COFFEE_VARIANT_LOGSPH solvers on the same
+ * device, each with its own grid, parameters and fields) advanced together:
+ * one kernel launch per phase covers every run, so small grids do not pay a
+ * launch each.  Results are those of coffee_solver_step on each solver.  At
+ * most 128 runs, all of one precision; the solvers must outlive the batch.
+ * coffee_batch_step advances every run by nsteps evolve_fields calls from
+ * times[m] and writes the new times back (advanced in field precision). */
+typedef struct coffee_batch coffee_batch;
+COFFEE_API int coffee_batch_create(coffee_solver* const* solvers, int n, void* stream,
+                                   coffee_batch** out);
+COFFEE_API int coffee_batch_step(coffee_batch* b, double* times, int nsteps);
+COFFEE_API int coffee_batch_destroy(coffee_batch* b);
 
 #ifdef __cplusplus
 }

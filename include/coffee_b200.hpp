@@ -358,6 +358,56 @@ class field_solver_EZ {
   coffee_solver* m_solver = nullptr;
 };
 
+// The solvers the reference has only in its GPU build share one shape:
+// (sim_data&, sim_environment&) and evolve_fields(Scalar time).
+class gpu_variant_solver {
+ public:
+  gpu_variant_solver(sim_data& mydata, sim_environment& env, int variant, const char* name,
+                     void* stream) {
+    coffee_check(coffee_solver_create(env.handle(), mydata.handle(), variant,
+                                      COFFEE_SEM_GPU_REF, stream, &m_solver),
+                 name);
+  }
+  ~gpu_variant_solver() { coffee_solver_destroy(m_solver); }
+  gpu_variant_solver(const gpu_variant_solver&) = delete;
+  gpu_variant_solver& operator=(const gpu_variant_solver&) = delete;
+
+  void evolve_fields(Scalar time) {
+    coffee_check(coffee_solver_step(m_solver, (double)time, 1), "evolve_fields");
+  }
+  void set_aux(bool enable) { coffee_check(coffee_solver_set_aux(m_solver, enable), "set_aux"); }
+  coffee_solver* handle() const { return m_solver; }
+
+ private:
+  coffee_solver* m_solver = nullptr;
+};
+
+// field_solver_EZ_spherical (src/algorithms/field_solver_EZ_spherical.h:6-32):
+// 2D, x = ln r, y = theta; N[2] = 1, guard[2] = 0, guard[1] >= 4.
+class field_solver_EZ_spherical : public gpu_variant_solver {
+ public:
+  field_solver_EZ_spherical(sim_data& mydata, sim_environment& env, void* stream = nullptr)
+      : gpu_variant_solver(mydata, env, COFFEE_VARIANT_LOGSPH, "field_solver_EZ_spherical",
+                           stream) {}
+};
+
+// field_solver_EZ_cylindrical (src/algorithms/field_solver_EZ_cylindrical.h:6-30):
+// 2D, x = R, y = z.  Evolves sim_data's P (the reference keeps its own).
+class field_solver_EZ_cylindrical : public gpu_variant_solver {
+ public:
+  field_solver_EZ_cylindrical(sim_data& mydata, sim_environment& env, void* stream = nullptr)
+      : gpu_variant_solver(mydata, env, COFFEE_VARIANT_CYL, "field_solver_EZ_cylindrical",
+                           stream) {}
+};
+
+// field_solver_gr_EZ (src/algorithms/field_solver_gr_EZ.h:6-32): Kerr-Schild
+// black hole of spin params().a; sim_data's E holds D.
+class field_solver_gr_EZ : public gpu_variant_solver {
+ public:
+  field_solver_gr_EZ(sim_data& mydata, sim_environment& env, void* stream = nullptr)
+      : gpu_variant_solver(mydata, env, COFFEE_VARIANT_GR, "field_solver_gr_EZ", stream) {}
+};
+
 }  // namespace Coffee
 
 #endif  // COFFEE_B200_HPP

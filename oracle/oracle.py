@@ -9,6 +9,12 @@ Two checkers live here, both CPU-only and never part of the product path:
 * ``run_reference`` - the reference's own CPU build (oracle/_ref, compiled by
   oracle/Makefile from the reference sources), driven through a config.toml
   and a .fld input file.
+* ``run_reference_gpu`` - the reference's own GPU build of its flat,
+  log-spherical, cylindrical and GR solvers (oracle/_ref/coffee_refgpu_*,
+  ``make -C oracle gpuref``), the same way; it needs a GPU.
+
+The numpy restatements of the log-spherical, cylindrical and GR solvers are
+in axisym_oracle.py and gr_oracle.py.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
 module.
@@ -167,6 +173,43 @@ def run_reference(p: SimParams, fields, nsteps: int, time0: float = 0.0, aux: bo
             for f in os.listdir(wd):
                 os.unlink(os.path.join(wd, f))
             os.rmdir(wd)
+
+
+def refgpu_binary(dtype=np.float32) -> str:
+    return os.path.join(REF_DIR, "coffee_refgpu_float" if np.dtype(dtype) == np.float32
+                        else "coffee_refgpu_double")
+
+
+def run_reference_gpu(solver: str, p: SimParams, fields, nsteps: int, time0: float = 0.0,
+                      aux: bool = False, timeout: float | None = 600):
+    """Run the reference's own GPU build (oracle/ref_harness_gpu) of one of
+    its solvers: "ez", "sph", "cyl" or "gr".  Needs a GPU.  Returns
+    (fields, aux_or_None, info) like run_reference."""
+    exe = refgpu_binary(fields[0].dtype)
+    if not os.path.exists(exe):
+        raise RuntimeError(f"{exe} missing: run `make -C oracle gpuref`")
+    wd = tempfile.mkdtemp(prefix="coffee_refgpu_")
+    try:
+        cfg = os.path.join(wd, "config.toml")
+        p.write_toml(cfg)
+        fin = os.path.join(wd, "in.fld")
+        fout = os.path.join(wd, "out.fld")
+        write_fld(fin, fields, guard=tuple(p.guard), time=time0)
+        cmd = [exe, solver, fin, fout, str(int(nsteps))] + (["--aux"] if aux else [])
+        env = dict(os.environ, COFFEE_ORACLE_CONFIG=cfg)
+        r = subprocess.run(cmd, cwd=wd, env=env, capture_output=True, text=True,
+                           timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference GPU run failed ({r.returncode}): {r.stderr[-2000:]}")
+        info = json.loads(r.stdout.strip().splitlines()[-1])
+        ff = read_fld(fout)
+        out = [a.copy() for a in ff.arrays[:7]]
+        auxa = [a.copy() for a in ff.arrays[7:12]] if aux else None
+        return out, auxa, info
+    finally:
+        for f in os.listdir(wd):
+            os.unlink(os.path.join(wd, f))
+        os.rmdir(wd)
 
 
 def rel_l2(a, b, interior=None):
