@@ -210,6 +210,24 @@ def cpu_reference_run(steps: int, warmup: int, nproc: int | None = None):
 
 # ------------------------------------------------------------------ arms
 
+def max_over_ranks(x: float, dist=None, device=None) -> float:
+    """The largest value of x over all ranks (x itself with one rank)."""
+    if dist is None:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64,
+                     device=device if device is not None else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(cells: int, steps: int, world: int, seconds_max: float) -> float:
+    """Whole-job cell-updates/s: every rank advances its own replica of
+    `cells` points by `steps` steps; the job takes the slowest rank's time."""
+    return cells * steps * world / seconds_max
+
+
 def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -265,12 +283,6 @@ def run_ours(args):
             dist.barrier(device_ids=[local])
         torch.cuda.synchronize(dev)
 
-    def max_over_ranks(x):
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     p = problems.turbulence_params(N_SIDE)
     cells = N_SIDE ** 3
     env = SimEnvironment(p, device=local)
@@ -302,12 +314,12 @@ def run_ours(args):
     barrier()
     clk = clocks.stop(w0, w1)
     ms = e0.elapsed_time(e1)
-    ms_max = max_over_ranks(ms)
+    ms_max = max_over_ranks(ms, dist, dev)
     timing = solver.last_timing()
     solver.set_timing(False)
     solver.check_finite()
 
-    value = cells * args.steps * ws / (ms_max / 1e3)
+    value = job_throughput(cells, args.steps, ws, ms_max / 1e3)
     step_ms = ms_max / args.steps
     hbm_gbs = BYTES_STEP * cells / (step_ms / 1e3) / 1e9
     n_stage = timing["launches"]["stage"]
@@ -332,9 +344,9 @@ def run_ours(args):
         energies.append(solver.total_energy("B"))
     data.download_packed(hnp)
     torch.cuda.synchronize(dev)
-    e2e_s = max_over_ranks(time.perf_counter() - w0)
+    e2e_s = max_over_ranks(time.perf_counter() - w0, dist, dev)
     barrier()
-    e2e_value = cells * args.steps * ws / e2e_s
+    e2e_value = job_throughput(cells, args.steps, ws, e2e_s)
     d2h_diag = 8 * (148 * 4)  # FP64 partials read back per energy diagnostic
 
     cpu = None
