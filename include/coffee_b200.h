@@ -250,6 +250,28 @@ COFFEE_API int coffee_batch_create(coffee_solver* const* solvers, int n, void* s
 COFFEE_API int coffee_batch_step(coffee_batch* b, double* times, int nsteps);
 COFFEE_API int coffee_batch_destroy(coffee_batch* b);
 
+/* ---- one step loop that allocates nothing ------------------------------
+ * No counterpart in the reference.  For callers that must not allocate
+ * device memory: hosts whose device memory is all handed out by their own
+ * allocator or pool, and hosts that cannot afford the device-wide
+ * synchronisation that cudaMalloc/cudaFree can cause in the middle of their
+ * own pipeline.  It runs the same kernels as coffee_solver_step on the 7 FP32
+ * field arrays the caller owns (Ex Ey Ez Bx By Bz P on the current device,
+ * the reference layout, dims = N + 2*guard), in place, nsteps evolve_fields
+ * calls from `time`, on `stream`.  Its scratch -- the second field buffer,
+ * the LSRK accumulators and the start-of-step copy -- lives in one static
+ * 32 MiB device array that every GPU loading the library holds until the
+ * process exits, so grids are limited to 399,457 points per array (e.g. a
+ * 64^3 interior with 3 guards, 70^3 = 343,000 points); larger grids are
+ * rejected with COFFEE_E_INVALID.  It calls no cudaMalloc or cudaFree.  The
+ * first call on a device looks up the array's device address for that
+ * device; make that first call before any stream capture.  All calls share
+ * the one array: calls that overlap on the GPU (other streams, other host
+ * threads) race.  J, divE and divB are not produced. */
+COFFEE_API int coffee_evolve_noalloc(const coffee_params* p, int semantics,
+                                     float* const fields[7], double time, int nsteps,
+                                     void* stream);
+
 #ifdef __cplusplus
 }
 #endif
