@@ -283,8 +283,9 @@ def run_ours(args):
             dist.barrier(device_ids=[local])
         torch.cuda.synchronize(dev)
 
-    p = problems.turbulence_params(N_SIDE)
-    cells = N_SIDE ** 3
+    n_side = args.n
+    p = problems.turbulence_params(n_side)
+    cells = n_side ** 3
     env = SimEnvironment(p, device=local)
     data = SimData(env, np.float32)
     modes = problems.turbulence_modes()
@@ -361,9 +362,10 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded random force-free turbulence, seed 20261203)",
-            "config": {"workload": "turbulence512", "grid": [N_SIDE] * 3, "guard": 3,
+            "config": {"workload": f"turbulence{n_side}", "grid": [n_side] * 3, "guard": 3,
                        "periodic": True, "cfl": 0.5, "semantics": "reference CPU build",
-                       "l2": "inputs larger than L2 (21 arrays x 556 MB resident), no flush",
+                       "l2": ("inputs larger than L2 (21 arrays x 556 MB resident), no flush"
+                              if n_side >= 512 else "smaller case (profiling)"),
                        "parallelism": f"replicas x{ws}"},
             "hbm_gbs": hbm_gbs,
             "roofline": {"kernel": "ez_stage_kernel (LSRK stages 2-5)", "bound": "hbm",
@@ -390,6 +392,182 @@ def run_ours(args):
     return 0
 
 
+# ------------------------------------------------- other solvers' workloads
+# Not the headline: measurement lines for the configurations of the other
+# solvers (--workload gr-wald | logsph-batch | logsph | cyl-pulsar).  Their reference
+# implementation exists only as the reference's GPU build, which
+# --impl reference times on the same case.
+
+VARIANT_STAGE_BYTES = {"gr-wald": 136, "logsph-batch": 112, "logsph": 112, "cyl-pulsar": 112}
+
+
+def _variant_cases(workload):
+    """(list of (solver class name, params, FP32 fields), description)."""
+    import numpy as np
+
+    from coffee_b200 import problems
+
+    if workload == "gr-wald":
+        p = problems.wald_params(N=256, half_size=20.0, a=0.9, pml=16)
+        return [("FieldSolverGrEZ", "gr", p, problems.wald_fields(p, np.float32))], {
+            "workload": "gr-wald256", "grid": [256] * 3, "spin": 0.9, "domain": [-20, 20],
+            "pml": 16, "note": "Wald field B0 = 1 along the spin axis, E = 0, P = 0"}
+    if workload == "logsph":
+        p = problems.sph_pulsar_params(nr=2048, nth=1024, guard=4, omega=0.2)
+        return [("FieldSolverEZSpherical", "sph", p, problems.sph_pulsar_fields(p, np.float32))], {
+            "workload": "logsph2048x1024", "grid": [2048, 1024], "r": [1, 100]}
+    if workload == "cyl-pulsar":
+        p = problems.cyl_pulsar_params(nR=1024, nz=2048, guard=3, R_max=64.0, radius=4.0)
+        return [("FieldSolverEZCylindrical", "cyl", p, problems.cyl_pulsar_fields(p, np.float32))], {
+            "workload": "cyl-pulsar1024x2048", "grid": [1024, 2048]}
+    rng = np.random.default_rng(20261203)
+    sizes = [(512, 256), (768, 384), (1024, 512), (2048, 1024)]
+    runs = []
+    for _ in range(64):
+        nr, nth = sizes[int(rng.integers(len(sizes)))]
+        r_lc = float(rng.uniform(3.0, 10.0))
+        p = problems.sph_pulsar_params(nr=nr, nth=nth, guard=4, omega=1.0 / r_lc)
+        runs.append(("FieldSolverEZSpherical", "sph", p, problems.sph_pulsar_fields(p, np.float32)))
+    return runs, {"workload": "logsph-batch64", "runs": 64,
+                  "grids": "r x theta drawn from 512x256, 768x384, 1024x512, 2048x1024 (seeded)",
+                  "r": [1, 100], "R_LC": [3, 10], "launch": "one kernel per phase for all runs"}
+
+
+def run_variant(args):
+    import numpy as np
+    import torch
+
+    from coffee_b200 import solver as sv
+
+    ws, rank, local = _dist()
+    if args.impl == "reference":
+        from oracle import oracle
+
+        if rank != 0:
+            return 0
+        runs, cfg = _variant_cases(args.workload)
+        secs, cells = 0.0, 0
+        for _cls, name, p, f in runs:
+            oracle.run_reference_gpu(name, p, f, args.warmup)
+            _, _, info = oracle.run_reference_gpu(name, p, f, args.steps)
+            secs += info["seconds"]
+            cells += int(np.prod(p.N))
+        value = cells * args.steps / secs
+        line = {"impl": "reference", "metric": "cell-updates/s", "value": value, "unit": UNIT,
+                "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": cfg,
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": 0,
+                                 "kind": "reference",
+                                 "sample": "the reference's own GPU build of this solver "
+                                           "(oracle/_ref/coffee_refgpu_float), one run at a "
+                                           "time; the reference has no CPU build of it"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    runs, cfg = _variant_cases(args.workload)
+    objs = []
+    cells = 0
+    for cls_name, _name, p, f in runs:
+        env = sv.SimEnvironment(p, device=local)
+        data = sv.SimData(env, np.float32)
+        data.upload(f)
+        solver = getattr(sv, cls_name)(data, env, stream=stream.cuda_stream)
+        objs.append((env, data, solver))
+        cells += int(np.prod(p.N))
+    batch = sv.SphBatch([o[2] for o in objs], stream=stream.cuda_stream) \
+        if args.workload == "logsph-batch" else None
+
+    def advance(n):
+        if batch is not None:
+            batch.step(n)
+        else:
+            objs[0][2].step(0.0, n)
+
+    advance(args.warmup)
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(local)
+    clocks.start()
+    if batch is None:
+        objs[0][2].set_timing(True)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    w0 = time.time()
+    e0.record(stream)
+    advance(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop(w0, time.time())
+    ms = e0.elapsed_time(e1)
+    step_ms = ms / args.steps
+    value = job_throughput(cells, args.steps, 1, ms / 1e3)
+    peak, peak_kind = _peaks()
+    if batch is None:
+        timing = objs[0][2].last_timing()
+        objs[0][2].set_timing(False)
+        n_stage = timing["launches"]["stage"]
+        avg = timing["ms"]["stage"] / max(1, n_stage)
+        kname = {"gr-wald": "gr_stage_kernel", "cyl-pulsar": "cyl_stage_kernel",
+                 "logsph": "sph_stage_kernel"}[args.workload]
+        roof = {"kernel": kname + " (LSRK stages 2-5)", "bound": "hbm",
+                "achieved": VARIANT_STAGE_BYTES[args.workload] * cells / (avg / 1e3) / 1e9,
+                "peak": peak, "unit": "GB/s", "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": VARIANT_STAGE_BYTES[args.workload] * cells,
+                "avg_launch_ms": avg}
+        launches = sum(timing["launches"].values())
+        launch_note = "stage + KO kernels counted by the solver's launch hooks"
+    else:
+        roof = {"kernel": "whole batched step (stage, axis and KO launches)", "bound": "hbm",
+                "achieved": BYTES_STEP * cells / (step_ms / 1e3) / 1e9, "peak": peak,
+                "unit": "GB/s", "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_step": BYTES_STEP * cells}
+        launches = 12 * args.steps + 1
+        launch_note = "5 stage + 5 axis + 1 KO + 1 axis per step, 1 axis per call"
+    roof["frac"] = roof["achieved"] / peak
+    # end to end: upload from pinned host memory, K steps, download
+    hosts = []
+    nbytes = 0
+    for env, data, _s in objs:
+        d0, d1, d2 = env.dims
+        h = torch.empty(7 * d0 * d1 * d2, dtype=torch.float32, pin_memory=True)
+        data.download_packed(h.numpy())
+        hosts.append(h)
+        nbytes += h.numel() * 4
+    torch.cuda.synchronize(dev)
+    w0 = time.perf_counter()
+    for (env, data, _s), h in zip(objs, hosts):
+        data.upload_packed(h.numpy())
+    advance(args.steps)
+    for (env, data, _s), h in zip(objs, hosts):
+        data.download_packed(h.numpy())
+    torch.cuda.synchronize(dev)
+    e2e_s = time.perf_counter() - w0
+    line = {"metric": "cell-updates/s", "value": value, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": cfg, "roofline": roof, "gpu_launches": launches,
+            "gpu_launches_note": launch_note,
+            "e2e": {"value": job_throughput(cells, args.steps, 1, e2e_s), "unit": UNIT,
+                    "h2d_bytes_per_step": nbytes / args.steps,
+                    "d2h_bytes_per_step": nbytes / args.steps},
+            "clocks": clk}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if batch is not None:
+        batch.close()
+    for env, data, s in objs:
+        s.close()
+        data.close()
+        env.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -397,9 +575,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--n", type=int, default=N_SIDE,
+                    help="grid side of the turbulence workload (512 is the benchmark)")
+    ap.add_argument("--workload", default="turbulence",
+                    choices=["turbulence", "gr-wald", "logsph-batch", "logsph", "cyl-pulsar"])
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.workload != "turbulence":
+        return run_variant(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_ours(args)

@@ -291,14 +291,18 @@ __device__ __forceinline__ void sph_stage_point(const SphConst<T>& c, const int 
   V7<T> w;
 #pragma unroll
   for (int a = 0; a < 7; ++a) w.v[a] = v[a];
-  const T th = c.y0 + c.dy * (T)(j - c.g1);
-  w = sph_pulsar(c, w, rc, sc, __ldg(c.ct + j), th, tst);
-  if ((flags & AX_LAST) && c.absorbing) {
+  // the out-of-line boundary code is entered only where it can act
+  if (rc < c.radius + c.dx) {
+    const T th = c.y0 + c.dy * (T)(j - c.g1);
+    w = sph_pulsar(c, w, rc, sc, __ldg(c.ct + j), th, tst);
+  }
+  const T xi = c.x0 + c.dx * (T)(i - c.g0);
+  if ((flags & AX_LAST) && c.absorbing && xi > c.xh) {
     V7<T> n;
 #pragma unroll
     for (int a = 0; a < 6; ++a) n.v[a] = un.p[a][o];
     n.v[6] = T(0);
-    w = sph_absorb(c, w, n, c.x0 + c.dx * (T)(i - c.g0), rc);
+    w = sph_absorb(c, w, n, xi, rc);
   }
 #pragma unroll
   for (int a = 0; a < 7; ++a) out.p[a][o] = w.v[a];
@@ -362,7 +366,8 @@ __device__ __forceinline__ void sph_ko_point(const SphConst<T>& c, const int i, 
   V7<T> w;
 #pragma unroll
   for (int a = 0; a < 7; ++a) w.v[a] = v[a];
-  w = sph_pulsar(c, w, rc, sc, __ldg(c.ct + j), c.y0 + c.dy * (T)(j - c.g1), tend);
+  if (rc < c.radius + c.dx)
+    w = sph_pulsar(c, w, rc, sc, __ldg(c.ct + j), c.y0 + c.dy * (T)(j - c.g1), tend);
 #pragma unroll
   for (int a = 0; a < 7; ++a) out.p[a][o] = w.v[a];
 }
@@ -648,8 +653,9 @@ __device__ __forceinline__ void cyl_finish(const CylConst<T>& c, int i, int j, l
                                           T t, bool last) {
   const T z = c.z0 + c.dz * (T)(j - c.g1);
   auto bc = [&](V7<T> w, long long p, T R) {
-    w = cyl_pulsar(c, w, R, z, t);
-    if (last && c.absorbing) {
+    // the out-of-line boundary code is entered only where it can act
+    if (R * R + z * z < T(4) * c.radius * c.radius + Tiny<T>::v) w = cyl_pulsar(c, w, R, z, t);
+    if (last && c.absorbing && (R > c.xh || z < c.yl || z > c.yh)) {
       V7<T> n;
       for (int a = 0; a < 6; ++a) n.v[a] = un.p[a][p];
       n.v[6] = T(0);

@@ -311,7 +311,9 @@ __global__ void __launch_bounds__(256) gr_stage_kernel(const __grid_constant__ G
   V7<T> w;
 #pragma unroll
   for (int a = 0; a < 7; ++a) w.v[a] = v[a];
-  if ((flags & AX_LAST) && c.absorbing) {
+  const bool in_layer = x > c.xh[0] || x < c.xl[0] || y > c.xh[1] || y < c.xl[1] ||
+                        z > c.xh[2] || z < c.xl[2] || m.r < c.r1;
+  if ((flags & AX_LAST) && c.absorbing && in_layer) {
     V7<T> n;
 #pragma unroll
     for (int a = 0; a < 6; ++a) n.v[a] = un.p[a][o];
