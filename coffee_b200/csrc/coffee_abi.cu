@@ -242,8 +242,15 @@ extern "C" int coffee_env_create(const coffee_params* p, int device, coffee_env*
 }
 
 extern "C" int coffee_env_destroy(coffee_env* env) {
-  delete env;
+  if (!env) return COFFEE_OK;
+  env->released = true;
+  if (env->users.load() == 0) delete env;
   return COFFEE_OK;
+}
+
+// A fields or solver object created on `env` is gone.
+static void env_drop_user(coffee_env* env) {
+  if (env->users.fetch_sub(1) == 1 && env->released.load()) delete env;
 }
 
 extern "C" int coffee_env_grid(const coffee_env* env, coffee_grid* grid) {
@@ -277,13 +284,15 @@ extern "C" int coffee_fields_create(coffee_env* env, int elem_size, coffee_field
     cudaError_t err = cudaMalloc(&f->d[a], f->n * elem_size);
     if (err == cudaSuccess) err = cudaMemset(f->d[a], 0, f->n * elem_size);
     if (err != cudaSuccess) {
+      const size_t bytes = f->n * (size_t)elem_size;
       for (int b = 0; b <= a; ++b) cudaFree(f->d[b]);
       delete f;
-      return fail(COFFEE_E_NOMEM, "cudaMalloc of field %d (%zu bytes) failed: %s", a,
-                  f->n * (size_t)elem_size, cudaGetErrorString(err));
+      return fail(COFFEE_E_NOMEM, "cudaMalloc of field %d (%zu bytes) failed: %s", a, bytes,
+                  cudaGetErrorString(err));
     }
   }
   f->generation = 1;
+  env->users++;
   *out = f;
   return COFFEE_OK;
 }
@@ -293,7 +302,10 @@ extern "C" int coffee_fields_destroy(coffee_fields* f) {
   cudaSetDevice(f->env->device);
   for (int a = 0; a < COFFEE_NUM_FIELDS; ++a)
     if (f->d[a]) cudaFree(f->d[a]);
+  (void)cudaGetLastError();  // leave no error of a release for the next call to find
+  coffee_env* env = f->env;
   delete f;
+  env_drop_user(env);
   return COFFEE_OK;
 }
 
@@ -548,6 +560,7 @@ extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int varia
     cleanup();
     return fail(COFFEE_E_NOMEM, "solver setup failed: %s", cudaGetErrorString(err));
   }
+  env->users++;
   *out = s;
   return COFFEE_OK;
 }
@@ -567,7 +580,10 @@ extern "C" int coffee_solver_destroy(coffee_solver* s) {
   cudaEventDestroy(s->ev_end);
   cudaFree(s->d_partials);
   cudaFree(s->d_count);
+  (void)cudaGetLastError();  // leave no error of a release for the next call to find
+  coffee_env* env = s->env;
   delete s;
+  env_drop_user(env);
   return COFFEE_OK;
 }
 

@@ -14,6 +14,7 @@
 // accumulators, and the start-of-step copy is written before it is read).
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <mutex>
 
 #include "coffee_b200.h"
@@ -111,6 +112,10 @@ extern "C" int coffee_evolve_noalloc(const coffee_params* p, int semantics,
   FlatLaunch launch;
   rc = flat_plan<float>(&env, semantics, &launch);
   if (rc) return rc;
+  // pair copies read 8-byte aligned element pairs: the caller's arrays must
+  // allow it (the scratch offsets are multiples of n, which is even then)
+  for (int f = 0; f < 7; ++f)
+    if (reinterpret_cast<uintptr_t>(fields[f]) % 8 != 0) launch.vec = false;
   EzConst<float> c;
   build_const<float>(&env, semantics, &c);
 

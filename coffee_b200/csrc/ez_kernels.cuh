@@ -197,24 +197,35 @@ __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7],
 
 // Per-thread table of the shared-memory slots and global offsets that a
 // CTA's threads copy for one (TX + 2H) x (TY + 2H) tile of one field plane.
-template <typename T, int TX, int TY, int H>
+// V = 1 copies one element per cp.async; V = 2 copies aligned pairs (8 bytes
+// in FP32), which needs an even row length d0: the copied row then starts at
+// the even column at or left of the tile's first column, `xoff` (0 or 1)
+// columns before it, and a row holds TX + 2H + 2 elements.
+template <typename T, int TX, int TY, int H, int V = 1>
 struct TileLoader {
-  static constexpr int SX = TX + 2 * H, SY = TY + 2 * H, PLANE = SX * SY, NT = TX * TY;
-  static constexpr int NLOAD = (PLANE + NT - 1) / NT;
-  static constexpr int FB = PLANE * (int)sizeof(T);  // bytes of one field plane
+  static_assert(V == 1 || V == 2, "one element or an aligned pair per copy");
+  static constexpr int SX = TX + 2 * H + (V == 2 ? 2 : 0);  // shared row stride (elements)
+  static constexpr int SY = TY + 2 * H, NT = TX * TY;
+  static constexpr int PER_ROW = SX / V;                    // copies per row
+  static constexpr int NCOPY = PER_ROW * SY;
+  static constexpr int NLOAD = (NCOPY + NT - 1) / NT;
+  static constexpr int FB = SX * SY * (int)sizeof(T);       // bytes of one field plane
   uint32_t sadd[NLOAD];   // shared byte address within slot 0, field 0
   long long goff[NLOAD];  // byte offset within a global plane
   bool lv[NLOAD];
+  int xoff;               // shared column of the tile's first column
 
   __device__ __forceinline__ TileLoader(const GridGeom& g, uint32_t sbase, int tid, int gx0,
                                         int gy0) {
+    xoff = (V == 2) ? (gx0 & 1) : 0;
+    const int xs = gx0 - xoff;
 #pragma unroll
     for (int m = 0; m < NLOAD; ++m) {
       const int e = tid + m * NT;
-      const int r = e / SX, cl = e - r * SX;
-      const int gx = gx0 + cl, gy = gy0 + r;
-      lv[m] = (e < PLANE) && gx < g.dims[0] && gy < g.dims[1];
-      sadd[m] = sbase + (uint32_t)(e * (int)sizeof(T));
+      const int r = e / PER_ROW, cl = (e - r * PER_ROW) * V;
+      const int gx = xs + cl, gy = gy0 + r;
+      lv[m] = (e < NCOPY) && gx + (V - 1) < g.dims[0] && gy < g.dims[1];
+      sadd[m] = sbase + (uint32_t)((r * SX + cl) * (int)sizeof(T));
       goff[m] = ((long long)gy * g.sy + gx) * (long long)sizeof(T);
     }
   }
@@ -228,7 +239,7 @@ struct TileLoader {
       const char* gb = reinterpret_cast<const char*>(uin.p[f]) + pb;
 #pragma unroll
       for (int m = 0; m < NLOAD; ++m)
-        if (lv[m]) cp_async<sizeof(T)>(sadd[m] + slot + (uint32_t)(f * FB), gb + goff[m]);
+        if (lv[m]) cp_async<sizeof(T) * V>(sadd[m] + slot + (uint32_t)(f * FB), gb + goff[m]);
     });
   }
 };
@@ -246,18 +257,18 @@ struct TileLoader {
 // Shared memory: a ring of 5 + PF planes of the 7 fields with a 2-point x/y
 // halo (z neighbours are read from the ring too), then PF + 1 planes of dU.
 // ---------------------------------------------------------------------------
-template <typename T, int TX, int TY, int PF>
+template <typename T, int TX, int TY, int PF, int V>
 constexpr size_t stage_smem_bytes(bool first) {
-  return (size_t)(5 + PF) * 7 * (TX + 4) * (TY + 4) * sizeof(T) +
+  return (size_t)(5 + PF) * 7 * TileLoader<T, TX, TY, 2, V>::FB +
          (first ? 0 : (size_t)(PF + 1) * 7 * TX * TY * sizeof(T));
 }
 
-template <typename T, int TX, int TY, int PF, bool FIRST, bool BC>
+template <typename T, int TX, int TY, int PF, bool FIRST, bool BC, int V>
 __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     ez_stage_kernel(const __grid_constant__ EzConst<T> c, const F7<const T> uin,
                     const F7<T> uout, const F7<T> du, const F7<T> un, const F5<T> aux,
                     const T As, const T Bs, const T tst, const int kchunk, const int flags) {
-  using L = TileLoader<T, TX, TY, 2>;
+  using L = TileLoader<T, TX, TY, 2, V>;
   constexpr int R = 5 + PF;
   constexpr int ES = (int)sizeof(T);
   constexpr int SX = L::SX, FB = L::FB, SB = 7 * FB;
@@ -307,7 +318,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
 
   const T six = c.inv_delta[0] / (T)12, siy = c.inv_delta[1] / (T)12,
           siz = c.inv_delta[2] / (T)12;
-  const uint32_t corner = sbase + (uint32_t)((ty * SX + tx) * ES);
+  const uint32_t corner = sbase + (uint32_t)((ty * SX + tx + loader.xoff) * ES);
 
 #pragma unroll 1
   for (int k = k0; k < k1; ++k) {
@@ -384,16 +395,16 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
 // planes k-3..k+3 per thread; shared memory keeps plane k (x/y neighbours)
 // and the arriving planes k+1..k+3+PF.
 // ---------------------------------------------------------------------------
-template <typename T, int TX, int TY, int PF>
+template <typename T, int TX, int TY, int PF, int V>
 constexpr size_t ko_smem_bytes() {
-  return (size_t)(4 + PF) * 7 * (TX + 6) * (TY + 6) * sizeof(T);
+  return (size_t)(4 + PF) * 7 * TileLoader<T, TX, TY, 3, V>::FB;
 }
 
-template <typename T, int TX, int TY, int PF, bool BC>
+template <typename T, int TX, int TY, int PF, bool BC, int V>
 __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     ez_ko_kernel(const __grid_constant__ EzConst<T> c, const F7<const T> uin,
                  const F7<T> uout, const T tko, const int kchunk) {
-  using L = TileLoader<T, TX, TY, 3>;
+  using L = TileLoader<T, TX, TY, 3, V>;
   constexpr int R = 4 + PF;
   constexpr int ES = (int)sizeof(T);
   constexpr int SX = L::SX, FB = L::FB, SB = 7 * FB;
@@ -430,7 +441,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
       for (int q = 0; q < 6; ++q) w[q][f] = uin.p[f][(long long)(k0 - 3 + q) * g.sz + own];
   }
   const bool ko_p = (c.semantics != SEM_CPU_REF);
-  const uint32_t corner = sbase + (uint32_t)((ty * SX + tx) * ES);
+  const uint32_t corner = sbase + (uint32_t)((ty * SX + tx + loader.xoff) * ES);
 #pragma unroll 1
   for (int k = k0; k < k1; ++k) {
     cp_async_wait<PF>();  // plane k+3 has landed

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 
@@ -19,6 +20,11 @@ struct coffee_env {
   coffee_params p;
   coffee_grid grid;
   int device;
+  // fields and solvers created on this environment keep it alive: it is
+  // deleted when it has been destroyed and the last of them is gone, in
+  // whatever order the host releases them
+  std::atomic<int> users{0};
+  std::atomic<bool> released{false};
 };
 
 namespace coffee {
@@ -28,7 +34,7 @@ template <typename T> struct Shape;
 // FP32 tile shapes; the defaults are the tuned values, the macros exist so
 // that a build can be made with other shapes to measure them.
 #ifndef COFFEE_F32_STY
-#define COFFEE_F32_STY 8
+#define COFFEE_F32_STY 16
 #endif
 #ifndef COFFEE_F32_SPF
 #define COFFEE_F32_SPF 1
@@ -48,15 +54,15 @@ template <> struct Shape<double> {
   static constexpr int KTX = 32, KTY = 4, KPF = 1;
 };
 
-template <typename T>
+template <typename T, int V>
 size_t stage_smem(bool first) {
   using S = Shape<T>;
-  return stage_smem_bytes<T, S::STX, S::STY, S::SPF>(first);
+  return stage_smem_bytes<T, S::STX, S::STY, S::SPF, V>(first);
 }
-template <typename T>
+template <typename T, int V>
 size_t ko_smem() {
   using S = Shape<T>;
-  return ko_smem_bytes<T, S::KTX, S::KTY, S::KPF>();
+  return ko_smem_bytes<T, S::KTX, S::KTY, S::KPF, V>();
 }
 
 // LSRK(5,4) coefficients of the reference (field_solver_EZ.cpp:1009-1014)
@@ -174,34 +180,36 @@ inline bool flat_needs_bc(const coffee_params& p, int semantics) {
 
 // Launch geometry of the flat kernels for one grid.
 struct FlatLaunch {
-  bool bc;
+  bool bc;   // star / absorbing-layer code compiled in
+  bool vec;  // planes copied as aligned element pairs (even row length d0)
   int kchunk_stage, kchunk_ko;
   dim3 grid_stage, grid_ko;
 };
 
-template <typename T, bool BC>
+template <typename T, bool BC, int V>
 struct FlatKernels {
   using S = Shape<T>;
-  static constexpr auto first = ez_stage_kernel<T, S::STX, S::STY, S::SPF, true, BC>;
-  static constexpr auto rest = ez_stage_kernel<T, S::STX, S::STY, S::SPF, false, BC>;
-  static constexpr auto ko = ez_ko_kernel<T, S::KTX, S::KTY, S::KPF, BC>;
+  static constexpr auto first = ez_stage_kernel<T, S::STX, S::STY, S::SPF, true, BC, V>;
+  static constexpr auto rest = ez_stage_kernel<T, S::STX, S::STY, S::SPF, false, BC, V>;
+  static constexpr auto ko = ez_ko_kernel<T, S::KTX, S::KTY, S::KPF, BC, V>;
 
   static cudaError_t set_attributes() {
     cudaError_t e = cudaFuncSetAttribute(first, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)stage_smem<T>(true));
+                                         (int)stage_smem<T, V>(true));
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(rest, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)stage_smem<T>(false));
+                               (int)stage_smem<T, V>(false));
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(ko, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)ko_smem<T>());
+                               (int)ko_smem<T, V>());
     return e;
   }
   static cudaError_t occupancy(int* stage, int* kop) {
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(stage, rest, S::STX * S::STY,
-                                                                  stage_smem<T>(false));
+                                                                  stage_smem<T, V>(false));
     if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(kop, ko, S::KTX * S::KTY, ko_smem<T>());
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(kop, ko, S::KTX * S::KTY,
+                                                        ko_smem<T, V>());
     return e;
   }
   static void stage(bool is_first, const FlatLaunch& L, cudaStream_t st, const EzConst<T>& c,
@@ -209,31 +217,45 @@ struct FlatKernels {
                     const F5<T>& aux, T As, T Bs, T tst, int flags) {
     const dim3 bs(S::STX, S::STY);
     if (is_first)
-      first<<<L.grid_stage, bs, stage_smem<T>(true), st>>>(c, src, dst, du, un, aux, As, Bs, tst,
-                                                           L.kchunk_stage, flags);
+      first<<<L.grid_stage, bs, stage_smem<T, V>(true), st>>>(c, src, dst, du, un, aux, As, Bs,
+                                                              tst, L.kchunk_stage, flags);
     else
-      rest<<<L.grid_stage, bs, stage_smem<T>(false), st>>>(c, src, dst, du, un, aux, As, Bs, tst,
-                                                           L.kchunk_stage, flags);
+      rest<<<L.grid_stage, bs, stage_smem<T, V>(false), st>>>(c, src, dst, du, un, aux, As, Bs,
+                                                              tst, L.kchunk_stage, flags);
   }
   static void ko_pass(const FlatLaunch& L, cudaStream_t st, const EzConst<T>& c,
                       const F7<const T>& src, const F7<T>& dst, T tko) {
-    ko<<<L.grid_ko, dim3(S::KTX, S::KTY), ko_smem<T>(), st>>>(c, src, dst, tko, L.kchunk_ko);
+    ko<<<L.grid_ko, dim3(S::KTX, S::KTY), ko_smem<T, V>(), st>>>(c, src, dst, tko, L.kchunk_ko);
   }
 };
+
+// Calls fn(FlatKernels<T, BC, V>{}) for the kernel set L selects.
+template <typename T, class Fn>
+inline void with_flat_kernels(const FlatLaunch& L, Fn&& fn) {
+  if (L.bc) {
+    if (L.vec) fn(FlatKernels<T, true, 2>{});
+    else fn(FlatKernels<T, true, 1>{});
+  } else {
+    if (L.vec) fn(FlatKernels<T, false, 2>{});
+    else fn(FlatKernels<T, false, 1>{});
+  }
+}
 
 // Set the shared-memory limits of every flat kernel of precision T on the
 // current device and plan the launch geometry of `env`'s grid.
 template <typename T>
 inline int flat_plan(const coffee_env* env, int semantics, FlatLaunch* L) {
   using S = Shape<T>;
-  COFFEE_CUDA_TRY((FlatKernels<T, true>::set_attributes()));
-  COFFEE_CUDA_TRY((FlatKernels<T, false>::set_attributes()));
+  COFFEE_CUDA_TRY((FlatKernels<T, true, 1>::set_attributes()));
+  COFFEE_CUDA_TRY((FlatKernels<T, false, 1>::set_attributes()));
+  COFFEE_CUDA_TRY((FlatKernels<T, true, 2>::set_attributes()));
+  COFFEE_CUDA_TRY((FlatKernels<T, false, 2>::set_attributes()));
   L->bc = flat_needs_bc(env->p, semantics);
+  L->vec = env->grid.dims[0] % 2 == 0;
   int per_sm_stage = 1, per_sm_ko = 1;
-  if (L->bc)
-    COFFEE_CUDA_TRY((FlatKernels<T, true>::occupancy(&per_sm_stage, &per_sm_ko)));
-  else
-    COFFEE_CUDA_TRY((FlatKernels<T, false>::occupancy(&per_sm_stage, &per_sm_ko)));
+  cudaError_t occ = cudaSuccess;
+  with_flat_kernels<T>(*L, [&](auto K) { occ = decltype(K)::occupancy(&per_sm_stage, &per_sm_ko); });
+  COFFEE_CUDA_TRY(occ);
   if (per_sm_stage < 1 || per_sm_ko < 1)
     return fail(COFFEE_E_CUDA, "stage/KO kernels cannot be resident (occupancy 0)");
   const int sms = num_sms(env->device);
@@ -281,12 +303,10 @@ inline int flat_steps(const EzConst<T>& c, const FlatLaunch& L, const F7<T>& A, 
         int rc = hook->before(kind);
         if (rc) return rc;
       }
-      if (L.bc)
-        FlatKernels<T, true>::stage(i == 0, L, st, c, srcc, dst, dU, Un, aux, (T)kAs[i],
-                                    (T)kBs[i], tst, flags);
-      else
-        FlatKernels<T, false>::stage(i == 0, L, st, c, srcc, dst, dU, Un, aux, (T)kAs[i],
-                                     (T)kBs[i], tst, flags);
+      with_flat_kernels<T>(L, [&](auto K) {
+        decltype(K)::stage(i == 0, L, st, c, srcc, dst, dU, Un, aux, (T)kAs[i], (T)kBs[i], tst,
+                           flags);
+      });
       COFFEE_CUDA_TRY(cudaGetLastError());
       if (hook) {
         int rc = hook->after(kind);
@@ -299,10 +319,7 @@ inline int flat_steps(const EzConst<T>& c, const FlatLaunch& L, const F7<T>& A, 
       int rc = hook->before(COFFEE_KERNEL_KO);
       if (rc) return rc;
     }
-    if (L.bc)
-      FlatKernels<T, true>::ko_pass(L, st, c, srcc, A, t + dt);
-    else
-      FlatKernels<T, false>::ko_pass(L, st, c, srcc, A, t + dt);
+    with_flat_kernels<T>(L, [&](auto K) { decltype(K)::ko_pass(L, st, c, srcc, A, t + dt); });
     COFFEE_CUDA_TRY(cudaGetLastError());
     if (hook) {
       int rc = hook->after(COFFEE_KERNEL_KO);

@@ -165,3 +165,29 @@ def test_turbulence512_properties():
     out2 = data2.download(("Ex", "By", "P"))
     for a, b in zip(out, out2):
         assert np.array_equal(a, b)
+
+
+def test_release_order_does_not_matter():
+    """The environment may be destroyed before the fields and solvers made on
+    it (as a garbage collector may do): they keep it alive, and no error of
+    the releases is left for the next call to report."""
+    p = problems.alfven_params(16)
+    f = problems.alfven_fields(p, np.float32)
+    env = SimEnvironment(p)
+    data = SimData(env, np.float32)
+    data.upload(f)
+    s = FieldSolverEZ(data, env, "cpu")
+    s.step(0.0, 1)
+    env.close()
+    s.close()
+    data.close()
+    p2 = problems.turbulence_params(32)
+    env2 = SimEnvironment(p2)
+    data2 = SimData(env2, np.float32)
+    data2.init_fourier((1.0, 0.0, 0.0), *problems.turbulence_modes())
+    s2 = FieldSolverEZ(data2, env2, "cpu")
+    s2.step(0.0, 1)
+    s2.check_finite()
+    s2.close()
+    data2.close()
+    env2.close()
