@@ -19,6 +19,13 @@ namespace coffee {
 
 enum AxiFlags { AX_LAST = 1, AX_AUX = 2, AX_WRITE_UN = 4 };
 
+// CTAs of 256 threads kept resident per SM (bounds the registers per thread;
+// the kernels are latency-bound on their stencil loads, so more warps help).
+#ifndef COFFEE_AXI_MIN_BLOCKS
+#define COFFEE_AXI_MIN_BLOCKS 4
+#endif
+constexpr int kAxiMinBlocks = COFFEE_AXI_MIN_BLOCKS;
+
 // ---- parameter block of the log-spherical solver ------------------------
 template <typename T>
 struct SphConst {
@@ -309,7 +316,7 @@ __device__ __forceinline__ void sph_stage_point(const SphConst<T>& c, const int 
 }
 
 template <typename T, bool FIRST>
-__global__ void __launch_bounds__(256) sph_stage_kernel(const __grid_constant__ SphConst<T> c,
+__global__ void __launch_bounds__(256, kAxiMinBlocks) sph_stage_kernel(const __grid_constant__ SphConst<T> c,
                                                         const F7<T> u, const F7<T> out,
                                                         const F7<T> du, const F7<T> un,
                                                         const F5<T> aux, const T As,
@@ -373,7 +380,7 @@ __device__ __forceinline__ void sph_ko_point(const SphConst<T>& c, const int i, 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) sph_ko_kernel(const __grid_constant__ SphConst<T> c,
+__global__ void __launch_bounds__(256, kAxiMinBlocks) sph_ko_kernel(const __grid_constant__ SphConst<T> c,
                                                      const F7<T> u, const F7<T> out,
                                                      const T tend) {
   const int i = c.lo0 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -467,7 +474,7 @@ __device__ __forceinline__ const SphBatchEntry<T>& sph_batch_entry(
 }
 
 template <typename T, bool FIRST>
-__global__ void __launch_bounds__(256) sph_stage_batch_kernel(
+__global__ void __launch_bounds__(256, kAxiMinBlocks) sph_stage_batch_kernel(
     const SphBatchEntry<T>* __restrict__ tab, const int n, const int to_b,
     const __grid_constant__ SphBatchTimes<T> tst, const T As, const T Bs, const int last) {
   __shared__ __align__(16) unsigned char buf[sizeof(SphBatchEntry<T>)];
@@ -484,7 +491,7 @@ __global__ void __launch_bounds__(256) sph_stage_batch_kernel(
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) sph_ko_batch_kernel(
+__global__ void __launch_bounds__(256, kAxiMinBlocks) sph_ko_batch_kernel(
     const SphBatchEntry<T>* __restrict__ tab, const int n,
     const __grid_constant__ SphBatchTimes<T> tend) {
   __shared__ __align__(16) unsigned char buf[sizeof(SphBatchEntry<T>)];
@@ -688,7 +695,7 @@ __device__ __forceinline__ void cyl_finish(const CylConst<T>& c, int i, int j, l
 // (field_solver_EZ_cylindrical.cu:143-234, 674-703).  The reference's
 // cylindrical stage writes no J / divE / divB.
 template <typename T, bool FIRST>
-__global__ void __launch_bounds__(256) cyl_stage_kernel(const __grid_constant__ CylConst<T> c,
+__global__ void __launch_bounds__(256, kAxiMinBlocks) cyl_stage_kernel(const __grid_constant__ CylConst<T> c,
                                                         const F7<T> u, const F7<T> out,
                                                         const F7<T> du, const F7<T> un,
                                                         const T As, const T Bs, const T tst,
@@ -755,7 +762,7 @@ __global__ void __launch_bounds__(256) cyl_stage_kernel(const __grid_constant__ 
 // _step2_thread, field_solver_EZ_cylindrical.cu:297-369; order of :705-712):
 // plain 6th differences in R and z, the clamps, then cyl_finish at t + dt.
 template <typename T>
-__global__ void __launch_bounds__(256) cyl_ko_kernel(const __grid_constant__ CylConst<T> c,
+__global__ void __launch_bounds__(256, kAxiMinBlocks) cyl_ko_kernel(const __grid_constant__ CylConst<T> c,
                                                      const F7<T> u, const F7<T> out,
                                                      const F7<T> un, const T tend) {
   const int i = c.lo0 + blockIdx.x * blockDim.x + threadIdx.x;

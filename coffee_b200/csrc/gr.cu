@@ -76,6 +76,7 @@ int gr_steps_t(const coffee_env* env, void* ehbuf, void* const A_[7], void* cons
   F7<T> eh;
   for (int k = 0; k < 6; ++k) eh.p[k] = static_cast<T*>(ehbuf) + k * n;
   eh.p[6] = nullptr;
+  const T* sgt = static_cast<const T*>(ehbuf) + 6 * n;  // sqrt(gamma), set up by gr_setup
   const dim3 gfull = grid_over(c.d[0], c.d[1], c.d[2]);
   const dim3 gbox = grid_over(c.hi[0] - c.lo[0], c.hi[1] - c.lo[1], c.hi[2] - c.lo[2]);
   for (int step = 0; step < nsteps; ++step) {
@@ -91,10 +92,10 @@ int gr_steps_t(const coffee_env* env, void* ehbuf, void* const A_[7], void* cons
       int rc = hook ? hook->before(kind) : COFFEE_OK;
       if (rc) return rc;
       if (s == 0)
-        gr_stage_kernel<T, true><<<gbox, kBlock, 0, st>>>(c, src, eh, dst, dU, Un, aux,
+        gr_stage_kernel<T, true><<<gbox, kBlock, 0, st>>>(c, src, eh, dst, dU, Un, aux, sgt,
                                                           (T)kAs[s], (T)kBs[s], flags);
       else
-        gr_stage_kernel<T, false><<<gbox, kBlock, 0, st>>>(c, src, eh, dst, dU, Un, aux,
+        gr_stage_kernel<T, false><<<gbox, kBlock, 0, st>>>(c, src, eh, dst, dU, Un, aux, sgt,
                                                            (T)kAs[s], (T)kBs[s], flags);
       COFFEE_CUDA_TRY(cudaGetLastError());
       if (hook && (rc = hook->after(kind))) return rc;
@@ -122,17 +123,38 @@ int gr_check(const coffee_env* env) {
   return COFFEE_OK;
 }
 
+namespace {
+template <typename T>
+int gr_fill_sqrt_gamma(const coffee_env* env, void* ehbuf) {
+  GrConst<T> c;
+  fill_gr_const<T>(env, &c);
+  const size_t n = (size_t)c.d[0] * c.d[1] * c.d[2];
+  gr_sqrt_gamma_kernel<T><<<grid_over(c.d[0], c.d[1], c.d[2]), kBlock>>>(
+      c, static_cast<T*>(ehbuf) + 6 * n);
+  COFFEE_CUDA_TRY(cudaGetLastError());
+  COFFEE_CUDA_TRY(cudaDeviceSynchronize());
+  return COFFEE_OK;
+}
+}  // namespace
+
+// Scratch of the GR solver: E and H (6 arrays) and the sqrt(gamma) table.
 int gr_setup(const coffee_env* env, int elem, void** ehbuf) {
   const coffee_grid& g = env->grid;
   const size_t n = (size_t)g.dims[0] * g.dims[1] * g.dims[2];
   *ehbuf = nullptr;
-  cudaError_t err = cudaMalloc(ehbuf, 6 * n * (size_t)elem);
+  cudaError_t err = cudaMalloc(ehbuf, 7 * n * (size_t)elem);
   if (err != cudaSuccess) {
     *ehbuf = nullptr;
-    return fail(COFFEE_E_NOMEM, "GR scratch (E, H) allocation failed: %s",
+    return fail(COFFEE_E_NOMEM, "GR scratch (E, H, sqrt(gamma)) allocation failed: %s",
                 cudaGetErrorString(err));
   }
-  return COFFEE_OK;
+  const int rc = elem == 4 ? gr_fill_sqrt_gamma<float>(env, *ehbuf)
+                           : gr_fill_sqrt_gamma<double>(env, *ehbuf);
+  if (rc) {
+    cudaFree(*ehbuf);
+    *ehbuf = nullptr;
+  }
+  return rc;
 }
 
 int gr_steps(const coffee_env* env, int elem, void* ehbuf, void* const A[7], void* const B[7],

@@ -112,6 +112,21 @@ __device__ __forceinline__ T gr_pos(const GrConst<T>& c, int a, int n) {
   return c.lower[a] + c.delta[a] * (T)(n - c.g[a]);
 }
 
+// sqrt(gamma) at every grid point, evaluated once per solver in FP64 and
+// rounded: the divergence stencil (div4, field_solver_gr_EZ.cu:44-86)
+// weights each neighbour by it.
+template <typename T>
+__global__ void gr_sqrt_gamma_kernel(const __grid_constant__ GrConst<T> c, T* sg) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= c.d[0] || j >= c.d[1] || k >= c.d[2]) return;
+  const long long o = i + (long long)c.d[0] * (j + (long long)c.d[1] * k);
+  const double x = (double)gr_pos(c, 0, i), y = (double)gr_pos(c, 1, j),
+               z = (double)gr_pos(c, 2, k);
+  sg[o] = (T)cks_sqrt_gamma<double>((double)c.a, x, y, z);
+}
+
 // E and H over the whole grid (kernel_compute_E_gr / kernel_compute_H_gr,
 // field_solver_gr_EZ.cu:88-186).  eh[0..2] = E, eh[3..5] = H.
 template <typename T>
@@ -209,8 +224,8 @@ __global__ void __launch_bounds__(256) gr_stage_kernel(const __grid_constant__ G
                                                        const F7<T> u, const F7<T> eh,
                                                        const F7<T> out, const F7<T> du,
                                                        const F7<T> un, const F5<T> aux,
-                                                       const T As, const T Bs,
-                                                       const int flags) {
+                                                       const T* __restrict__ sgt, const T As,
+                                                       const T Bs, const int flags) {
   const int i = c.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = c.lo[1] + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = c.lo[2] + blockIdx.z * blockDim.z + threadIdx.z;
@@ -233,21 +248,15 @@ __global__ void __launch_bounds__(256) gr_stage_kernel(const __grid_constant__ G
   const T rotE[3] = {(d1(eh.p[2], 1) - d1(eh.p[1], 2)) * igms,
                      (d1(eh.p[0], 2) - d1(eh.p[2], 0)) * igms,
                      (d1(eh.p[1], 0) - d1(eh.p[0], 1)) * igms};
-  // div4 (:44-86): sqrt(gamma) at the coordinates shifted by +-1, 2 delta
+  // div4 (:44-86): each neighbour weighted by sqrt(gamma) there (the
+  // per-solver table; the reference evaluates it at the shifted coordinates)
   T divD = T(0), divB = T(0);
   {
-    const T pos[3] = {x, y, z};
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
-      T w[4];
-      const T off[4] = {T(-2), T(-1), T(1), T(2)};
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        T p3[3] = {pos[0], pos[1], pos[2]};
-        p3[ax] = pos[ax] + off[q] * c.delta[ax];
-        w[q] = cks_sqrt_gamma(c.a, p3[0], p3[1], p3[2]);
-      }
       const long long s = st[ax];
+      const T w[4] = {__ldg(sgt + o - 2 * s), __ldg(sgt + o - s), __ldg(sgt + o + s),
+                      __ldg(sgt + o + 2 * s)};
       const T* fD = u.p[ax];
       const T* fB = u.p[3 + ax];
       divD += d1_4w(__ldg(fD + o - 2 * s) * w[0], __ldg(fD + o - s) * w[1],
