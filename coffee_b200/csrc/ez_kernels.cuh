@@ -254,12 +254,15 @@ struct TileLoader {
 //   U'  <- U + Bs dU
 //   U'  <- clamps, star boundary at tst, absorbing layer (ST_LAST)
 // reading U from `uin` and writing U' (with guard images) to `uout`.
-// Shared memory: a ring of 5 + PF planes of the 7 fields with a 2-point x/y
-// halo (z neighbours are read from the ring too), then PF + 1 planes of dU.
+// Shared memory: a ring of 3 + PF planes (k .. k+2, then the prefetch) of
+// the 7 fields with a 2-point x/y halo, then PF + 1 planes of dU.  The z
+// neighbours of a thread's own column are kept in a register window of
+// planes k-2 .. k+2: each plane is read from shared memory once, as the
+// window's leading plane.
 // ---------------------------------------------------------------------------
 template <typename T, int TX, int TY, int PF, int V>
 constexpr size_t stage_smem_bytes(bool first) {
-  return (size_t)(5 + PF) * 7 * TileLoader<T, TX, TY, 2, V>::FB +
+  return (size_t)(3 + PF) * 7 * TileLoader<T, TX, TY, 2, V>::FB +
          (first ? 0 : (size_t)(PF + 1) * 7 * TX * TY * sizeof(T));
 }
 
@@ -269,7 +272,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
                     const F7<T> uout, const F7<T> du, const F7<T> un, const F5<T> aux,
                     const T As, const T Bs, const T tst, const int kchunk, const int flags) {
   using L = TileLoader<T, TX, TY, 2, V>;
-  constexpr int R = 5 + PF;
+  constexpr int R = 3 + PF;
   constexpr int ES = (int)sizeof(T);
   constexpr int SX = L::SX, FB = L::FB, SB = 7 * FB;
   constexpr int NT = TX * TY, DFB = NT * ES, DSB = 7 * DFB;
@@ -314,11 +317,20 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     cp_async_commit();
   };
 #pragma unroll 1
-  for (int p = 0; p < R; ++p) issue(k0 - 2 + p);
+  for (int p = 0; p < R; ++p) issue(k0 + p);
 
   const T six = c.inv_delta[0] / (T)12, siy = c.inv_delta[1] / (T)12,
           siz = c.inv_delta[2] / (T)12;
   const uint32_t corner = sbase + (uint32_t)((ty * SX + tx + loader.xoff) * ES);
+  // w[q][f] = field f at (i, j, k - 2 + q): planes k-2 .. k+1 are carried
+  // from the previous plane, k+2 is read from the ring
+  T w[5][7];
+  if (active) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int f = 0; f < 7; ++f) w[q][f] = uin.p[f][(long long)(k0 - 2 + q) * g.sz + own];
+  }
 
 #pragma unroll 1
   for (int k = k0; k < k1; ++k) {
@@ -326,9 +338,6 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     __syncthreads();
     if (active) {
       const uint32_t a0 = corner + (uint32_t)((k % R) * SB);
-      const uint32_t am2 = corner + (uint32_t)(((k - 2) % R) * SB);
-      const uint32_t am1 = corner + (uint32_t)(((k - 1) % R) * SB);
-      const uint32_t ap1 = corner + (uint32_t)(((k + 1) % R) * SB);
       const uint32_t ap2 = corner + (uint32_t)(((k + 2) % R) * SB);
       // The stencil is consumed field group by field group (B, then E, then
       // P); the warp-level fence between groups keeps the shared loads of the
@@ -338,13 +347,13 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
       auto d1 = [&](auto fc, T* dxyz) {
         constexpr int f = decltype(fc)::value;
         constexpr int o = f * FB;
-        u[f] = lds<T, o + CEN>(a0);
         dxyz[0] = d1_4(lds<T, o + CEN - 2 * ES>(a0), lds<T, o + CEN - ES>(a0),
                        lds<T, o + CEN + ES>(a0), lds<T, o + CEN + 2 * ES>(a0), six);
         dxyz[1] = d1_4(lds<T, o + 2 * ES>(a0), lds<T, o + (SX + 2) * ES>(a0),
                        lds<T, o + (3 * SX + 2) * ES>(a0), lds<T, o + (4 * SX + 2) * ES>(a0), siy);
-        dxyz[2] = d1_4(lds<T, o + CEN>(am2), lds<T, o + CEN>(am1), lds<T, o + CEN>(ap1),
-                       lds<T, o + CEN>(ap2), siz);
+        w[4][f] = lds<T, o + CEN>(ap2);
+        u[f] = w[2][f];
+        dxyz[2] = d1_4(w[0][f], w[1][f], w[3][f], w[4][f], siz);
       };
       {
         T bxd[3], byd[3], bzd[3];
@@ -378,6 +387,10 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
       }
       stage_point<T, FIRST, BC>(c, u, dv, dold, As, Bs, tst, flags, col, k,
                             (long long)k * g.sz + own, du, un, aux, uout);
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int f = 0; f < 7; ++f) w[q][f] = w[q + 1][f];
     }
     __syncthreads();
     issue(k + 3 + PF);
