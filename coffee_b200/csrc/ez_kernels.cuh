@@ -260,6 +260,25 @@ struct TileLoader {
 // planes k-2 .. k+2: each plane is read from shared memory once, as the
 // window's leading plane.
 // ---------------------------------------------------------------------------
+// z-loop unroll of the stage kernel: 5 (the window length, no register
+// moves) or 1 (one plane per iteration, window shifted by moves), chosen
+// separately for the instances without and with the boundary code (BC):
+// the five copies of the out-of-line boundary calls make the BC instance
+// spill, and it runs faster plane by plane.
+#ifndef COFFEE_STAGE_ZUNROLL
+#define COFFEE_STAGE_ZUNROLL 5
+#endif
+#ifndef COFFEE_STAGE_ZUNROLL_BC
+#define COFFEE_STAGE_ZUNROLL_BC 1
+#endif
+template <bool BC>
+__host__ __device__ constexpr int stage_zunroll() {
+  return BC ? COFFEE_STAGE_ZUNROLL_BC : COFFEE_STAGE_ZUNROLL;
+}
+static_assert((stage_zunroll<false>() == 1 || stage_zunroll<false>() == 5) &&
+                  (stage_zunroll<true>() == 1 || stage_zunroll<true>() == 5),
+              "stage z unroll is 1 or 5");
+
 template <typename T, int TX, int TY, int PF, int V>
 constexpr size_t stage_smem_bytes(bool first) {
   return (size_t)(3 + PF) * 7 * TileLoader<T, TX, TY, 2, V>::FB +
@@ -273,6 +292,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
                     const T As, const T Bs, const T tst, const int kchunk, const int flags) {
   using L = TileLoader<T, TX, TY, 2, V>;
   constexpr int R = 3 + PF;
+  constexpr int ZU = stage_zunroll<BC>();
   constexpr int ES = (int)sizeof(T);
   constexpr int SX = L::SX, FB = L::FB, SB = 7 * FB;
   constexpr int NT = TX * TY, DFB = NT * ES, DSB = 7 * DFB;
@@ -322,8 +342,11 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
   const T six = c.inv_delta[0] / (T)12, siy = c.inv_delta[1] / (T)12,
           siz = c.inv_delta[2] / (T)12;
   const uint32_t corner = sbase + (uint32_t)((ty * SX + tx + loader.xoff) * ES);
-  // w[q][f] = field f at (i, j, k - 2 + q): planes k-2 .. k+1 are carried
-  // from the previous plane, k+2 is read from the ring
+  // Register window: in window phase S, w[(S + q) % 5][f] = field f at
+  // (i, j, k - 2 + q).  Planes k-2 .. k+1 are carried from the previous
+  // plane and k+2 is read from the ring into the slot of the dead plane k-3,
+  // so advancing the window moves no registers when the z loop is unrolled
+  // by the window length (ZU = 5).
   T w[5][7];
   if (active) {
 #pragma unroll
@@ -332,11 +355,11 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
       for (int f = 0; f < 7; ++f) w[q][f] = uin.p[f][(long long)(k0 - 2 + q) * g.sz + own];
   }
 
-#pragma unroll 1
-  for (int k = k0; k < k1; ++k) {
+  auto plane = [&](auto sc, const int k) {
+    constexpr int S = decltype(sc)::value;
     cp_async_wait<PF>();
     __syncthreads();
-    if (active) {
+    if (active && k < k1) {
       const uint32_t a0 = corner + (uint32_t)((k % R) * SB);
       const uint32_t ap2 = corner + (uint32_t)(((k + 2) % R) * SB);
       // The stencil is consumed field group by field group (B, then E, then
@@ -351,9 +374,10 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
                        lds<T, o + CEN + ES>(a0), lds<T, o + CEN + 2 * ES>(a0), six);
         dxyz[1] = d1_4(lds<T, o + 2 * ES>(a0), lds<T, o + (SX + 2) * ES>(a0),
                        lds<T, o + (3 * SX + 2) * ES>(a0), lds<T, o + (4 * SX + 2) * ES>(a0), siy);
-        w[4][f] = lds<T, o + CEN>(ap2);
-        u[f] = w[2][f];
-        dxyz[2] = d1_4(w[0][f], w[1][f], w[3][f], w[4][f], siz);
+        w[(S + 4) % 5][f] = lds<T, o + CEN>(ap2);
+        u[f] = w[(S + 2) % 5][f];
+        dxyz[2] = d1_4(w[S % 5][f], w[(S + 1) % 5][f], w[(S + 3) % 5][f], w[(S + 4) % 5][f],
+                       siz);
       };
       {
         T bxd[3], byd[3], bzd[3];
@@ -386,14 +410,32 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
         });
       }
       stage_point<T, FIRST, BC>(c, u, dv, dold, As, Bs, tst, flags, col, k,
-                            (long long)k * g.sz + own, du, un, aux, uout);
+                                (long long)k * g.sz + own, du, un, aux, uout);
+      if constexpr (ZU == 1) {
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
+        for (int q = 0; q < 4; ++q)
 #pragma unroll
-        for (int f = 0; f < 7; ++f) w[q][f] = w[q + 1][f];
+          for (int f = 0; f < 7; ++f) w[q][f] = w[q + 1][f];
+      }
     }
     __syncthreads();
     issue(k + 3 + PF);
+  };
+  if constexpr (ZU == 5) {
+    // planes past k1 in the last group only wait, synchronise and commit
+    // empty copy groups (issue() copies nothing past kend), so the ring's
+    // group accounting stays the same as plane-by-plane
+#pragma unroll 1
+    for (int k = k0; k < k1; k += 5) {
+      plane(std::integral_constant<int, 0>{}, k);
+      plane(std::integral_constant<int, 1>{}, k + 1);
+      plane(std::integral_constant<int, 2>{}, k + 2);
+      plane(std::integral_constant<int, 3>{}, k + 3);
+      plane(std::integral_constant<int, 4>{}, k + 4);
+    }
+  } else {
+#pragma unroll 1
+    for (int k = k0; k < k1; ++k) plane(std::integral_constant<int, 0>{}, k);
   }
   cp_async_wait<0>();
 }
@@ -408,6 +450,25 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
 // planes k-3..k+3 per thread; shared memory keeps plane k (x/y neighbours)
 // and the arriving planes k+1..k+3+PF.
 // ---------------------------------------------------------------------------
+// z-loop unroll of the KO kernel: 7 (the window length, no register moves)
+// or 1 (one plane per iteration, window shifted by moves), per instance as
+// measured: the instance without boundary code is faster plane by plane, the
+// one with it (whose window moves compete with the boundary calls for
+// registers) unrolled.
+#ifndef COFFEE_KO_ZUNROLL
+#define COFFEE_KO_ZUNROLL 1
+#endif
+#ifndef COFFEE_KO_ZUNROLL_BC
+#define COFFEE_KO_ZUNROLL_BC 7
+#endif
+template <bool BC>
+__host__ __device__ constexpr int ko_zunroll() {
+  return BC ? COFFEE_KO_ZUNROLL_BC : COFFEE_KO_ZUNROLL;
+}
+static_assert((ko_zunroll<false>() == 1 || ko_zunroll<false>() == 7) &&
+                  (ko_zunroll<true>() == 1 || ko_zunroll<true>() == 7),
+              "KO z unroll is 1 or 7");
+
 template <typename T, int TX, int TY, int PF, int V>
 constexpr size_t ko_smem_bytes() {
   return (size_t)(4 + PF) * 7 * TileLoader<T, TX, TY, 3, V>::FB;
@@ -419,6 +480,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
                  const F7<T> uout, const T tko, const int kchunk) {
   using L = TileLoader<T, TX, TY, 3, V>;
   constexpr int R = 4 + PF;
+  constexpr int ZU = ko_zunroll<BC>();
   constexpr int ES = (int)sizeof(T);
   constexpr int SX = L::SX, FB = L::FB, SB = 7 * FB;
   constexpr int CEN = (3 * SX + 3) * ES;  // own point, from the corner of its 7x7 patch
@@ -445,7 +507,10 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
 #pragma unroll 1
   for (int p = 0; p < R; ++p) issue(k0 + p);
 
-  // w[q][f] = field f at (i, j, k - 3 + q); q = 0..5 carried, 6 read each plane
+  // Register window: in window phase S, w[(S + q) % 7][f] = field f at
+  // (i, j, k - 3 + q); planes k-3 .. k+2 are carried, k+3 is read from the
+  // ring into the slot of the dead plane k-4 (no register moves when the z
+  // loop is unrolled by the window length, ZU = 7).
   T w[7][7];
   if (active) {
 #pragma unroll
@@ -455,19 +520,19 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
   }
   const bool ko_p = (c.semantics != SEM_CPU_REF);
   const uint32_t corner = sbase + (uint32_t)((ty * SX + tx + loader.xoff) * ES);
-#pragma unroll 1
-  for (int k = k0; k < k1; ++k) {
+  auto plane = [&](auto sc, const int k) {
+    constexpr int S = decltype(sc)::value;
     cp_async_wait<PF>();  // plane k+3 has landed
     __syncthreads();
-    if (active) {
+    if (active && k < k1) {
       const uint32_t a0 = corner + (uint32_t)((k % R) * SB);
       const uint32_t a3 = corner + (uint32_t)(((k + 3) % R) * SB);
       T nu[7];
       static_for<7>([&](auto fc) {
         constexpr int f = decltype(fc)::value;
         constexpr int o = f * FB;
-        w[6][f] = lds<T, o + CEN>(a3);
-        const T cv = w[3][f];
+        w[(S + 6) % 7][f] = lds<T, o + CEN>(a3);
+        const T cv = w[(S + 3) % 7][f];
         if (f < 6 || ko_p) {
           const T kx = d6_2(lds<T, o + CEN - 3 * ES>(a0), lds<T, o + CEN - 2 * ES>(a0),
                             lds<T, o + CEN - ES>(a0), cv, lds<T, o + CEN + ES>(a0),
@@ -476,7 +541,8 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
                             lds<T, o + (2 * SX + 3) * ES>(a0), cv,
                             lds<T, o + (4 * SX + 3) * ES>(a0), lds<T, o + (5 * SX + 3) * ES>(a0),
                             lds<T, o + (6 * SX + 3) * ES>(a0));
-          const T kz = d6_2(w[0][f], w[1][f], w[2][f], cv, w[4][f], w[5][f], w[6][f]);
+          const T kz = d6_2(w[S % 7][f], w[(S + 1) % 7][f], w[(S + 2) % 7][f], cv,
+                            w[(S + 4) % 7][f], w[(S + 5) % 7][f], w[(S + 6) % 7][f]);
           nu[f] = fma(kx + ky + kz, c.ko_c, cv);
         } else {
           nu[f] = cv;
@@ -485,13 +551,32 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
       apply_clamps(c, nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
       if constexpr (BC) star_boundary(c, i, j, k, tko, nu);
       store_with_images(g, col, uout, k, (long long)k * g.sz + own, nu);
+      if constexpr (ZU == 1) {
 #pragma unroll
-      for (int q = 0; q < 6; ++q)
+        for (int q = 0; q < 6; ++q)
 #pragma unroll
-        for (int f = 0; f < 7; ++f) w[q][f] = w[q + 1][f];
+          for (int f = 0; f < 7; ++f) w[q][f] = w[q + 1][f];
+      }
     }
     __syncthreads();
     issue(k + R);
+  };
+  if constexpr (ZU == 7) {
+    // planes past k1 in the last group only wait, synchronise and commit
+    // empty copy groups (issue() copies nothing past kend)
+#pragma unroll 1
+    for (int k = k0; k < k1; k += 7) {
+      plane(std::integral_constant<int, 0>{}, k);
+      plane(std::integral_constant<int, 1>{}, k + 1);
+      plane(std::integral_constant<int, 2>{}, k + 2);
+      plane(std::integral_constant<int, 3>{}, k + 3);
+      plane(std::integral_constant<int, 4>{}, k + 4);
+      plane(std::integral_constant<int, 5>{}, k + 5);
+      plane(std::integral_constant<int, 6>{}, k + 6);
+    }
+  } else {
+#pragma unroll 1
+    for (int k = k0; k < k1; ++k) plane(std::integral_constant<int, 0>{}, k);
   }
   cp_async_wait<0>();
 }
