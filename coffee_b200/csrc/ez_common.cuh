@@ -64,6 +64,14 @@ __device__ __forceinline__ void cp_async(uint32_t dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(dst), "l"(src),
                "n"(BYTES));
 }
+// the same with a compile-time offset OFF added to the shared address
+template <int BYTES, int OFF>
+__device__ __forceinline__ void cp_async_off(uint32_t dst, const void* src) {
+  static_assert(BYTES == 4 || BYTES == 8 || BYTES == 16, "cp.async size");
+  static_assert(OFF >= 0, "offsets are measured from the slot base");
+  asm volatile("cp.async.ca.shared.global [%0+%3], [%1], %2;\n" ::"r"(dst), "l"(src),
+               "n"(BYTES), "n"(OFF));
+}
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;\n" ::);
 }

@@ -15,7 +15,9 @@
 // memory is addressed by 32-bit addresses with the field / neighbour offsets
 // as compile-time immediates (lds<T, OFF>), loops over the 7 fields are
 // unrolled at compile time (static_for), and the guard-image bookkeeping is
-// skipped for points that have no image.
+// skipped for points that have no image.  Global element offsets are 32-bit
+// (an array has fewer than 2^31 points: flat_plan checks it), so that every
+// global address is one wide multiply-add of an offset onto an array base.
 #pragma once
 
 #include "ez_physics.cuh"
@@ -55,7 +57,7 @@ __device__ __forceinline__ T d6_2(T m3, T m2, T m1, T c, T p1, T p2, T p3) {
 // point and at its periodic guard images.
 template <typename T>
 __device__ __forceinline__ void store_with_images(const GridGeom& g, const ColumnCtx<T>& col,
-                                                  const F7<T>& out, int k, long long o,
+                                                  const F7<T>& out, int k, uint32_t o,
                                                   const T u[7]) {
   if (col.xy_simple && only_self(g, 2, k)) {
 #pragma unroll
@@ -75,7 +77,8 @@ __device__ __forceinline__ void store_with_images(const GridGeom& g, const Colum
 #pragma unroll
       for (int a = 0; a < 2; ++a) {
         if (a >= nx) break;
-        const long long q = (long long)zs[cz] * g.sz + (long long)ys[b] * g.sy + xs[a];
+        const uint32_t q = (uint32_t)zs[cz] * (uint32_t)g.sz + (uint32_t)ys[b] * (uint32_t)g.sy +
+                           (uint32_t)xs[a];
 #pragma unroll
         for (int f = 0; f < 7; ++f) out.p[f][q] = u[f];
       }
@@ -101,7 +104,7 @@ __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7],
                                             const Derivs<T>& dv, const T dold[7],
                                             const T As, const T Bs, const T tst,
                                             const int flags, const ColumnCtx<T>& col,
-                                            const int k, const long long o, const F7<T>& du,
+                                            const int k, const uint32_t o, const F7<T>& du,
                                             const F7<T>& un, const F5<T>& aux,
                                             const F7<T>& uout) {
   const bool cpu = c.semantics == SEM_CPU_REF;
@@ -210,8 +213,8 @@ struct TileLoader {
   static constexpr int NCOPY = PER_ROW * SY;
   static constexpr int NLOAD = (NCOPY + NT - 1) / NT;
   static constexpr int FB = SX * SY * (int)sizeof(T);       // bytes of one field plane
-  uint32_t sadd[NLOAD];   // shared byte address within slot 0, field 0
-  long long goff[NLOAD];  // byte offset within a global plane
+  uint32_t sadd[NLOAD];  // shared byte address within slot 0, field 0
+  uint32_t eoff[NLOAD];  // element offset within a global plane
   bool lv[NLOAD];
   int xoff;               // shared column of the tile's first column
 
@@ -226,21 +229,23 @@ struct TileLoader {
       const int gx = xs + cl, gy = gy0 + r;
       lv[m] = (e < NCOPY) && gx + (V - 1) < g.dims[0] && gy < g.dims[1];
       sadd[m] = sbase + (uint32_t)((r * SX + cl) * (int)sizeof(T));
-      goff[m] = ((long long)gy * g.sy + gx) * (long long)sizeof(T);
+      eoff[m] = (uint32_t)gy * (uint32_t)g.sy + (uint32_t)gx;
     }
   }
 
-  // Copy one plane (byte offset pb into each field array) of the 7 fields
-  // into the ring slot at byte offset `slot`.
-  __device__ __forceinline__ void copy(const F7<const T>& uin, long long pb,
+  // Copy one plane (element offset pe into each field array) of the 7
+  // fields into the ring slot at byte offset `slot`.
+  __device__ __forceinline__ void copy(const F7<const T>& uin, uint32_t pe,
                                        uint32_t slot) const {
-    static_for<7>([&](auto fc) {
-      constexpr int f = decltype(fc)::value;
-      const char* gb = reinterpret_cast<const char*>(uin.p[f]) + pb;
 #pragma unroll
-      for (int m = 0; m < NLOAD; ++m)
-        if (lv[m]) cp_async<sizeof(T) * V>(sadd[m] + slot + (uint32_t)(f * FB), gb + goff[m]);
-    });
+    for (int m = 0; m < NLOAD; ++m) {
+      if (!lv[m]) continue;
+      const uint32_t e = pe + eoff[m], d = sadd[m] + slot;
+      static_for<7>([&](auto fc) {
+        constexpr int f = decltype(fc)::value;
+        cp_async_off<sizeof(T) * V, f * FB>(d, uin.p[f] + e);
+      });
+    }
   }
 };
 
@@ -254,8 +259,9 @@ struct TileLoader {
 //   U'  <- U + Bs dU
 //   U'  <- clamps, star boundary at tst, absorbing layer (ST_LAST)
 // reading U from `uin` and writing U' (with guard images) to `uout`.
-// Shared memory: a ring of 3 + PF planes (k .. k+2, then the prefetch) of
-// the 7 fields with a 2-point x/y halo, then PF + 1 planes of dU.  The z
+// Shared memory: a ring of 3 + PF + kRingSpare planes (k .. k+2, the
+// prefetch, the spare) of the 7 fields with a 2-point x/y halo, then
+// PF + 1 + kRingSpare planes of dU.  The z
 // neighbours of a thread's own column are kept in a register window of
 // planes k-2 .. k+2: each plane is read from shared memory once, as the
 // window's leading plane.
@@ -279,10 +285,27 @@ static_assert((stage_zunroll<false>() == 1 || stage_zunroll<false>() == 5) &&
                   (stage_zunroll<true>() == 1 || stage_zunroll<true>() == 5),
               "stage z unroll is 1 or 5");
 
+// Spare ring slots (0 or 1) of the stage and KO kernels.  With a spare slot
+// the copies of a new plane are issued right after the one barrier at the
+// top of an iteration, into the slot of the plane the previous iteration
+// finished with; without it they wait for a second barrier after the
+// iteration's arithmetic.  Measured at 512^3: the stage kernel is faster with
+// the spare slot, the KO kernel (two CTAs per SM) without.
+#ifndef COFFEE_STAGE_RING_SPARE
+#define COFFEE_STAGE_RING_SPARE 1
+#endif
+#ifndef COFFEE_KO_RING_SPARE
+#define COFFEE_KO_RING_SPARE 0
+#endif
+constexpr int kRingSpare = COFFEE_STAGE_RING_SPARE;
+constexpr int kKoRingSpare = COFFEE_KO_RING_SPARE;
+static_assert((kRingSpare == 0 || kRingSpare == 1) && (kKoRingSpare == 0 || kKoRingSpare == 1),
+              "0 or 1 spare ring slot");
+
 template <typename T, int TX, int TY, int PF, int V>
 constexpr size_t stage_smem_bytes(bool first) {
-  return (size_t)(3 + PF) * 7 * TileLoader<T, TX, TY, 2, V>::FB +
-         (first ? 0 : (size_t)(PF + 1) * 7 * TX * TY * sizeof(T));
+  return (size_t)(3 + PF + kRingSpare) * 7 * TileLoader<T, TX, TY, 2, V>::FB +
+         (first ? 0 : (size_t)(PF + 1 + kRingSpare) * 7 * TX * TY * sizeof(T));
 }
 
 template <typename T, int TX, int TY, int PF, bool FIRST, bool BC, int V>
@@ -291,7 +314,8 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
                     const F7<T> uout, const F7<T> du, const F7<T> un, const F5<T> aux,
                     const T As, const T Bs, const T tst, const int kchunk, const int flags) {
   using L = TileLoader<T, TX, TY, 2, V>;
-  constexpr int R = 3 + PF;
+  constexpr int R = 3 + PF + kRingSpare;   // field ring slots
+  constexpr int DR = PF + 1 + kRingSpare;  // dU ring slots
   constexpr int ZU = stage_zunroll<BC>();
   constexpr int ES = (int)sizeof(T);
   constexpr int SX = L::SX, FB = L::FB, SB = 7 * FB;
@@ -312,32 +336,31 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
   // groups below are executed by these lanes only (a tile that overhangs
   // the grid has idle lanes, which must not be named in the mask)
   const unsigned amask = __ballot_sync(0xffffffffu, active);
-  const long long own = (long long)j * g.sy + i;
+  const uint32_t sz = (uint32_t)g.sz;
+  const uint32_t own = (uint32_t)j * (uint32_t)g.sy + (uint32_t)i;
   const ColumnCtx<T> col = make_column(c, i, j);
   const L loader(g, sbase, tid, g.lo[0] + (int)blockIdx.x * TX - 2,
                  g.lo[1] + (int)blockIdx.y * TY - 2);
-  const long long pbytes = g.sz * ES;
   const uint32_t dme = dbase + (uint32_t)(tid * ES);
-  const long long own_b = own * ES;
   const int kend = k1 + 2;  // planes [k0-2, k1+2) are read
 
   auto issue = [&](int kp) {
-    if (kp < kend) loader.copy(uin, kp * pbytes, (uint32_t)((kp % R) * SB));
+    if (kp < kend) loader.copy(uin, (uint32_t)kp * sz, (uint32_t)((kp % R) * SB));
     if constexpr (!FIRST) {
       const int kd = kp - 2;
       if (kd >= k0 && kd < k1 && active) {
-        const uint32_t ds = dme + (uint32_t)((kd % (PF + 1)) * DSB);
-        const long long pb = kd * pbytes + own_b;
+        const uint32_t ds = dme + (uint32_t)((kd % DR) * DSB);
+        const uint32_t e = (uint32_t)kd * sz + own;
         static_for<7>([&](auto fc) {
           constexpr int f = decltype(fc)::value;
-          cp_async<sizeof(T)>(ds + f * DFB, reinterpret_cast<const char*>(du.p[f]) + pb);
+          cp_async_off<sizeof(T), f * DFB>(ds, du.p[f] + e);
         });
       }
     }
     cp_async_commit();
   };
 #pragma unroll 1
-  for (int p = 0; p < R; ++p) issue(k0 + p);
+  for (int p = 0; p < 3 + PF; ++p) issue(k0 + p);
 
   const T six = c.inv_delta[0] / (T)12, siy = c.inv_delta[1] / (T)12,
           siz = c.inv_delta[2] / (T)12;
@@ -352,13 +375,14 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
 #pragma unroll
     for (int q = 0; q < 4; ++q)
 #pragma unroll
-      for (int f = 0; f < 7; ++f) w[q][f] = uin.p[f][(long long)(k0 - 2 + q) * g.sz + own];
+      for (int f = 0; f < 7; ++f) w[q][f] = uin.p[f][(uint32_t)(k0 - 2 + q) * sz + own];
   }
 
   auto plane = [&](auto sc, const int k) {
     constexpr int S = decltype(sc)::value;
-    cp_async_wait<PF>();
+    cp_async_wait<PF>();  // planes up to k+2 (and the dU of k) have landed
     __syncthreads();
+    if constexpr (kRingSpare == 1) issue(k + 3 + PF);  // into the slot of plane k-1
     if (active && k < k1) {
       const uint32_t a0 = corner + (uint32_t)((k % R) * SB);
       const uint32_t ap2 = corner + (uint32_t)(((k + 2) % R) * SB);
@@ -403,14 +427,14 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
       __syncwarp(amask);
       d1(std::integral_constant<int, 6>{}, dv.gradP);
       if constexpr (!FIRST) {
-        const uint32_t ad = dme + (uint32_t)((k % (PF + 1)) * DSB);
+        const uint32_t ad = dme + (uint32_t)((k % DR) * DSB);
         static_for<7>([&](auto fc) {
           constexpr int f = decltype(fc)::value;
           dold[f] = lds<T, f * DFB>(ad);
         });
       }
       stage_point<T, FIRST, BC>(c, u, dv, dold, As, Bs, tst, flags, col, k,
-                                (long long)k * g.sz + own, du, un, aux, uout);
+                                (uint32_t)k * sz + own, du, un, aux, uout);
       if constexpr (ZU == 1) {
 #pragma unroll
         for (int q = 0; q < 4; ++q)
@@ -418,8 +442,10 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
           for (int f = 0; f < 7; ++f) w[q][f] = w[q + 1][f];
       }
     }
-    __syncthreads();
-    issue(k + 3 + PF);
+    if constexpr (kRingSpare == 0) {
+      __syncthreads();
+      issue(k + 3 + PF);  // into the slot of plane k
+    }
   };
   if constexpr (ZU == 5) {
     // planes past k1 in the last group only wait, synchronise and commit
@@ -451,12 +477,10 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
 // and the arriving planes k+1..k+3+PF.
 // ---------------------------------------------------------------------------
 // z-loop unroll of the KO kernel: 7 (the window length, no register moves)
-// or 1 (one plane per iteration, window shifted by moves), per instance as
-// measured: the instance without boundary code is faster plane by plane, the
-// one with it (whose window moves compete with the boundary calls for
-// registers) unrolled.
+// or 1 (one plane per iteration, window shifted by moves), per instance
+// (with and without the boundary code); both are faster unrolled.
 #ifndef COFFEE_KO_ZUNROLL
-#define COFFEE_KO_ZUNROLL 1
+#define COFFEE_KO_ZUNROLL 7
 #endif
 #ifndef COFFEE_KO_ZUNROLL_BC
 #define COFFEE_KO_ZUNROLL_BC 7
@@ -471,7 +495,7 @@ static_assert((ko_zunroll<false>() == 1 || ko_zunroll<false>() == 7) &&
 
 template <typename T, int TX, int TY, int PF, int V>
 constexpr size_t ko_smem_bytes() {
-  return (size_t)(4 + PF) * 7 * TileLoader<T, TX, TY, 3, V>::FB;
+  return (size_t)(4 + PF + kKoRingSpare) * 7 * TileLoader<T, TX, TY, 3, V>::FB;
 }
 
 template <typename T, int TX, int TY, int PF, bool BC, int V>
@@ -479,7 +503,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     ez_ko_kernel(const __grid_constant__ EzConst<T> c, const F7<const T> uin,
                  const F7<T> uout, const T tko, const int kchunk) {
   using L = TileLoader<T, TX, TY, 3, V>;
-  constexpr int R = 4 + PF;
+  constexpr int R = 4 + PF + kKoRingSpare;
   constexpr int ZU = ko_zunroll<BC>();
   constexpr int ES = (int)sizeof(T);
   constexpr int SX = L::SX, FB = L::FB, SB = 7 * FB;
@@ -494,18 +518,18 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
   const int k0 = g.lo[2] + blockIdx.z * kchunk;
   const int k1 = min(k0 + kchunk, g.hi[2]);
   const bool active = (i < g.hi[0]) && (j < g.hi[1]);
-  const long long own = (long long)j * g.sy + i;
+  const uint32_t sz = (uint32_t)g.sz;
+  const uint32_t own = (uint32_t)j * (uint32_t)g.sy + (uint32_t)i;
   const ColumnCtx<T> col = make_column(c, i, j);
   const L loader(g, sbase, tid, g.lo[0] + (int)blockIdx.x * TX - 3,
                  g.lo[1] + (int)blockIdx.y * TY - 3);
-  const long long pbytes = g.sz * ES;
   const int kend = k1 + 3;  // planes [k0, k1+3) pass through shared memory
   auto issue = [&](int kp) {
-    if (kp < kend) loader.copy(uin, kp * pbytes, (uint32_t)((kp % R) * SB));
+    if (kp < kend) loader.copy(uin, (uint32_t)kp * sz, (uint32_t)((kp % R) * SB));
     cp_async_commit();
   };
 #pragma unroll 1
-  for (int p = 0; p < R; ++p) issue(k0 + p);
+  for (int p = 0; p < 4 + PF; ++p) issue(k0 + p);
 
   // Register window: in window phase S, w[(S + q) % 7][f] = field f at
   // (i, j, k - 3 + q); planes k-3 .. k+2 are carried, k+3 is read from the
@@ -516,7 +540,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
 #pragma unroll
     for (int f = 0; f < 7; ++f)
 #pragma unroll
-      for (int q = 0; q < 6; ++q) w[q][f] = uin.p[f][(long long)(k0 - 3 + q) * g.sz + own];
+      for (int q = 0; q < 6; ++q) w[q][f] = uin.p[f][(uint32_t)(k0 - 3 + q) * sz + own];
   }
   const bool ko_p = (c.semantics != SEM_CPU_REF);
   const uint32_t corner = sbase + (uint32_t)((ty * SX + tx + loader.xoff) * ES);
@@ -524,6 +548,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     constexpr int S = decltype(sc)::value;
     cp_async_wait<PF>();  // plane k+3 has landed
     __syncthreads();
+    if constexpr (kKoRingSpare == 1) issue(k + 4 + PF);  // into the slot of plane k-1
     if (active && k < k1) {
       const uint32_t a0 = corner + (uint32_t)((k % R) * SB);
       const uint32_t a3 = corner + (uint32_t)(((k + 3) % R) * SB);
@@ -550,7 +575,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
       });
       apply_clamps(c, nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
       if constexpr (BC) star_boundary(c, i, j, k, tko, nu);
-      store_with_images(g, col, uout, k, (long long)k * g.sz + own, nu);
+      store_with_images(g, col, uout, k, (uint32_t)k * sz + own, nu);
       if constexpr (ZU == 1) {
 #pragma unroll
         for (int q = 0; q < 6; ++q)
@@ -558,8 +583,10 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
           for (int f = 0; f < 7; ++f) w[q][f] = w[q + 1][f];
       }
     }
-    __syncthreads();
-    issue(k + R);
+    if constexpr (kKoRingSpare == 0) {
+      __syncthreads();
+      issue(k + 4 + PF);  // into the slot of plane k
+    }
   };
   if constexpr (ZU == 7) {
     // planes past k1 in the last group only wait, synchronise and commit

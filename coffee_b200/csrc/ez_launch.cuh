@@ -250,6 +250,14 @@ inline int flat_plan(const coffee_env* env, int semantics, FlatLaunch* L) {
   COFFEE_CUDA_TRY((FlatKernels<T, false, 1>::set_attributes()));
   COFFEE_CUDA_TRY((FlatKernels<T, true, 2>::set_attributes()));
   COFFEE_CUDA_TRY((FlatKernels<T, false, 2>::set_attributes()));
+  // the flat kernels index an array with 32-bit element offsets (an FP32
+  // array of 2^31 points alone would take a twentieth of the GPU's memory,
+  // and a run holds at least 21 of them)
+  const long long npts =
+      (long long)env->grid.dims[0] * env->grid.dims[1] * (long long)env->grid.dims[2];
+  if (npts >= (1LL << 31))
+    return fail(COFFEE_E_CONFIG, "%lld points per array: the flat solver takes fewer than 2^31",
+                npts);
   L->bc = flat_needs_bc(env->p, semantics);
   L->vec = env->grid.dims[0] % 2 == 0;
   int per_sm_stage = 1, per_sm_ko = 1;
