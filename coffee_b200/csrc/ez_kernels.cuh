@@ -302,10 +302,26 @@ constexpr int kKoRingSpare = COFFEE_KO_RING_SPARE;
 static_assert((kRingSpare == 0 || kRingSpare == 1) && (kKoRingSpare == 0 || kKoRingSpare == 1),
               "0 or 1 spare ring slot");
 
-template <typename T, int TX, int TY, int PF, int V>
+// Ring slots of the stage kernel.  Plane k lives in slot (k - lo[2]) % R of
+// the field ring and its dU in slot (k - lo[2]) % DR of the dU ring.  With
+// PF = 1 and the spare slot the field ring has 5 slots, the z unroll length:
+// every chunk then starts a multiple of 5 planes from lo[2] (the host picks
+// such chunks) and the field slot of every plane an unrolled iteration
+// touches is a compile-time constant.  (Rings grown to make the dU slots
+// constant too measured slower: shared memory taken from the L1 cache.)
+template <bool BC, int PF>
+__host__ __device__ constexpr int stage_ring() {
+  return 3 + PF + kRingSpare;
+}
+template <bool BC, int PF>
+__host__ __device__ constexpr int stage_dring() {
+  return PF + 1 + kRingSpare;
+}
+
+template <typename T, int TX, int TY, int PF, int V, bool BC>
 constexpr size_t stage_smem_bytes(bool first) {
-  return (size_t)(3 + PF + kRingSpare) * 7 * TileLoader<T, TX, TY, 2, V>::FB +
-         (first ? 0 : (size_t)(PF + 1 + kRingSpare) * 7 * TX * TY * sizeof(T));
+  return (size_t)stage_ring<BC, PF>() * 7 * TileLoader<T, TX, TY, 2, V>::FB +
+         (first ? 0 : (size_t)stage_dring<BC, PF>() * 7 * TX * TY * sizeof(T));
 }
 
 template <typename T, int TX, int TY, int PF, bool FIRST, bool BC, int V>
@@ -314,9 +330,10 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
                     const F7<T> uout, const F7<T> du, const F7<T> un, const F5<T> aux,
                     const T As, const T Bs, const T tst, const int kchunk, const int flags) {
   using L = TileLoader<T, TX, TY, 2, V>;
-  constexpr int R = 3 + PF + kRingSpare;   // field ring slots
-  constexpr int DR = PF + 1 + kRingSpare;  // dU ring slots
+  constexpr int R = stage_ring<BC, PF>();    // field ring slots
+  constexpr int DR = stage_dring<BC, PF>();  // dU ring slots
   constexpr int ZU = stage_zunroll<BC>();
+
   constexpr int ES = (int)sizeof(T);
   constexpr int SX = L::SX, FB = L::FB, SB = 7 * FB;
   constexpr int NT = TX * TY, DFB = NT * ES, DSB = 7 * DFB;
@@ -343,13 +360,28 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
                  g.lo[1] + (int)blockIdx.y * TY - 2);
   const uint32_t dme = dbase + (uint32_t)(tid * ES);
   const int kend = k1 + 2;  // planes [k0-2, k1+2) are read
+  const int lo2 = g.lo[2];
+  // byte offsets of the ring slots of plane k + OFF in window phase S:
+  // compile-time constants in the unrolled loop
+  auto fslot = [&](auto sc, auto oc, int k) -> uint32_t {
+    constexpr int S = decltype(sc)::value, OFF = decltype(oc)::value;
+    if constexpr (ZU == R) return (uint32_t)(((S + OFF) % R) * SB);
+    else return (uint32_t)(((k + OFF - lo2) % R) * SB);
+  };
+  auto dslot = [&](auto sc, auto oc, int k) -> uint32_t {
+    constexpr int S = decltype(sc)::value, OFF = decltype(oc)::value;
+    if constexpr (ZU == DR) return (uint32_t)(((S + OFF) % DR) * DSB);
+    else return (uint32_t)(((k + OFF - lo2) % DR) * DSB);
+  };
 
-  auto issue = [&](int kp) {
-    if (kp < kend) loader.copy(uin, (uint32_t)kp * sz, (uint32_t)((kp % R) * SB));
+  // copy plane kp into field slot fs and the dU of plane kp - 2 into dU
+  // slot ds
+  auto issue = [&](int kp, uint32_t fs, uint32_t dsl) {
+    if (kp < kend) loader.copy(uin, (uint32_t)kp * sz, fs);
     if constexpr (!FIRST) {
       const int kd = kp - 2;
       if (kd >= k0 && kd < k1 && active) {
-        const uint32_t ds = dme + (uint32_t)((kd % DR) * DSB);
+        const uint32_t ds = dme + dsl;
         const uint32_t e = (uint32_t)kd * sz + own;
         static_for<7>([&](auto fc) {
           constexpr int f = decltype(fc)::value;
@@ -360,7 +392,9 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     cp_async_commit();
   };
 #pragma unroll 1
-  for (int p = 0; p < 3 + PF; ++p) issue(k0 + p);
+  for (int p = 0; p < 3 + PF; ++p)
+    issue(k0 + p, (uint32_t)(((k0 + p - lo2) % R) * SB),
+          (uint32_t)((((k0 + p - 2 - lo2) % DR + DR) % DR) * DSB));
 
   const T six = c.inv_delta[0] / (T)12, siy = c.inv_delta[1] / (T)12,
           siz = c.inv_delta[2] / (T)12;
@@ -382,10 +416,15 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     constexpr int S = decltype(sc)::value;
     cp_async_wait<PF>();  // planes up to k+2 (and the dU of k) have landed
     __syncthreads();
-    if constexpr (kRingSpare == 1) issue(k + 3 + PF);  // into the slot of plane k-1
+    using Z = std::integral_constant<int, 0>;
+    using P2 = std::integral_constant<int, 2>;
+    using PN = std::integral_constant<int, 3 + PF>;   // the plane issued now
+    using PD = std::integral_constant<int, 1 + PF>;   // and its dU plane
+    if constexpr (kRingSpare == 1)  // into the slot of plane k-1
+      issue(k + 3 + PF, fslot(sc, PN{}, k), dslot(sc, PD{}, k));
     if (active && k < k1) {
-      const uint32_t a0 = corner + (uint32_t)((k % R) * SB);
-      const uint32_t ap2 = corner + (uint32_t)(((k + 2) % R) * SB);
+      const uint32_t a0 = corner + fslot(sc, Z{}, k);
+      const uint32_t ap2 = corner + fslot(sc, P2{}, k);
       // The stencil is consumed field group by field group (B, then E, then
       // P); the warp-level fence between groups keeps the shared loads of the
       // next group from being hoisted, which bounds the live registers.
@@ -427,7 +466,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
       __syncwarp(amask);
       d1(std::integral_constant<int, 6>{}, dv.gradP);
       if constexpr (!FIRST) {
-        const uint32_t ad = dme + (uint32_t)((k % DR) * DSB);
+        const uint32_t ad = dme + dslot(sc, Z{}, k);
         static_for<7>([&](auto fc) {
           constexpr int f = decltype(fc)::value;
           dold[f] = lds<T, f * DFB>(ad);
@@ -444,7 +483,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     }
     if constexpr (kRingSpare == 0) {
       __syncthreads();
-      issue(k + 3 + PF);  // into the slot of plane k
+      issue(k + 3 + PF, fslot(sc, PN{}, k), dslot(sc, PD{}, k));  // into the slot of plane k
     }
   };
   if constexpr (ZU == 5) {
@@ -493,9 +532,18 @@ static_assert((ko_zunroll<false>() == 1 || ko_zunroll<false>() == 7) &&
                   (ko_zunroll<true>() == 1 || ko_zunroll<true>() == 7),
               "KO z unroll is 1 or 7");
 
-template <typename T, int TX, int TY, int PF, int V>
+// Ring slots of the KO kernel (plane k in slot (k - lo[2]) % R).  A 7-slot
+// ring, matching the z unroll, would make the slots compile-time constants
+// but measured far slower (its shared memory leaves the two resident CTAs
+// little L1 cache).
+template <bool BC, int PF>
+__host__ __device__ constexpr int ko_ring() {
+  return 4 + PF + kKoRingSpare;
+}
+
+template <typename T, int TX, int TY, int PF, int V, bool BC>
 constexpr size_t ko_smem_bytes() {
-  return (size_t)(4 + PF + kKoRingSpare) * 7 * TileLoader<T, TX, TY, 3, V>::FB;
+  return (size_t)ko_ring<BC, PF>() * 7 * TileLoader<T, TX, TY, 3, V>::FB;
 }
 
 template <typename T, int TX, int TY, int PF, bool BC, int V>
@@ -503,8 +551,9 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     ez_ko_kernel(const __grid_constant__ EzConst<T> c, const F7<const T> uin,
                  const F7<T> uout, const T tko, const int kchunk) {
   using L = TileLoader<T, TX, TY, 3, V>;
-  constexpr int R = 4 + PF + kKoRingSpare;
+  constexpr int R = ko_ring<BC, PF>();
   constexpr int ZU = ko_zunroll<BC>();
+
   constexpr int ES = (int)sizeof(T);
   constexpr int SX = L::SX, FB = L::FB, SB = 7 * FB;
   constexpr int CEN = (3 * SX + 3) * ES;  // own point, from the corner of its 7x7 patch
@@ -524,12 +573,19 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
   const L loader(g, sbase, tid, g.lo[0] + (int)blockIdx.x * TX - 3,
                  g.lo[1] + (int)blockIdx.y * TY - 3);
   const int kend = k1 + 3;  // planes [k0, k1+3) pass through shared memory
-  auto issue = [&](int kp) {
-    if (kp < kend) loader.copy(uin, (uint32_t)kp * sz, (uint32_t)((kp % R) * SB));
+  const int lo2 = g.lo[2];
+  // byte offset of the ring slot of plane k + OFF in window phase S
+  auto fslot = [&](auto sc, auto oc, int k) -> uint32_t {
+    constexpr int S = decltype(sc)::value, OFF = decltype(oc)::value;
+    if constexpr (ZU == R) return (uint32_t)(((S + OFF) % R) * SB);
+    else return (uint32_t)(((k + OFF - lo2) % R) * SB);
+  };
+  auto issue = [&](int kp, uint32_t fs) {
+    if (kp < kend) loader.copy(uin, (uint32_t)kp * sz, fs);
     cp_async_commit();
   };
 #pragma unroll 1
-  for (int p = 0; p < 4 + PF; ++p) issue(k0 + p);
+  for (int p = 0; p < 4 + PF; ++p) issue(k0 + p, (uint32_t)(((k0 + p - lo2) % R) * SB));
 
   // Register window: in window phase S, w[(S + q) % 7][f] = field f at
   // (i, j, k - 3 + q); planes k-3 .. k+2 are carried, k+3 is read from the
@@ -548,10 +604,11 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     constexpr int S = decltype(sc)::value;
     cp_async_wait<PF>();  // plane k+3 has landed
     __syncthreads();
-    if constexpr (kKoRingSpare == 1) issue(k + 4 + PF);  // into the slot of plane k-1
+    using PN = std::integral_constant<int, 4 + PF>;  // the plane issued now
+    if constexpr (kKoRingSpare == 1) issue(k + 4 + PF, fslot(sc, PN{}, k));  // slot of plane k-1
     if (active && k < k1) {
-      const uint32_t a0 = corner + (uint32_t)((k % R) * SB);
-      const uint32_t a3 = corner + (uint32_t)(((k + 3) % R) * SB);
+      const uint32_t a0 = corner + fslot(sc, std::integral_constant<int, 0>{}, k);
+      const uint32_t a3 = corner + fslot(sc, std::integral_constant<int, 3>{}, k);
       T nu[7];
       static_for<7>([&](auto fc) {
         constexpr int f = decltype(fc)::value;
@@ -585,7 +642,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     }
     if constexpr (kKoRingSpare == 0) {
       __syncthreads();
-      issue(k + 4 + PF);  // into the slot of plane k
+      issue(k + 4 + PF, fslot(sc, PN{}, k));  // into the slot of plane k (or k-2 of 7)
     }
   };
   if constexpr (ZU == 7) {

@@ -54,15 +54,15 @@ template <> struct Shape<double> {
   static constexpr int KTX = 32, KTY = 4, KPF = 1;
 };
 
-template <typename T, int V>
+template <typename T, int V, bool BC>
 size_t stage_smem(bool first) {
   using S = Shape<T>;
-  return stage_smem_bytes<T, S::STX, S::STY, S::SPF, V>(first);
+  return stage_smem_bytes<T, S::STX, S::STY, S::SPF, V, BC>(first);
 }
-template <typename T, int V>
+template <typename T, int V, bool BC>
 size_t ko_smem() {
   using S = Shape<T>;
-  return ko_smem_bytes<T, S::KTX, S::KTY, S::KPF, V>();
+  return ko_smem_bytes<T, S::KTX, S::KTY, S::KPF, V, BC>();
 }
 
 // LSRK(5,4) coefficients of the reference (field_solver_EZ.cpp:1009-1014)
@@ -72,11 +72,14 @@ constexpr double kBs[5] = {0.1496590219993, 0.3792103129999, 0.8229550293869, 0.
 constexpr double kCs[5] = {0, 0.1496590219993, 0.3704009573644, 0.6222557631345, 0.9582821306784};
 
 // Choose the z chunk of a CTA: enough CTAs to fill the GPU in whole waves,
-// while the 2H halo planes each chunk re-reads stay a small fraction.
-inline int pick_kchunk(int nz, int nxy_tiles, int slots, int halo) {
+// while the 2H halo planes each chunk re-reads stay a small fraction.  The
+// chunk is a multiple of `mult` (the kernel's z unroll, whose ring slots are
+// then compile-time constants), except that it may be all nz planes.
+inline int pick_kchunk(int nz, int nxy_tiles, int slots, int halo, int mult) {
   int best = nz;
   double best_cost = 1e300;
-  for (int kc = 4; kc <= nz + 3; kc += 4) {
+  const int step = mult > 1 ? mult : 4;
+  for (int kc = step; kc <= nz + step - 1; kc += step) {
     const int kk = std::min(kc, nz);
     const long long ctas = (long long)nxy_tiles * ((nz + kk - 1) / kk);
     const double waves = std::ceil((double)ctas / (double)slots);
@@ -195,21 +198,21 @@ struct FlatKernels {
 
   static cudaError_t set_attributes() {
     cudaError_t e = cudaFuncSetAttribute(first, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)stage_smem<T, V>(true));
+                                         (int)stage_smem<T, V, BC>(true));
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(rest, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)stage_smem<T, V>(false));
+                               (int)stage_smem<T, V, BC>(false));
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(ko, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)ko_smem<T, V>());
+                               (int)ko_smem<T, V, BC>());
     return e;
   }
   static cudaError_t occupancy(int* stage, int* kop) {
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(stage, rest, S::STX * S::STY,
-                                                                  stage_smem<T, V>(false));
+                                                                  stage_smem<T, V, BC>(false));
     if (e == cudaSuccess)
       e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(kop, ko, S::KTX * S::KTY,
-                                                        ko_smem<T, V>());
+                                                        ko_smem<T, V, BC>());
     return e;
   }
   static void stage(bool is_first, const FlatLaunch& L, cudaStream_t st, const EzConst<T>& c,
@@ -217,15 +220,15 @@ struct FlatKernels {
                     const F5<T>& aux, T As, T Bs, T tst, int flags) {
     const dim3 bs(S::STX, S::STY);
     if (is_first)
-      first<<<L.grid_stage, bs, stage_smem<T, V>(true), st>>>(c, src, dst, du, un, aux, As, Bs,
+      first<<<L.grid_stage, bs, stage_smem<T, V, BC>(true), st>>>(c, src, dst, du, un, aux, As, Bs,
                                                               tst, L.kchunk_stage, flags);
     else
-      rest<<<L.grid_stage, bs, stage_smem<T, V>(false), st>>>(c, src, dst, du, un, aux, As, Bs,
+      rest<<<L.grid_stage, bs, stage_smem<T, V, BC>(false), st>>>(c, src, dst, du, un, aux, As, Bs,
                                                               tst, L.kchunk_stage, flags);
   }
   static void ko_pass(const FlatLaunch& L, cudaStream_t st, const EzConst<T>& c,
                       const F7<const T>& src, const F7<T>& dst, T tko) {
-    ko<<<L.grid_ko, dim3(S::KTX, S::KTY), ko_smem<T, V>(), st>>>(c, src, dst, tko, L.kchunk_ko);
+    ko<<<L.grid_ko, dim3(S::KTX, S::KTY), ko_smem<T, V, BC>(), st>>>(c, src, dst, tko, L.kchunk_ko);
   }
 };
 
@@ -271,10 +274,18 @@ inline int flat_plan(const coffee_env* env, int semantics, FlatLaunch* L) {
   int box[3];
   for (int a = 0; a < 3; ++a) box[a] = p.N[a] + 2 * p.shift_ghost;
   const int sx = (box[0] + S::STX - 1) / S::STX, sy = (box[1] + S::STY - 1) / S::STY;
-  L->kchunk_stage = pick_kchunk(box[2], sx * sy, sms * per_sm_stage, 4);
+  // a kernel whose ring length equals its z unroll needs chunks of a
+  // multiple of it (its ring slots are then compile-time constants)
+  auto chunk_mult = [](int unroll, int ring) { return unroll == ring ? unroll : 1; };
+  L->kchunk_stage = pick_kchunk(
+      box[2], sx * sy, sms * per_sm_stage, 4,
+      L->bc ? chunk_mult(stage_zunroll<true>(), stage_ring<true, S::SPF>())
+            : chunk_mult(stage_zunroll<false>(), stage_ring<false, S::SPF>()));
   L->grid_stage = dim3(sx, sy, (box[2] + L->kchunk_stage - 1) / L->kchunk_stage);
   const int kx = (box[0] + S::KTX - 1) / S::KTX, ky = (box[1] + S::KTY - 1) / S::KTY;
-  L->kchunk_ko = pick_kchunk(box[2], kx * ky, sms * per_sm_ko, 6);
+  L->kchunk_ko = pick_kchunk(box[2], kx * ky, sms * per_sm_ko, 6,
+                             L->bc ? chunk_mult(ko_zunroll<true>(), ko_ring<true, S::KPF>())
+                                   : chunk_mult(ko_zunroll<false>(), ko_ring<false, S::KPF>()));
   L->grid_ko = dim3(kx, ky, (box[2] + L->kchunk_ko - 1) / L->kchunk_ko);
   return COFFEE_OK;
 }
