@@ -100,6 +100,7 @@ SIGNATURES = {
                                         _P(_d), _P(_d)]),
     "coffee_solver_launches_per_step": (_i, [_vp]),
     "coffee_diag_reduce": (_i, [_vp, _i, _P(_d)]),
+    "coffee_diag_luminosity": (_i, [_vp, _d, _P(_d)]),
     "coffee_solver_check_finite": (_i, [_vp]),
     "coffee_solver_save_snapshot": (_i, [_vp, ctypes.c_char_p, _d, ctypes.c_int64]),
     "coffee_solver_load_snapshot": (_i, [_vp, ctypes.c_char_p, _P(_d), _P(ctypes.c_int64)]),

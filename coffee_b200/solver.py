@@ -222,6 +222,13 @@ class FieldSolverEZ:
         """field_solver_EZ::total_energy of E or B, accumulated in FP64."""
         return self.diag("energy_" + which)
 
+    def luminosity(self, r: float) -> float:
+        """FP64 Poynting luminosity through the sphere |x| = r (flat solver):
+        the flux of E x B out of a shell of one grid spacing around r."""
+        out = ctypes.c_double()
+        check(self.lib.coffee_diag_luminosity(self.handle, float(r), ctypes.byref(out)))
+        return out.value
+
     def check_finite(self):
         check(self.lib.coffee_solver_check_finite(self.handle))
 

@@ -224,6 +224,13 @@ COFFEE_API int coffee_fields_init_fourier(coffee_fields* f, const double b0[3], 
  * src/algorithms/field_solver_EZ.cu:755-795, and the checks listed with
  * COFFEE_DIAG_*).  Synchronises. */
 COFFEE_API int coffee_diag_reduce(coffee_solver* s, int what, double* out);
+/* FP64 Poynting luminosity of the flat solver's fields through the sphere
+ * |x| = r: the flux of S = E x B averaged over a shell around r,
+ * sum over interior points of (S . x/|x|) w(|x| - r) dx dy dz with the tent
+ * w(s) = max(0, 1 - |s|/h) / h, h the largest grid spacing.  No reference
+ * counterpart (the reference reports total_energy only); the spindown
+ * luminosity of a rotator.  Synchronises. */
+COFFEE_API int coffee_diag_luminosity(coffee_solver* s, double r, double* out);
 /* Check every field for NaN/Inf: COFFEE_OK or COFFEE_E_NONFINITE. */
 COFFEE_API int coffee_solver_check_finite(coffee_solver* s);
 

@@ -349,6 +349,13 @@ class field_solver_EZ {
     coffee_check(coffee_diag_reduce(m_solver, what, &out), "total_energy");
     return (Scalar)out;
   }
+  // FP64 Poynting luminosity through the sphere |x| = r (no reference
+  // counterpart; coffee_diag_luminosity).
+  double poynting_luminosity(double r) {
+    double out = 0;
+    coffee_check(coffee_diag_luminosity(m_solver, r, &out), "poynting_luminosity");
+    return out;
+  }
   void set_aux(bool enable) { coffee_check(coffee_solver_set_aux(m_solver, enable), "set_aux"); }
   coffee_solver* handle() const { return m_solver; }
 
