@@ -219,8 +219,15 @@ __device__ __noinline__ V7<T> gr_absorb(const GrConst<T>& c, V7<T> v, V7<T> n, T
 // field_solver_gr_EZ.cu:188-420, then the clamps and, in the last stage,
 // the absorbing layers: order of :876-893).  u: D, B, P of the current
 // buffer; eh: E, H of the same buffer.
+// Minimum resident 256-thread CTAs per SM of the stage kernel: the kernel is
+// bound by the latency of its stencil loads, and 6 CTAs (40 registers, a
+// little spilling) hide it best (1.31 -> 1.19 ms per launch at 256^3; 7 or 8
+// CTAs spill too much).
+#ifndef COFFEE_GR_STAGE_MIN_BLOCKS
+#define COFFEE_GR_STAGE_MIN_BLOCKS 6
+#endif
 template <typename T, bool FIRST>
-__global__ void __launch_bounds__(256) gr_stage_kernel(const __grid_constant__ GrConst<T> c,
+__global__ void __launch_bounds__(256, COFFEE_GR_STAGE_MIN_BLOCKS) gr_stage_kernel(const __grid_constant__ GrConst<T> c,
                                                        const F7<T> u, const F7<T> eh,
                                                        const F7<T> out, const F7<T> du,
                                                        const F7<T> un, const F5<T> aux,
