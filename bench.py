@@ -527,8 +527,10 @@ def run_variant(args):
                 "achieved": BYTES_STEP * cells / (step_ms / 1e3) / 1e9, "peak": peak,
                 "unit": "GB/s", "peak_kind": peak_kind, "traffic": None,
                 "algorithmic_bytes_per_step": BYTES_STEP * cells}
-        launches = 12 * args.steps + 1
-        launch_note = "5 stage + 5 axis + 1 KO + 1 axis per step, 1 axis per call"
+        launches = 13 * args.steps + 1
+        launch_note = ("5 stage + 5 axis + 1 KO + 1 axis + 1 time-advance per step (one captured "
+                       "CUDA graph, replayed per step), 1 axis per call")
+        cfg["autotuned"] = batch.info()
     roof["frac"] = roof["achieved"] / peak
     # end to end: upload from pinned host memory, K steps, download
     hosts = []

@@ -106,6 +106,7 @@ SIGNATURES = {
     "coffee_solver_load_snapshot": (_i, [_vp, ctypes.c_char_p, _P(_d), _P(ctypes.c_int64)]),
     "coffee_batch_create": (_i, [_P(_vp), _i, _vp, _P(_vp)]),
     "coffee_batch_step": (_i, [_vp, _P(_d), _i]),
+    "coffee_batch_info": (_i, [_vp, _P(_i), _P(_i), _P(_i), _P(_d)]),
     "coffee_batch_destroy": (_i, [_vp]),
     "coffee_evolve_noalloc": (_i, [_P(CoffeeParams), _i, _P(_vp), _d, _i, _vp]),
 }

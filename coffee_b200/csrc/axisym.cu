@@ -3,6 +3,7 @@
 // batched step loop of many log-spherical runs.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -293,13 +294,17 @@ int make_sph_table(const coffee_env* env, void** tab) {
   return COFFEE_OK;
 }
 
+// Run table for tile shape tx x ty (tx * ty = 256) with the runs in `order`
+// (indices into runs); e.index keeps each run's position in the batch.
 template <typename T>
-int sph_batch_create_t(const SphRun* runs, int n, void** dev_table, int* nblocks,
-                       int* naxis_blocks) {
+int sph_batch_table_t(const SphRun* runs, const std::vector<int>& order, int tx, int ty,
+                      void** dev_table, int* nblocks, int* naxis_blocks) {
+  const int n = (int)order.size();
   std::vector<SphBatchEntry<T>> h(n);
   int tiles = 0, axis = 0;
-  for (int m = 0; m < n; ++m) {
-    SphBatchEntry<T>& e = h[m];
+  for (int q = 0; q < n; ++q) {
+    const int m = order[q];
+    SphBatchEntry<T>& e = h[q];
     std::memset(&e, 0, sizeof(e));
     fill_sph_const<T>(runs[m].env, runs[m].tab, &e.c);
     e.A = as_f7<T>(runs[m].A);
@@ -312,10 +317,10 @@ int sph_batch_create_t(const SphRun* runs, int n, void** dev_table, int* nblocks
     e.want_aux = runs[m].want_aux;
     e.index = m;
     const Box b = update_box(runs[m].env);
-    const dim3 g = box_grid(b);
+    const int gx = (b.hi0 - b.lo0 + tx - 1) / tx, gy = (b.hi1 - b.lo1 + ty - 1) / ty;
     e.tile0 = tiles;
-    e.tiles_x = (int)g.x;
-    tiles += (int)(g.x * g.y);
+    e.tiles_x = gx;
+    tiles += gx * gy;
     e.axis0 = axis;
     axis += (b.hi0 - b.lo0 + 127) / 128;
   }
@@ -333,64 +338,203 @@ int sph_batch_create_t(const SphRun* runs, int n, void** dev_table, int* nblocks
   return COFFEE_OK;
 }
 
+// Tile shapes the autotuner tries (256 threads each: the kernels' launch
+// bounds) and the run orders.
+constexpr int kTuneShapes[][2] = {{32, 8}, {64, 4}, {128, 2}, {16, 16}};
+
+template <typename T>
+int sph_batch_plan_t(const SphRun* runs, int n, bool tune, cudaStream_t st, SphBatchPlan* pl) {
+  pl->elem = (int)sizeof(T);
+  pl->n = n;
+  std::vector<int> given(n), largest(n);
+  for (int m = 0; m < n; ++m) given[m] = largest[m] = m;
+  auto points = [&](int m) {
+    const Box b = update_box(runs[m].env);
+    return (long long)(b.hi0 - b.lo0) * (b.hi1 - b.lo1);
+  };
+  std::stable_sort(largest.begin(), largest.end(),
+                   [&](int a, int b) { return points(a) > points(b); });
+  int best_shape = 0, best_order = 0;
+  double best_ms = 0;
+  if (tune) {
+    cudaEvent_t e0, e1;
+    COFFEE_CUDA_TRY(cudaEventCreate(&e0));
+    COFFEE_CUDA_TRY(cudaEventCreate(&e1));
+    // every run at its own time: the first stage only evaluates the star
+    std::vector<T> h0(n, T(0)), hdt(n);
+    for (int m = 0; m < n; ++m) hdt[m] = (T)runs[m].env->p.dt;
+    void *t0 = nullptr, *tdt = nullptr;
+    cudaError_t err = cudaMalloc(&t0, sizeof(T) * n);
+    if (err == cudaSuccess) err = cudaMalloc(&tdt, sizeof(T) * n);
+    if (err == cudaSuccess) err = cudaMemcpy(t0, h0.data(), sizeof(T) * n, cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) err = cudaMemcpy(tdt, hdt.data(), sizeof(T) * n, cudaMemcpyHostToDevice);
+    int rc = err == cudaSuccess ? COFFEE_OK
+                                : fail(COFFEE_E_NOMEM, "batch tuning: %s", cudaGetErrorString(err));
+    for (int o = 0; o < 2 && rc == COFFEE_OK; ++o) {
+      for (int sh = 0; sh < 4 && rc == COFFEE_OK; ++sh) {
+        const int tx = kTuneShapes[sh][0], ty = kTuneShapes[sh][1];
+        void* tab = nullptr;
+        int nb = 0, na = 0;
+        rc = sph_batch_table_t<T>(runs, o ? largest : given, tx, ty, &tab, &nb, &na);
+        if (rc) break;
+        const auto* tt = static_cast<const SphBatchEntry<T>*>(tab);
+        float best = 1e30f;
+        for (int rep = 0; rep < 4 && rc == COFFEE_OK; ++rep) {
+          cudaEventRecord(e0, st);
+          sph_stage_batch_kernel<T, true><<<nb, dim3(tx, ty, 1), 0, st>>>(
+              tt, n, 1, static_cast<const T*>(t0), static_cast<const T*>(tdt), T(0), (T)kAs[0],
+              (T)kBs[0], 0);
+          cudaEventRecord(e1, st);
+          err = cudaEventSynchronize(e1);
+          if (err == cudaSuccess) err = cudaGetLastError();
+          float ms = 0;
+          if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+          if (err != cudaSuccess) {
+            rc = fail(COFFEE_E_CUDA, "batch tuning launch: %s", cudaGetErrorString(err));
+            break;
+          }
+          if (rep > 0) best = std::min(best, ms);  // the first launch warms up
+        }
+        cudaFree(tab);
+        if (rc == COFFEE_OK && (best_ms == 0 || best < best_ms)) {
+          best_ms = best;
+          best_shape = sh;
+          best_order = o;
+        }
+      }
+    }
+    cudaFree(t0);
+    cudaFree(tdt);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+  }
+  pl->tx = kTuneShapes[best_shape][0];
+  pl->ty = kTuneShapes[best_shape][1];
+  pl->order = best_order;
+  pl->tuned_ms = best_ms;
+  int rc = sph_batch_table_t<T>(runs, best_order ? largest : given, pl->tx, pl->ty, &pl->table,
+                                &pl->nblocks, &pl->naxis);
+  if (rc) return rc;
+  std::vector<T> hdt(n);
+  for (int m = 0; m < n; ++m) hdt[m] = (T)runs[m].env->p.dt;
+  cudaError_t err = cudaMalloc(&pl->tnow, sizeof(T) * n);
+  if (err == cudaSuccess) err = cudaMalloc(&pl->tdt, sizeof(T) * n);
+  if (err == cudaSuccess)
+    err = cudaMemcpy(pl->tdt, hdt.data(), sizeof(T) * n, cudaMemcpyHostToDevice);
+  if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&pl->cap, cudaStreamNonBlocking);
+  if (err != cudaSuccess) return fail(COFFEE_E_NOMEM, "batch plan: %s", cudaGetErrorString(err));
+  return COFFEE_OK;
+}
+
+// The launches of one step of every run: 5 x (stage + axis), KO + axis,
+// then t += dt.  The times come from plan->tnow / tdt.
+template <typename T>
+int sph_batch_step_launches(const SphBatchPlan* pl, cudaStream_t st) {
+  const auto* tab = static_cast<const SphBatchEntry<T>*>(pl->table);
+  const T* tnow = static_cast<const T*>(pl->tnow);
+  const T* tdt = static_cast<const T*>(pl->tdt);
+  const int n = pl->n;
+  const dim3 block(pl->tx, pl->ty, 1);
+  for (int s = 0; s < 5; ++s) {
+    const int to_b = (s % 2 == 0) ? 1 : 0;
+    if (s == 0)
+      sph_stage_batch_kernel<T, true><<<pl->nblocks, block, 0, st>>>(
+          tab, n, to_b, tnow, tdt, (T)kCs[s], (T)kAs[s], (T)kBs[s], 0);
+    else
+      sph_stage_batch_kernel<T, false><<<pl->nblocks, block, 0, st>>>(
+          tab, n, to_b, tnow, tdt, (T)kCs[s], (T)kAs[s], (T)kBs[s], s == 4);
+    COFFEE_CUDA_TRY(cudaGetLastError());
+    sph_axis_batch_kernel<T><<<pl->naxis, 128, 0, st>>>(tab, n, to_b);
+    COFFEE_CUDA_TRY(cudaGetLastError());
+  }
+  sph_ko_batch_kernel<T><<<pl->nblocks, block, 0, st>>>(tab, n, tnow, tdt);
+  COFFEE_CUDA_TRY(cudaGetLastError());
+  sph_axis_batch_kernel<T><<<pl->naxis, 128, 0, st>>>(tab, n, 0);
+  COFFEE_CUDA_TRY(cudaGetLastError());
+  sph_batch_advance_kernel<T><<<(n + 127) / 128, 128, 0, st>>>(static_cast<T*>(pl->tnow), tdt, n);
+  COFFEE_CUDA_TRY(cudaGetLastError());
+  return COFFEE_OK;
+}
+
+template <typename T>
+int sph_batch_capture(SphBatchPlan* pl) {
+  COFFEE_CUDA_TRY(cudaStreamBeginCapture(pl->cap, cudaStreamCaptureModeThreadLocal));
+  const int rc = sph_batch_step_launches<T>(pl, pl->cap);
+  cudaGraph_t g = nullptr;
+  const cudaError_t err = cudaStreamEndCapture(pl->cap, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (err != cudaSuccess) return fail(COFFEE_E_CUDA, "batch step capture: %s", cudaGetErrorString(err));
+  const cudaError_t e2 = cudaGraphInstantiate(&pl->step, g, 0);
+  cudaGraphDestroy(g);
+  if (e2 != cudaSuccess) {
+    pl->step = nullptr;
+    return fail(COFFEE_E_CUDA, "batch step graph: %s", cudaGetErrorString(e2));
+  }
+  return COFFEE_OK;
+}
+
 // nsteps evolve_fields calls of every run of the batch, each from its own
 // time (advanced in field precision by its own dt): the stage / axis / KO
 // sequence of sph_steps with one launch per phase for the whole batch.
 template <typename T>
-int sph_batch_steps_t(const void* dev_table, int n, const SphRun* runs, double* times,
-                      int nsteps, int nblocks, int naxis, cudaStream_t st) {
-  const auto* tab = static_cast<const SphBatchEntry<T>*>(dev_table);
+int sph_batch_run_t(SphBatchPlan* pl, const SphRun* runs, double* times, int nsteps,
+                    bool use_graph, cudaStream_t st) {
+  const int n = pl->n;
+  if (nsteps <= 0) return COFFEE_OK;
   std::vector<T> t(n), dt(n);
   for (int m = 0; m < n; ++m) {
     t[m] = (T)times[m];
     dt[m] = (T)runs[m].env->p.dt;
   }
-  const dim3 block(kTX, kTY, 1);
-  if (nsteps > 0) {
-    sph_axis_batch_kernel<T><<<naxis, 128, 0, st>>>(tab, n, 0);
-    COFFEE_CUDA_TRY(cudaGetLastError());
+  // pageable source: staged at once, so the vector may go out of scope
+  COFFEE_CUDA_TRY(cudaMemcpyAsync(pl->tnow, t.data(), sizeof(T) * n, cudaMemcpyHostToDevice, st));
+  sph_axis_batch_kernel<T><<<pl->naxis, 128, 0, st>>>(
+      static_cast<const SphBatchEntry<T>*>(pl->table), n, 0);
+  COFFEE_CUDA_TRY(cudaGetLastError());
+  if (use_graph && !pl->step) {
+    int rc = sph_batch_capture<T>(pl);
+    if (rc) return rc;
   }
-  SphBatchTimes<T> ts;
-  std::memset(&ts, 0, sizeof(ts));
   for (int step = 0; step < nsteps; ++step) {
-    for (int s = 0; s < 5; ++s) {
-      for (int m = 0; m < n; ++m) ts.t[m] = (T)(t[m] + (T)kCs[s] * dt[m]);
-      const int to_b = (s % 2 == 0) ? 1 : 0;
-      if (s == 0)
-        sph_stage_batch_kernel<T, true><<<nblocks, block, 0, st>>>(tab, n, to_b, ts, (T)kAs[s],
-                                                                   (T)kBs[s], 0);
-      else
-        sph_stage_batch_kernel<T, false><<<nblocks, block, 0, st>>>(tab, n, to_b, ts, (T)kAs[s],
-                                                                    (T)kBs[s], s == 4);
-      COFFEE_CUDA_TRY(cudaGetLastError());
-      sph_axis_batch_kernel<T><<<naxis, 128, 0, st>>>(tab, n, to_b);
-      COFFEE_CUDA_TRY(cudaGetLastError());
+    if (use_graph) {
+      COFFEE_CUDA_TRY(cudaGraphLaunch(pl->step, st));
+    } else {
+      int rc = sph_batch_step_launches<T>(pl, st);
+      if (rc) return rc;
     }
-    for (int m = 0; m < n; ++m) ts.t[m] = (T)(t[m] + dt[m]);
-    sph_ko_batch_kernel<T><<<nblocks, block, 0, st>>>(tab, n, ts);
-    COFFEE_CUDA_TRY(cudaGetLastError());
-    sph_axis_batch_kernel<T><<<naxis, 128, 0, st>>>(tab, n, 0);
-    COFFEE_CUDA_TRY(cudaGetLastError());
-    for (int m = 0; m < n; ++m) t[m] = (T)(t[m] + dt[m]);
   }
+  // the same field-precision arithmetic as the device's t += dt
+  for (int step = 0; step < nsteps; ++step)
+    for (int m = 0; m < n; ++m) t[m] = (T)(t[m] + dt[m]);
   for (int m = 0; m < n; ++m) times[m] = (double)t[m];
   return COFFEE_OK;
 }
 
 }  // namespace
 
-int sph_batch_create(const SphRun* runs, int n, int elem, void** dev_table, int* nblocks,
-                     int* naxis_blocks) {
-  return elem == 4 ? sph_batch_create_t<float>(runs, n, dev_table, nblocks, naxis_blocks)
-                   : sph_batch_create_t<double>(runs, n, dev_table, nblocks, naxis_blocks);
+int sph_batch_plan(const SphRun* runs, int n, int elem, bool tune, cudaStream_t st,
+                   SphBatchPlan* plan) {
+  return elem == 4 ? sph_batch_plan_t<float>(runs, n, tune, st, plan)
+                   : sph_batch_plan_t<double>(runs, n, tune, st, plan);
 }
 
-int sph_batch_steps(const void* dev_table, int n, int elem, const SphRun* runs, double* times,
-                    int nsteps, int nblocks, int naxis_blocks, cudaStream_t st) {
-  return elem == 4 ? sph_batch_steps_t<float>(dev_table, n, runs, times, nsteps, nblocks,
-                                              naxis_blocks, st)
-                   : sph_batch_steps_t<double>(dev_table, n, runs, times, nsteps, nblocks,
-                                               naxis_blocks, st);
+int sph_batch_run(SphBatchPlan* plan, const SphRun* runs, double* times, int nsteps,
+                  bool use_graph, cudaStream_t st) {
+  return plan->elem == 4 ? sph_batch_run_t<float>(plan, runs, times, nsteps, use_graph, st)
+                         : sph_batch_run_t<double>(plan, runs, times, nsteps, use_graph, st);
+}
+
+void sph_batch_free(SphBatchPlan* plan) {
+  if (plan->step) cudaGraphExecDestroy(plan->step);
+  if (plan->cap) cudaStreamDestroy(plan->cap);
+  if (plan->table) cudaFree(plan->table);
+  if (plan->tnow) cudaFree(plan->tnow);
+  if (plan->tdt) cudaFree(plan->tdt);
+  *plan = SphBatchPlan();
 }
 
 int axisym_check(const coffee_env* env, int variant) {

@@ -444,10 +444,17 @@ struct SphBatchEntry {
   int index;    // position in the batch
 };
 
-template <typename T>
-struct SphBatchTimes {
-  T t[kSphBatchMax];
-};
+// Times of the runs of a batch live in device memory (the current step's
+// start time t and the time step dt of each run), so that one captured step
+// serves every step.  A stage at t + cs dt evaluates that time exactly as the
+// host loop of a single run does, in field precision with one rounding per
+// operation (no fused multiply-add).
+__device__ __forceinline__ float batch_time(float t, float cs, float dt) {
+  return __fadd_rn(t, __fmul_rn(cs, dt));
+}
+__device__ __forceinline__ double batch_time(double t, double cs, double dt) {
+  return __dadd_rn(t, __dmul_rn(cs, dt));
+}
 
 template <typename T>
 __device__ __forceinline__ const SphBatchEntry<T>& sph_batch_entry(
@@ -476,7 +483,8 @@ __device__ __forceinline__ const SphBatchEntry<T>& sph_batch_entry(
 template <typename T, bool FIRST>
 __global__ void __launch_bounds__(256, kAxiMinBlocks) sph_stage_batch_kernel(
     const SphBatchEntry<T>* __restrict__ tab, const int n, const int to_b,
-    const __grid_constant__ SphBatchTimes<T> tst, const T As, const T Bs, const int last) {
+    const T* __restrict__ tnow, const T* __restrict__ tdt, const T cs, const T As, const T Bs,
+    const int last) {
   __shared__ __align__(16) unsigned char buf[sizeof(SphBatchEntry<T>)];
   const SphBatchEntry<T>& e = sph_batch_entry(tab, n, (int)blockIdx.x, false, buf);
   const int lt = (int)blockIdx.x - e.tile0;
@@ -486,21 +494,30 @@ __global__ void __launch_bounds__(256, kAxiMinBlocks) sph_stage_batch_kernel(
   int flags = 0;
   if (last) flags |= AX_LAST | (e.want_aux ? AX_AUX : 0);
   if (FIRST && e.c.absorbing) flags |= AX_WRITE_UN;
+  const T tst = batch_time(tnow[e.index], cs, tdt[e.index]);
   sph_stage_point<T, FIRST>(e.c, i, j, to_b ? e.A : e.B, to_b ? e.B : e.A, e.dU, e.Un, e.aux,
-                            As, Bs, tst.t[e.index], flags);
+                            As, Bs, tst, flags);
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256, kAxiMinBlocks) sph_ko_batch_kernel(
-    const SphBatchEntry<T>* __restrict__ tab, const int n,
-    const __grid_constant__ SphBatchTimes<T> tend) {
+    const SphBatchEntry<T>* __restrict__ tab, const int n, const T* __restrict__ tnow,
+    const T* __restrict__ tdt) {
   __shared__ __align__(16) unsigned char buf[sizeof(SphBatchEntry<T>)];
   const SphBatchEntry<T>& e = sph_batch_entry(tab, n, (int)blockIdx.x, false, buf);
   const int lt = (int)blockIdx.x - e.tile0;
   const int i = e.c.lo0 + (lt % e.tiles_x) * blockDim.x + threadIdx.x;
   const int j = e.c.lo1 + (lt / e.tiles_x) * blockDim.y + threadIdx.y;
   if (i >= e.c.hi0 || j >= e.c.hi1) return;
-  sph_ko_point(e.c, i, j, e.B, e.A, tend.t[e.index]);
+  sph_ko_point(e.c, i, j, e.B, e.A, batch_time(tnow[e.index], T(1), tdt[e.index]));
+}
+
+// end of a step: t += dt for every run, in field precision
+template <typename T>
+__global__ void sph_batch_advance_kernel(T* __restrict__ tnow, const T* __restrict__ tdt,
+                                         const int n) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m < n) tnow[m] = batch_time(tnow[m], T(1), tdt[m]);
 }
 
 // axis boundary of every run; `on_b`: the buffer that was just written

@@ -740,12 +740,18 @@ extern "C" int coffee_solver_step(coffee_solver* s, double time, int nsteps) {
 struct coffee_batch {
   std::vector<coffee_solver*> solvers;
   std::vector<SphRun> runs;
-  void* table;
-  int nblocks, naxis;
+  SphBatchPlan plan;
   int elem;
   int device;
   cudaStream_t stream;
 };
+
+// COFFEE_BATCH_NO_TUNE=1 / COFFEE_BATCH_NO_GRAPH=1 in the environment keep
+// the default tile shape / launch every kernel of every step (comparisons).
+static bool env_flag(const char* name) {
+  const char* v = std::getenv(name);
+  return v != nullptr && v[0] == '1';
+}
 
 extern "C" int coffee_batch_create(coffee_solver* const* solvers, int n, void* stream,
                                    coffee_batch** out) {
@@ -784,12 +790,25 @@ extern "C" int coffee_batch_create(coffee_solver* const* solvers, int n, void* s
     for (int k = 0; k < 5; ++k) r.aux[k] = s->f->d[COFFEE_JX + k];
     r.want_aux = s->aux;
   }
-  int rc = sph_batch_create(b->runs.data(), n, b->elem, &b->table, &b->nblocks, &b->naxis);
+  int rc = sph_batch_plan(b->runs.data(), n, b->elem, !env_flag("COFFEE_BATCH_NO_TUNE"),
+                          b->stream, &b->plan);
   if (rc) {
+    sph_batch_free(&b->plan);
     delete b;
     return rc;
   }
   *out = b;
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_batch_info(coffee_batch* b, int* tile_x, int* tile_y, int* order,
+                                 double* tuned_ms) {
+  clear_error();
+  if (!b) return fail(COFFEE_E_INVALID, "coffee_batch_info: null argument");
+  if (tile_x) *tile_x = b->plan.tx;
+  if (tile_y) *tile_y = b->plan.ty;
+  if (order) *order = b->plan.order;
+  if (tuned_ms) *tuned_ms = b->plan.tuned_ms;
   return COFFEE_OK;
 }
 
@@ -808,15 +827,15 @@ extern "C" int coffee_batch_step(coffee_batch* b, double* times, int nsteps) {
       s->synced_generation = f->generation;
     }
   }
-  return sph_batch_steps(b->table, (int)b->runs.size(), b->elem, b->runs.data(), times, nsteps,
-                         b->nblocks, b->naxis, b->stream);
+  return sph_batch_run(&b->plan, b->runs.data(), times, nsteps, !env_flag("COFFEE_BATCH_NO_GRAPH"),
+                       b->stream);
 }
 
 extern "C" int coffee_batch_destroy(coffee_batch* b) {
   if (!b) return COFFEE_OK;
   cudaSetDevice(b->device);
   cudaStreamSynchronize(b->stream);
-  cudaFree(b->table);
+  sph_batch_free(&b->plan);
   delete b;
   return COFFEE_OK;
 }

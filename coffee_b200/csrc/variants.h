@@ -30,10 +30,31 @@ struct SphRun {
   int want_aux;
 };
 constexpr int kMaxBatch = 128;
-int sph_batch_create(const SphRun* runs, int n, int elem, void** dev_table, int* nblocks,
-                     int* naxis_blocks);
-int sph_batch_steps(const void* dev_table, int n, int elem, const SphRun* runs, double* times,
-                    int nsteps, int nblocks, int naxis_blocks, cudaStream_t st);
+
+// A batch ready to step: its run table (laid out for the chosen tile shape
+// and run order), the runs' times in device memory, and the captured step.
+struct SphBatchPlan {
+  int elem = 4, n = 0;
+  void* table = nullptr;  // SphBatchEntry<T>[n]
+  int nblocks = 0, naxis = 0;
+  int tx = 32, ty = 8;    // tile shape of the stage / KO launches (autotuned)
+  int order = 0;          // 0: runs in the given order, 1: largest first
+  double tuned_ms = 0;    // first-stage time of the chosen layout
+  void* tnow = nullptr;   // field-precision start time of the current step, per run
+  void* tdt = nullptr;    // field-precision dt, per run
+  cudaStream_t cap = nullptr;          // stream the step is captured on
+  cudaGraphExec_t step = nullptr;      // one captured step (made on first use)
+};
+// Build the plan; with `tune`, time the first stage for every candidate tile
+// shape and run order (the first stage writes only scratch: the second field
+// buffer and dU) and keep the fastest.
+int sph_batch_plan(const SphRun* runs, int n, int elem, bool tune, cudaStream_t st,
+                   SphBatchPlan* plan);
+// nsteps steps of every run from times[m] (updated on return); with
+// use_graph the step is the captured graph, replayed nsteps times.
+int sph_batch_run(SphBatchPlan* plan, const SphRun* runs, double* times, int nsteps,
+                  bool use_graph, cudaStream_t st);
+void sph_batch_free(SphBatchPlan* plan);
 
 // GR force-free solver in Kerr-Schild coordinates (COFFEE_VARIANT_GR).
 int gr_check(const coffee_env* env);

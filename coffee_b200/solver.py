@@ -332,6 +332,14 @@ class SphBatch:
                                          int(nsteps)))
         self.times = t
 
+    def info(self) -> dict:
+        """The autotuner's choice: tile shape, run order, first-stage ms."""
+        tx, ty, order, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        check(self.lib.coffee_batch_info(self.handle, ctypes.byref(tx), ctypes.byref(ty),
+                                         ctypes.byref(order), ctypes.byref(ms)))
+        return {"tile": [tx.value, ty.value], "order": ["given", "largest first"][order.value],
+                "first_stage_ms": ms.value}
+
     def close(self):
         if getattr(self, "handle", None):
             self.lib.coffee_batch_destroy(self.handle)

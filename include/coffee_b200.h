@@ -249,12 +249,20 @@ COFFEE_API int coffee_solver_load_snapshot(coffee_solver* s, const char* path, d
  * one kernel launch per phase covers every run, so small grids do not pay a
  * launch each.  Results are those of coffee_solver_step on each solver.  At
  * most 128 runs, all of one precision; the solvers must outlive the batch.
- * coffee_batch_step advances every run by nsteps evolve_fields calls from
- * times[m] and writes the new times back (advanced in field precision). */
+ * coffee_batch_create autotunes the batch: it times the first-stage kernel
+ * (which writes only the solvers' scratch) for four 256-thread tile shapes
+ * and two run orders and keeps the fastest.  coffee_batch_step advances
+ * every run by nsteps evolve_fields calls from times[m] and writes the new
+ * times back (advanced in field precision); one step of the batch is a
+ * captured CUDA graph, made on the first call and replayed for every step. */
 typedef struct coffee_batch coffee_batch;
 COFFEE_API int coffee_batch_create(coffee_solver* const* solvers, int n, void* stream,
                                    coffee_batch** out);
 COFFEE_API int coffee_batch_step(coffee_batch* b, double* times, int nsteps);
+/* The autotuner's choice: tile shape, run order (0 as given, 1 largest
+ * first) and the first stage's time with it in ms. */
+COFFEE_API int coffee_batch_info(coffee_batch* b, int* tile_x, int* tile_y, int* order,
+                                 double* tuned_ms);
 COFFEE_API int coffee_batch_destroy(coffee_batch* b);
 
 /* ---- one step loop that allocates nothing ------------------------------
