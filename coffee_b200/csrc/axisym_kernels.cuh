@@ -20,11 +20,27 @@ namespace coffee {
 enum AxiFlags { AX_LAST = 1, AX_AUX = 2, AX_WRITE_UN = 4 };
 
 // CTAs of 256 threads kept resident per SM (bounds the registers per thread;
-// the kernels are latency-bound on their stencil loads, so more warps help).
-#ifndef COFFEE_AXI_MIN_BLOCKS
-#define COFFEE_AXI_MIN_BLOCKS 4
+// the kernels are latency-bound on their stencil loads, so more warps help,
+// until spilling costs more).  Measured on 2048 x 1024 / 1024 x 2048 grids:
+// the log-spherical kernels are fastest with 8 (32 registers), the
+// cylindrical stage with 6 (40), the cylindrical KO with 4 (64); the
+// batched log-spherical kernels (64 runs) with 4.
+#ifndef COFFEE_SPH_MIN_BLOCKS
+#define COFFEE_SPH_MIN_BLOCKS 8
 #endif
-constexpr int kAxiMinBlocks = COFFEE_AXI_MIN_BLOCKS;
+#ifndef COFFEE_SPH_BATCH_MIN_BLOCKS
+#define COFFEE_SPH_BATCH_MIN_BLOCKS 4
+#endif
+#ifndef COFFEE_CYL_STAGE_MIN_BLOCKS
+#define COFFEE_CYL_STAGE_MIN_BLOCKS 6
+#endif
+#ifndef COFFEE_CYL_KO_MIN_BLOCKS
+#define COFFEE_CYL_KO_MIN_BLOCKS 4
+#endif
+constexpr int kSphMinBlocks = COFFEE_SPH_MIN_BLOCKS;
+constexpr int kSphBatchMinBlocks = COFFEE_SPH_BATCH_MIN_BLOCKS;
+constexpr int kCylStageMinBlocks = COFFEE_CYL_STAGE_MIN_BLOCKS;
+constexpr int kCylKoMinBlocks = COFFEE_CYL_KO_MIN_BLOCKS;
 
 // ---- parameter block of the log-spherical solver ------------------------
 template <typename T>
@@ -316,7 +332,7 @@ __device__ __forceinline__ void sph_stage_point(const SphConst<T>& c, const int 
 }
 
 template <typename T, bool FIRST>
-__global__ void __launch_bounds__(256, kAxiMinBlocks) sph_stage_kernel(const __grid_constant__ SphConst<T> c,
+__global__ void __launch_bounds__(256, kSphMinBlocks) sph_stage_kernel(const __grid_constant__ SphConst<T> c,
                                                         const F7<T> u, const F7<T> out,
                                                         const F7<T> du, const F7<T> un,
                                                         const F5<T> aux, const T As,
@@ -380,7 +396,7 @@ __device__ __forceinline__ void sph_ko_point(const SphConst<T>& c, const int i, 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256, kAxiMinBlocks) sph_ko_kernel(const __grid_constant__ SphConst<T> c,
+__global__ void __launch_bounds__(256, kSphMinBlocks) sph_ko_kernel(const __grid_constant__ SphConst<T> c,
                                                      const F7<T> u, const F7<T> out,
                                                      const T tend) {
   const int i = c.lo0 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -481,7 +497,7 @@ __device__ __forceinline__ const SphBatchEntry<T>& sph_batch_entry(
 }
 
 template <typename T, bool FIRST>
-__global__ void __launch_bounds__(256, kAxiMinBlocks) sph_stage_batch_kernel(
+__global__ void __launch_bounds__(256, kSphBatchMinBlocks) sph_stage_batch_kernel(
     const SphBatchEntry<T>* __restrict__ tab, const int n, const int to_b,
     const T* __restrict__ tnow, const T* __restrict__ tdt, const T cs, const T As, const T Bs,
     const int last) {
@@ -500,7 +516,7 @@ __global__ void __launch_bounds__(256, kAxiMinBlocks) sph_stage_batch_kernel(
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256, kAxiMinBlocks) sph_ko_batch_kernel(
+__global__ void __launch_bounds__(256, kSphBatchMinBlocks) sph_ko_batch_kernel(
     const SphBatchEntry<T>* __restrict__ tab, const int n, const T* __restrict__ tnow,
     const T* __restrict__ tdt) {
   __shared__ __align__(16) unsigned char buf[sizeof(SphBatchEntry<T>)];
@@ -712,7 +728,7 @@ __device__ __forceinline__ void cyl_finish(const CylConst<T>& c, int i, int j, l
 // (field_solver_EZ_cylindrical.cu:143-234, 674-703).  The reference's
 // cylindrical stage writes no J / divE / divB.
 template <typename T, bool FIRST>
-__global__ void __launch_bounds__(256, kAxiMinBlocks) cyl_stage_kernel(const __grid_constant__ CylConst<T> c,
+__global__ void __launch_bounds__(256, kCylStageMinBlocks) cyl_stage_kernel(const __grid_constant__ CylConst<T> c,
                                                         const F7<T> u, const F7<T> out,
                                                         const F7<T> du, const F7<T> un,
                                                         const T As, const T Bs, const T tst,
@@ -779,7 +795,7 @@ __global__ void __launch_bounds__(256, kAxiMinBlocks) cyl_stage_kernel(const __g
 // _step2_thread, field_solver_EZ_cylindrical.cu:297-369; order of :705-712):
 // plain 6th differences in R and z, the clamps, then cyl_finish at t + dt.
 template <typename T>
-__global__ void __launch_bounds__(256, kAxiMinBlocks) cyl_ko_kernel(const __grid_constant__ CylConst<T> c,
+__global__ void __launch_bounds__(256, kCylKoMinBlocks) cyl_ko_kernel(const __grid_constant__ CylConst<T> c,
                                                      const F7<T> u, const F7<T> out,
                                                      const F7<T> un, const T tend) {
   const int i = c.lo0 + blockIdx.x * blockDim.x + threadIdx.x;
