@@ -46,6 +46,7 @@ N_SIDE = 512
 BYTES_STAGE = 112
 BYTES_STEP = 616
 SLAB_Z = 8
+FP64_CHECK_STEPS = 20  # length of the FP32-vs-FP64 comparison of the turbulence run
 
 
 def _peaks():
@@ -257,6 +258,58 @@ def run_reference_arm(args):
     return 0
 
 
+class _DeviceArray:
+    """A device array seen through __cuda_array_interface__ (zero-copy into torch)."""
+
+    def __init__(self, ptr, shape, dtype):
+        import numpy as np
+
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": np.dtype(dtype).str,
+                                         "data": (int(ptr), False), "version": 3,
+                                         "strides": None}
+
+
+def fp64_error(env, steps, modes):
+    """Per-field relative L2 (interior) between the FP32 and the FP64 run of
+    the same algorithm from the same device initial condition after `steps`
+    steps.  Both use the reference GPU build's semantics: the CPU build's
+    P-gradient taper offsets points by a SIMD-lane count that differs between
+    its float and double builds, i.e. it is not the same algorithm in the two
+    precisions."""
+    import numpy as np
+    import torch
+
+    from coffee_b200.solver import FIELD_NAMES, FieldSolverEZ, SimData
+
+    runs = {}
+    for dtype in (np.float32, np.float64):
+        d = SimData(env, dtype)
+        d.init_fourier((1.0, 0.0, 0.0), *modes)
+        sv = FieldSolverEZ(d, env, "gpu")
+        sv.step(0.0, steps)
+        sv.check_finite()
+        runs[np.dtype(dtype).name] = (d, sv)
+    g = list(env.grid().guard)
+    d0, d1, d2 = env.dims
+    out, rms = {}, {}
+    for name in FIELD_NAMES:
+        a = torch.as_tensor(_DeviceArray(runs["float32"][0].dev_ptr(name), (d2, d1, d0),
+                                         np.float32), device="cuda")
+        b = torch.as_tensor(_DeviceArray(runs["float64"][0].dev_ptr(name), (d2, d1, d0),
+                                         np.float64), device="cuda")
+        sl = (slice(g[2], d2 - g[2]), slice(g[1], d1 - g[1]), slice(g[0], d0 - g[0]))
+        ai, bi = a[sl].double(), b[sl]
+        den = torch.linalg.vector_norm(bi).item()
+        out[name] = torch.linalg.vector_norm(ai - bi).item() / den if den > 0 else 0.0
+        rms[name] = den / math.sqrt(bi.numel())
+        del a, b, ai, bi
+    for d, sv in runs.values():
+        sv.close()
+        d.close()
+    torch.cuda.synchronize()
+    return out, rms
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -350,6 +403,14 @@ def run_ours(args):
     e2e_value = job_throughput(cells, args.steps, ws, e2e_s)
     d2h_diag = 8 * (148 * 4)  # FP64 partials read back per energy diagnostic
 
+    err64 = None
+    if rank == 0 and ws == 1 and not args.no_fp64_check:
+        rel, rms = fp64_error(env, FP64_CHECK_STEPS, modes)
+        err64 = {"steps": FP64_CHECK_STEPS, "semantics": "reference GPU build, both precisions",
+                 "rel_l2": rel, "rms_fp64": rms,
+                 "note": ("P starts at 0 and grows from the rounding of div B, so its relative "
+                          "error is that of noise; compare its rms")}
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_run(steps=2, warmup=1)
@@ -381,6 +442,7 @@ def run_ours(args):
                     "h2d_bytes_per_step": nbytes / args.steps,
                     "d2h_bytes_per_step": nbytes / args.steps + d2h_diag},
             "cpu_baseline": cpu,
+            "error_vs_fp64": err64,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)
@@ -577,6 +639,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-check", action="store_true",
+                    help="skip the FP32-vs-FP64 error report of the turbulence run")
     ap.add_argument("--n", type=int, default=N_SIDE,
                     help="grid side of the turbulence workload (512 is the benchmark)")
     ap.add_argument("--workload", default="turbulence",
