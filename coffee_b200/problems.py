@@ -53,6 +53,49 @@ def alfven_fields(p: SimParams, dtype=np.float32, amp=0.1, width2=0.02, vz=0.1):
     return [a.astype(ft) for a in (Ex, Ey, Ez, Bx, By, Bz, P)]
 
 
+def _xyz(p: SimParams, dtype):
+    g = Grid.from_params(p, dtype)
+    z, y, x = g.coords(2, np.float64), g.coords(1, np.float64), g.coords(0, np.float64)
+    return np.meshgrid(z, y, x, indexing="ij")
+
+
+def alfven_plane_wave_fields(p: SimParams, dtype=np.float32, xi0=0.1):
+    """Plane Alfven wave on B0 = x-hat in a periodic box, the initial
+    condition of the reference's wave driver (``src/main-wave.cpp`` with
+    ``src/user_alfven.hpp``, its EZ branch): wave vector
+    k = (2 * 2 pi / Lx, 0, 2 pi / Lz), frequency w = k.B0 / |B0| (c = 1),
+    E along e = (k x B0) x B0 normalised, b = k x e, and
+    E = -xi0 sin(k.x) e, B = B0 - xi0 sin(k.x) b / w, P = 0."""
+    Z, Y, X = _xyz(p, dtype)
+    b0 = np.array([1.0, 0.0, 0.0])
+    k = np.array([2.0 * 2.0 * math.pi / p.size[0], 0.0, 1.0 * 2.0 * math.pi / p.size[2]])
+    w = float(k @ b0) / float(np.linalg.norm(b0))
+    e = np.cross(np.cross(k, b0), b0)
+    e = e / np.linalg.norm(e)
+    b = np.cross(k, e)
+    s = np.sin(k[0] * X + k[1] * Y + k[2] * Z)
+    E = [-xi0 * s * e[a] for a in range(3)]
+    B = [b0[a] - xi0 * s * b[a] / w for a in range(3)]
+    ft = np.dtype(dtype)
+    return [np.asarray(a, dtype=ft) for a in (*E, *B, np.zeros_like(X))]
+
+
+def emwave_fields(p: SimParams, dtype=np.float32):
+    """Vacuum electromagnetic plane wave (``src/user_emwave.hpp``): k in the
+    x-y plane, k = 2 pi (kn[0] / Lx, kn[1] / Ly), E = e sin(k.x) with the unit
+    vector e in the x-y plane normal to k, B = z-hat sin(k.x), P = 0."""
+    Z, Y, X = _xyz(p, dtype)
+    kx = p.kn[0] * 2.0 * math.pi / p.size[0]
+    ky = p.kn[1] * 2.0 * math.pi / p.size[1]
+    ex, ey = (1.0, -kx / ky) if ky != 0 else (-ky / kx, 1.0)
+    nrm = math.hypot(ex, ey)
+    ex, ey = ex / nrm, ey / nrm
+    s = np.sin(kx * X + ky * Y)
+    zero = np.zeros_like(X)
+    ft = np.dtype(dtype)
+    return [np.asarray(a, dtype=ft) for a in (ex * s, ey * s, zero, zero, zero, s, zero)]
+
+
 # ------------------------------------------------------------- turbulence
 
 TURB_SEED = 20261203
