@@ -19,11 +19,13 @@ ERRORS = {
 }
 
 FIELD_IDS = {"Ex": 0, "Ey": 1, "Ez": 2, "Bx": 3, "By": 4, "Bz": 5, "P": 6,
-             "Jx": 7, "Jy": 8, "Jz": 9, "divE": 10, "divB": 11}
+             "Jx": 7, "Jy": 8, "Jz": 9, "divE": 10, "divB": 11,
+             "B0x": 12, "B0y": 13, "B0z": 14}
 VARIANT_FLAT = 0
 VARIANT_LOGSPH = 1
 VARIANT_CYL = 2
 VARIANT_GR = 3
+VARIANT_YEE = 4
 KERNEL_STAGE_FIRST, KERNEL_STAGE, KERNEL_KO = 0, 1, 2
 SEM_CPU_REF = 0
 SEM_GPU_REF = 1

@@ -16,6 +16,7 @@
 #include "coffee_internal.h"
 #include "ez_launch.cuh"
 #include "variants.h"
+#include "yee_kernels.cuh"
 
 #define COFFEE_VERSION_STRING "coffee_b200 0.1 (sm_100a)"
 
@@ -114,10 +115,25 @@ __device__ __forceinline__ double warp_max(double v) {
 // COFFEE_DIAG_*.  The energy region is that of total_energy
 // (field_solver_EZ.cu:755-795): outside the star (problem 1) and strictly
 // inside the absorbing layers.
+// Staggered fields (COFFEE_VARIANT_YEE): each component is first
+// interpolated to the vertex, as field_solver::total_energy does
+// (field_solver.cu:829-866), and div B is the cell-centred forward
+// difference that the staggered update keeps constant.
+template <typename T>
+__device__ __forceinline__ void vertex_values(const F7<const T>& u, uint32_t o, int sy, int sz,
+                                              double e[3], double b[3]) {
+  e[0] = interp_at<kStE[0], kStRho>(u.p[0], o, sy, sz);
+  e[1] = interp_at<kStE[1], kStRho>(u.p[1], o, sy, sz);
+  e[2] = interp_at<kStE[2], kStRho>(u.p[2], o, sy, sz);
+  b[0] = interp_at<kStB[0], kStRho>(u.p[3], o, sy, sz);
+  b[1] = interp_at<kStB[1], kStRho>(u.p[4], o, sy, sz);
+  b[2] = interp_at<kStB[2], kStRho>(u.p[5], o, sy, sz);
+}
+
 template <typename T>
 __global__ void diag_kernel(const EzConst<T> c, const F7<const T> u, const int what,
                             const T pml_xl0, const T pml_xl1, const T pml_xl2, const T pml_xh0,
-                            const T pml_xh1, const T pml_xh2, double* partials) {
+                            const T pml_xh1, const T pml_xh2, const int stag, double* partials) {
   const GridGeom& g = c.g;
   const int n0 = g.N[0], n1 = g.N[1], n2 = g.N[2];
   const long long total = (long long)n0 * n1 * n2;
@@ -137,11 +153,26 @@ __global__ void diag_kernel(const EzConst<T> c, const F7<const T> u, const int w
       if (!in_star && x < pml_xh0 && x > pml_xl0 && y < pml_xh1 && y > pml_xl1 &&
           z < pml_xh2 && z > pml_xl2) {
         const int b = (what == COFFEE_DIAG_ENERGY_E) ? 0 : 3;
-        for (int a = 0; a < 3; ++a) {
-          const double f = (double)u.p[b + a][o];
-          v += f * f;
+        if (stag) {
+          double e[3], bb[3];
+          vertex_values(u, (uint32_t)o, (int)g.sy, (int)g.sz, e, bb);
+          const double* f = b == 0 ? e : bb;
+          v = f[0] * f[0] + f[1] * f[1] + f[2] * f[2];
+        } else {
+          for (int a = 0; a < 3; ++a) {
+            const double f = (double)u.p[b + a][o];
+            v += f * f;
+          }
         }
       }
+    } else if (what == COFFEE_DIAG_DIVB_L2 && stag) {
+      const long long s[3] = {1, g.sy, g.sz};
+      double d = 0.0;
+      for (int a = 0; a < 3; ++a) {
+        const T* f = u.p[3 + a];
+        d += ((double)f[o + s[a]] - (double)f[o]) * (double)c.inv_delta[a];
+      }
+      v = d * d;
     } else if (what == COFFEE_DIAG_DIVB_L2) {
       double d = 0.0;
       const long long s[3] = {1, g.sy, g.sz};
@@ -152,8 +183,11 @@ __global__ void diag_kernel(const EzConst<T> c, const F7<const T> u, const int w
       }
       v = d * d;
     } else {
-      const double ex = u.p[0][o], ey = u.p[1][o], ez = u.p[2][o];
-      const double bx = u.p[3][o], by = u.p[4][o], bz = u.p[5][o];
+      double e[3] = {u.p[0][o], u.p[1][o], u.p[2][o]};
+      double bb[3] = {u.p[3][o], u.p[4][o], u.p[5][o]};
+      if (stag) vertex_values(u, (uint32_t)o, (int)g.sy, (int)g.sz, e, bb);
+      const double ex = e[0], ey = e[1], ez = e[2];
+      const double bx = bb[0], by = bb[1], bz = bb[2];
       const double B2 = fmax(bx * bx + by * by + bz * bz, (double)Tiny<T>::v);
       if (what == COFFEE_DIAG_MAX_EDOTB)
         v = fabs(ex * bx + ey * by + ez * bz) / B2;
@@ -245,12 +279,13 @@ extern "C" int coffee_env_create(const coffee_params* p, int device, coffee_env*
   *out = nullptr;
   for (int a = 0; a < 3; ++a) {
     if (p->N[a] < 1) return fail(COFFEE_E_CONFIG, "N[%d] = %d must be >= 1", a, p->N[a]);
-    // an axis of one point without guards is the third axis of a 2D run
+    // an axis of one point without guards is the third axis of a 2D run;
+    // every solver reads at least one point beyond the update box (the EZ
+    // solvers check their own three at solver creation)
     const bool plane_axis = p->N[a] == 1 && p->guard[a] == 0;
-    if (!plane_axis && p->guard[a] < p->shift_ghost + 3)
-      return fail(COFFEE_E_CONFIG,
-                  "guard[%d] = %d: the KO stencil needs guard >= shift_ghost + 3 = %d", a,
-                  p->guard[a], p->shift_ghost + 3);
+    if (!plane_axis && p->guard[a] < p->shift_ghost + 1)
+      return fail(COFFEE_E_CONFIG, "guard[%d] = %d: needs guard >= shift_ghost + 1 = %d", a,
+                  p->guard[a], p->shift_ghost + 1);
     if (p->periodic_boundary[a] && p->N[a] < p->guard[a])
       return fail(COFFEE_E_CONFIG, "periodic axis %d needs N >= guard (N=%d, guard=%d)", a,
                   p->N[a], p->guard[a]);
@@ -531,7 +566,8 @@ extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int varia
   *out = nullptr;
   if (f->env != env) return fail(COFFEE_E_INVALID, "fields belong to another environment");
   if (variant != COFFEE_VARIANT_FLAT && variant != COFFEE_VARIANT_LOGSPH &&
-      variant != COFFEE_VARIANT_CYL && variant != COFFEE_VARIANT_GR)
+      variant != COFFEE_VARIANT_CYL && variant != COFFEE_VARIANT_GR &&
+      variant != COFFEE_VARIANT_YEE)
     return fail(COFFEE_E_INVALID, "solver variant %d is not available", variant);
   if (semantics != COFFEE_SEM_CPU_REF && semantics != COFFEE_SEM_GPU_REF)
     return fail(COFFEE_E_INVALID, "unknown semantics %d", semantics);
@@ -545,7 +581,9 @@ extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int varia
                     a);
   } else {
     // the reference has these solvers only in its GPU build
-    int rc = variant == COFFEE_VARIANT_GR ? gr_check(env) : axisym_check(env, variant);
+    int rc = variant == COFFEE_VARIANT_GR    ? gr_check(env)
+             : variant == COFFEE_VARIANT_YEE ? yee_check(env)
+                                             : axisym_check(env, variant);
     if (rc) return rc;
   }
   COFFEE_CUDA_TRY(cudaSetDevice(env->device));
@@ -560,8 +598,10 @@ extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int varia
   s->timing = 0;
   s->events_used = 0;
   s->synced_generation = 0;
-  // the GR solver's inner absorbing region always needs the start-of-step copy
-  bool abs_any = env->p.shift_ghost > 0 || variant == COFFEE_VARIANT_GR;
+  // the GR solver's inner absorbing region always needs the start-of-step
+  // copy; the staggered solver's substeps read it
+  bool abs_any = env->p.shift_ghost > 0 || variant == COFFEE_VARIANT_GR ||
+                 variant == COFFEE_VARIANT_YEE;
   for (int a = 0; a < 3; ++a) abs_any = abs_any || env->p.pml[a] > 0;
   s->absorbing = abs_any;
   const size_t bytes = f->n * f->elem;
@@ -587,6 +627,7 @@ extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int varia
     }
   }
   int rc = variant == COFFEE_VARIANT_GR     ? gr_setup(env, f->elem, &s->vtab)
+           : variant == COFFEE_VARIANT_YEE  ? COFFEE_OK
            : variant != COFFEE_VARIANT_FLAT ? axisym_setup(env, variant, f->elem, &s->vtab)
            : (f->elem == 4)               ? configure_solver<float>(s)
                                           : configure_solver<double>(s);
@@ -633,6 +674,8 @@ extern "C" int coffee_solver_destroy(coffee_solver* s) {
 extern "C" int coffee_solver_set_aux(coffee_solver* s, int enable) {
   clear_error();
   if (!s) return fail(COFFEE_E_INVALID, "coffee_solver_set_aux: null argument");
+  if (enable && s->variant == COFFEE_VARIANT_YEE)
+    return fail(COFFEE_E_INVALID, "the staggered solver writes no J, divE, divB");
   if (enable)
     for (int id = COFFEE_JX; id <= COFFEE_DIVB; ++id) {
       int rc = ensure_field(s->f, id);
@@ -651,6 +694,10 @@ extern "C" int coffee_solver_set_timing(coffee_solver* s, int enable) {
 extern "C" int coffee_solver_launches_per_step(coffee_solver* s) {
   if (s && s->variant == COFFEE_VARIANT_LOGSPH) return 12;  // + axis after each, + 1 per call
   if (s && s->variant == COFFEE_VARIANT_GR) return 11;      // + an E, H pass before each stage
+  if (s && s->variant == COFFEE_VARIANT_YEE)
+    // shell + update + clamp per substep; the star boundary adds its three
+    // passes and the guard pass (the box problem: one guard pass per call)
+    return s->env->p.problem == 1 ? 21 : 9;
   return 6;  // 5 stage kernels + 1 KO kernel
 }
 
@@ -707,6 +754,15 @@ static int run_steps(coffee_solver* s, double time, int nsteps) {
   s->events_used = 0;
   EventHook hook(s);
   if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(s->ev_begin, st));
+  if (s->variant == COFFEE_VARIANT_YEE) {
+    void* b0[3] = {f->d[COFFEE_B0X], f->d[COFFEE_B0Y], f->d[COFFEE_B0Z]};
+    const bool has_b0 = b0[0] && b0[1] && b0[2];
+    int rc = yee_steps(s->env, f->elem, f->d, has_b0 ? b0 : nullptr, s->dU, s->Un, s->B, time,
+                       nsteps, st, s->timing ? &hook : nullptr);
+    if (rc) return rc;
+    if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(s->ev_end, st));
+    return COFFEE_OK;
+  }
   if (s->variant != COFFEE_VARIANT_FLAT) {
     void* auxp[5];
     for (int a = 0; a < 5; ++a) auxp[a] = f->d[COFFEE_JX + a];
@@ -875,9 +931,10 @@ static int diag_t(coffee_solver* s, int what, double* out) {
     xh[a] = (T)p.lower[a] + (T)p.size[a] - (T)p.pml[a] * c.delta[a];
     xl[a] = (T)p.lower[a] + (T)p.pml[a] * c.delta[a];
   }
+  const int stag = s->variant == COFFEE_VARIANT_YEE ? 1 : 0;
   diag_kernel<T><<<s->partial_blocks, 256, 0, s->stream>>>(c, f7c<T>(s->f->d), what, xl[0],
                                                            xl[1], xl[2], xh[0], xh[1], xh[2],
-                                                           s->d_partials);
+                                                           stag, s->d_partials);
   COFFEE_CUDA_TRY(cudaGetLastError());
   std::vector<double> h(s->partial_blocks);
   COFFEE_CUDA_TRY(cudaMemcpyAsync(h.data(), s->d_partials, sizeof(double) * h.size(),

@@ -63,4 +63,12 @@ int gr_steps(const coffee_env* env, int elem, void* ehbuf, void* const A[7], voi
              void* const dU[7], void* const Un[7], void* const aux[5], int nsteps,
              cudaStream_t st, LaunchHook* hook);
 
+// Staggered (Yee) RK3 solver (COFFEE_VARIANT_YEE).  A: state E, B (and P,
+// untouched); B0: background field or null; Es: E*, B' scratch; Un: the
+// start-of-step copies; Tb: scratch of the star boundary.
+int yee_check(const coffee_env* env);
+int yee_steps(const coffee_env* env, int elem, void* const A[7], void* const B0[3],
+              void* const Es[7], void* const Un[7], void* const Tb[7], double time, int nsteps,
+              cudaStream_t st, LaunchHook* hook);
+
 }  // namespace coffee

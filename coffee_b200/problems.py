@@ -53,47 +53,70 @@ def alfven_fields(p: SimParams, dtype=np.float32, amp=0.1, width2=0.02, vz=0.1):
     return [a.astype(ft) for a in (Ex, Ey, Ez, Bx, By, Bz, P)]
 
 
-def _xyz(p: SimParams, dtype):
+def _xyz(p: SimParams, dtype, stagger: int = 0b111):
+    """Z, Y, X of every grid point at `stagger` (bit a set: the vertex along
+    axis a, clear: half a cell above it; ``Grid::pos``, src/data/grid.h:103-134)."""
     g = Grid.from_params(p, dtype)
-    z, y, x = g.coords(2, np.float64), g.coords(1, np.float64), g.coords(0, np.float64)
-    return np.meshgrid(z, y, x, indexing="ij")
+    c = [g.coords(a, np.float64) + (0.0 if (stagger >> a) & 1 else 0.5 * g.delta[a])
+         for a in range(3)]
+    return np.meshgrid(c[2], c[1], c[0], indexing="ij")
 
 
-def alfven_plane_wave_fields(p: SimParams, dtype=np.float32, xi0=0.1):
+# Stagger of each component on the staggered (Yee) grid (src/data/sim_data.cpp:19-25)
+YEE_STAGGER = (0b110, 0b101, 0b011, 0b001, 0b010, 0b100, 0b111)
+
+
+def _per_component(fn, p: SimParams, dtype, yee: bool):
+    """The 7 arrays fn(Z, Y, X, c) (c = 0..6: Ex Ey Ez Bx By Bz P, float64),
+    each component taken at its own position on the staggered grid when
+    `yee` (what vector_field::initialize does with the Yee staggering) or at
+    the vertices otherwise."""
+    ft = np.dtype(dtype)
+    if not yee:
+        Z, Y, X = _xyz(p, dtype)
+        return [np.asarray(fn(Z, Y, X, c), dtype=ft) for c in range(7)]
+    return [np.asarray(fn(*_xyz(p, dtype, st), c), dtype=ft) for c, st in enumerate(YEE_STAGGER)]
+
+
+def alfven_plane_wave_fields(p: SimParams, dtype=np.float32, xi0=0.1, yee: bool = False):
     """Plane Alfven wave on B0 = x-hat in a periodic box, the initial
     condition of the reference's wave driver (``src/main-wave.cpp`` with
     ``src/user_alfven.hpp``, its EZ branch): wave vector
     k = (2 * 2 pi / Lx, 0, 2 pi / Lz), frequency w = k.B0 / |B0| (c = 1),
     E along e = (k x B0) x B0 normalised, b = k x e, and
-    E = -xi0 sin(k.x) e, B = B0 - xi0 sin(k.x) b / w, P = 0."""
-    Z, Y, X = _xyz(p, dtype)
+    E = -xi0 sin(k.x) e, B = B0 - xi0 sin(k.x) b / w, P = 0.  With `yee`
+    each component is evaluated at its staggered position."""
     b0 = np.array([1.0, 0.0, 0.0])
     k = np.array([2.0 * 2.0 * math.pi / p.size[0], 0.0, 1.0 * 2.0 * math.pi / p.size[2]])
     w = float(k @ b0) / float(np.linalg.norm(b0))
     e = np.cross(np.cross(k, b0), b0)
     e = e / np.linalg.norm(e)
     b = np.cross(k, e)
-    s = np.sin(k[0] * X + k[1] * Y + k[2] * Z)
-    E = [-xi0 * s * e[a] for a in range(3)]
-    B = [b0[a] - xi0 * s * b[a] / w for a in range(3)]
-    ft = np.dtype(dtype)
-    return [np.asarray(a, dtype=ft) for a in (*E, *B, np.zeros_like(X))]
+
+    def fn(Z, Y, X, c):
+        if c == 6:
+            return np.zeros_like(X)
+        s = np.sin(k[0] * X + k[1] * Y + k[2] * Z)
+        return -xi0 * s * e[c] if c < 3 else b0[c - 3] - xi0 * s * b[c - 3] / w
+    return _per_component(fn, p, dtype, yee)
 
 
-def emwave_fields(p: SimParams, dtype=np.float32):
+def emwave_fields(p: SimParams, dtype=np.float32, yee: bool = False):
     """Vacuum electromagnetic plane wave (``src/user_emwave.hpp``): k in the
     x-y plane, k = 2 pi (kn[0] / Lx, kn[1] / Ly), E = e sin(k.x) with the unit
-    vector e in the x-y plane normal to k, B = z-hat sin(k.x), P = 0."""
-    Z, Y, X = _xyz(p, dtype)
+    vector e in the x-y plane normal to k, B = z-hat sin(k.x), P = 0.  With
+    `yee` each component is evaluated at its staggered position."""
     kx = p.kn[0] * 2.0 * math.pi / p.size[0]
     ky = p.kn[1] * 2.0 * math.pi / p.size[1]
     ex, ey = (1.0, -kx / ky) if ky != 0 else (-ky / kx, 1.0)
     nrm = math.hypot(ex, ey)
     ex, ey = ex / nrm, ey / nrm
-    s = np.sin(kx * X + ky * Y)
-    zero = np.zeros_like(X)
-    ft = np.dtype(dtype)
-    return [np.asarray(a, dtype=ft) for a in (ex * s, ey * s, zero, zero, zero, s, zero)]
+
+    def fn(Z, Y, X, c):
+        if c not in (0, 1, 5):
+            return np.zeros_like(X)
+        return {0: ex, 1: ey, 5: 1.0}[c] * np.sin(kx * X + ky * Y)
+    return _per_component(fn, p, dtype, yee)
 
 
 # ------------------------------------------------------------- turbulence
@@ -239,19 +262,18 @@ def _dipole2(x, y, z, p1, p2, p3, phase, tiny):
     return [(3.0 * q * pr / (r2 + tiny) - pq) / den for q, pq in ((x, p1t), (y, p2t), (z, p3t))]
 
 
-def pulsar_fields(p: SimParams, dtype=np.float32):
+def pulsar_fields(p: SimParams, dtype=np.float32, yee: bool = False):
     """B = b0 * dipole(p1, p2, p3), E = 0, P = 0 at every point
-    (``src/user_pulsar3d_EZ.hpp``; the quadrupole terms are zero unless set)."""
-    g = Grid.from_params(p, dtype)
+    (``src/user_pulsar3d_EZ.hpp``; the quadrupole terms are zero unless set).
+    With `yee`, each B component at its staggered position
+    (``src/user_pulsar3d.hpp``, the staggered solver's initial condition)."""
     tiny = 1e-7 if np.dtype(dtype) == np.float32 else 1e-11
-    x = g.coords(0, np.float64)
-    y = g.coords(1, np.float64)
-    z = g.coords(2, np.float64)
-    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
-    b = _dipole2(X, Y, Z, p.p1, p.p2, p.p3, 0.0, tiny)
-    zeros = np.zeros_like(X)
-    arrs = [zeros, zeros, zeros, p.b0 * b[0], p.b0 * b[1], p.b0 * b[2], zeros]
-    return [np.asarray(a, dtype=dtype).copy() for a in arrs]
+
+    def fn(Z, Y, X, c):
+        if c < 3 or c == 6:
+            return np.zeros_like(X)
+        return p.b0 * _dipole2(X, Y, Z, p.p1, p.p2, p.p3, 0.0, tiny)[c - 3]
+    return [a.copy() for a in _per_component(fn, p, dtype, yee)]
 
 
 # ------------------------------------------------ 2D log-spherical pulsar

@@ -121,6 +121,14 @@ class SimData:
             raise ValueError(f"array shape {a.shape} != grid {self.shape}")
         check(self.lib.coffee_fields_upload(self.handle, int(fid), a.ctypes.data_as(ctypes.c_void_p)))
 
+    def upload_background(self, arrays):
+        """sim_data::B0 (3 host arrays), the background field the staggered
+        solver subtracts in curl B."""
+        if len(arrays) != 3:
+            raise ValueError("need 3 arrays (B0x B0y B0z)")
+        for fid, a in zip(("B0x", "B0y", "B0z"), arrays):
+            self.upload_field(_lib.FIELD_IDS[fid], a)
+
     def upload_packed(self, buf: np.ndarray):
         """Upload 7 arrays stored back to back in one (pinned or pageable) buffer."""
         check(self.lib.coffee_fields_upload(self.handle, -1, buf.ctypes.data_as(ctypes.c_void_p)))
@@ -304,6 +312,21 @@ class FieldSolverGrEZ(FieldSolverEZ):
     (set_aux) receive J, div D and div B."""
 
     VARIANT = _lib.VARIANT_GR
+
+    def __init__(self, data: SimData, env: SimEnvironment, stream: int | None = None):
+        super().__init__(data, env, semantics="gpu", stream=stream)
+
+
+class FieldSolver(FieldSolverEZ):
+    """``field_solver(sim_data&, sim_environment&)`` (src/algorithms/field_solver.h:8-35):
+    the staggered (Yee) solver, 2nd-order curl, SSP-RK3, the force-free
+    current from rho = div E, and E.B = 0 / |E| <= |B| after the substeps
+    (src/algorithms/field_solver.cu:690-726).  E and B sit on the staggered
+    positions of src/data/sim_data.cpp:19-25; sim_data's B0
+    (``SimData.upload_background``) is subtracted in curl B.  The reference
+    has it only in its GPU build.  Problems 0 (box) and 1 (rotating star)."""
+
+    VARIANT = _lib.VARIANT_YEE
 
     def __init__(self, data: SimData, env: SimEnvironment, stream: int | None = None):
         super().__init__(data, env, semantics="gpu", stream=stream)

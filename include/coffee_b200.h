@@ -13,6 +13,9 @@
  *   sim_environment  (src/sim_env.h:17-87)      -> coffee_env
  *   sim_data         (src/data/sim_data.h:11-24) -> coffee_fields
  *   field_solver_EZ  (src/algorithms/field_solver_EZ.h:6-33) -> coffee_solver
+ * The reference's staggered RK3 solver, Coffee::field_solver::evolve_fields
+ * (src/algorithms/field_solver.h:8-35, src/algorithms/field_solver.cu:690-726),
+ * is the variant COFFEE_VARIANT_YEE of the same handle.
  * include/coffee_b200.hpp re-creates the reference's C++ classes on top of
  * these calls.
  *
@@ -55,13 +58,19 @@ enum {
 enum { /* field ids for coffee_fields_ptr / upload / download */
   COFFEE_EX = 0, COFFEE_EY, COFFEE_EZ, COFFEE_BX, COFFEE_BY, COFFEE_BZ, COFFEE_P,
   COFFEE_JX, COFFEE_JY, COFFEE_JZ, COFFEE_DIVE, COFFEE_DIVB,
+  /* background field sim_data::B0, read by the staggered solver (allocated
+   * on first use; zero until written) */
+  COFFEE_B0X, COFFEE_B0Y, COFFEE_B0Z,
   COFFEE_NUM_FIELDS
 };
 enum { /* solver variants */
   COFFEE_VARIANT_FLAT = 0,   /* Cartesian EZ, field_solver_EZ */
   COFFEE_VARIANT_LOGSPH = 1, /* 2D log-spherical EZ, field_solver_EZ_spherical (GPU build) */
   COFFEE_VARIANT_CYL = 2,    /* 2D cylindrical EZ, field_solver_EZ_cylindrical (GPU build) */
-  COFFEE_VARIANT_GR = 3      /* Kerr-Schild GR EZ, field_solver_gr_EZ (GPU build); E holds D */
+  COFFEE_VARIANT_GR = 3,     /* Kerr-Schild GR EZ, field_solver_gr_EZ (GPU build); E holds D */
+  COFFEE_VARIANT_YEE = 4     /* staggered (Yee) RK3, field_solver (GPU build only): E and B on
+                              * the staggered positions of sim_data.cpp:19-25, B0 subtracted
+                              * in curl B; problems 0 and 1, shift_ghost 0 */
 };
 enum { /* which reference build the flat solver reproduces */
   COFFEE_SEM_CPU_REF = 0, /* field_solver_EZ.cpp (the parity oracle build) */
@@ -192,15 +201,18 @@ COFFEE_API int coffee_solver_destroy(coffee_solver* s);
 COFFEE_API int coffee_solver_step(coffee_solver* s, double time, int nsteps);
 /* Request J, divE, divB (the reference stores them on every stage) to be
  * written by the last stage of the following steps (1) or not (0, the
- * default: they cost 20 bytes per cell per stage). */
+ * default: they cost 20 bytes per cell per stage).  The staggered solver
+ * has no such outputs (COFFEE_E_INVALID). */
 COFFEE_API int coffee_solver_set_aux(coffee_solver* s, int enable);
 /* Bracket every kernel launch of the following coffee_solver_step calls with
  * CUDA events on the solver's stream (1) or not (0, the default). */
 COFFEE_API int coffee_solver_set_timing(coffee_solver* s, int enable);
 enum { /* kernel kinds reported by coffee_solver_last_timing */
-  COFFEE_KERNEL_STAGE_FIRST = 0, /* first LSRK stage (As = 0: dU is not read) */
-  COFFEE_KERNEL_STAGE = 1,       /* LSRK stages 2-5 */
-  COFFEE_KERNEL_KO = 2           /* Kreiss-Oliger + clamps + boundary pass */
+  COFFEE_KERNEL_STAGE_FIRST = 0, /* first LSRK stage (As = 0: dU is not read);
+                                  * staggered solver: update pass of substep 1 */
+  COFFEE_KERNEL_STAGE = 1,       /* LSRK stages 2-5; staggered: update passes 2-3 */
+  COFFEE_KERNEL_KO = 2           /* Kreiss-Oliger + clamps + boundary pass;
+                                  * staggered: the clamp passes */
 };
 /* Device time of the last coffee_solver_step call in timing mode: summed
  * milliseconds ms[kind] and launch counts launches[kind] per kernel kind,

@@ -6,13 +6,18 @@
 //           sph  field_solver_EZ_spherical  (src/algorithms/field_solver_EZ_spherical.cu)
 //           cyl  field_solver_EZ_cylindrical(src/algorithms/field_solver_EZ_cylindrical.cu)
 //           gr   field_solver_gr_EZ         (src/algorithms/field_solver_gr_EZ.cu)
+//           yee  field_solver               (src/algorithms/field_solver.cu), the
+//                staggered RK3 solver; keeps sim_data's Yee staggering
+//                (src/data/sim_data.cpp:19-25) and, when IN.fld holds 10
+//                arrays, loads arrays 7-9 as the background field B0
 //
 // The config is read by the reference's parse_config through the single-rank
 // environment double (ref_gpu_env.cu), which also fills the reference's
 // __constant__ dev_params / dev_grid.  IN.fld holds E, B, P with guard cells
 // in the reference layout (i fastest).  The driver:
 //   1. builds sim_data, sets the collocated stagger 0b111 as the reference's
-//      user files do (src/user_pulsar_sph.hpp:6-9, src/user_wald2.hpp:7-11);
+//      user files do (src/user_pulsar_sph.hpp:6-9, src/user_wald2.hpp:7-11),
+//      except for yee;
 //   2. constructs the solver (before the data is loaded, as the reference's
 //      drivers do: src/main-pulsar2d-spherical.cpp:25-27);
 //   3. loads E, B, P to the host arrays and copies them to the device; the
@@ -43,6 +48,7 @@
 #include "algorithms/field_solver_EZ_cylindrical.h"
 #include "algorithms/field_solver_EZ_spherical.h"
 #include "algorithms/field_solver_gr_EZ.h"
+#include "algorithms/field_solver.h"
 #include "coffee_fld.h"
 #include "data/sim_data.h"
 #include "sim_env.h"
@@ -51,7 +57,7 @@ using namespace Coffee;
 
 int main(int argc, char** argv) {
   if (argc < 5) {
-    std::fprintf(stderr, "usage: %s ez|sph|cyl|gr IN.fld OUT.fld NSTEPS [--aux] [--warmup W]\n",
+    std::fprintf(stderr, "usage: %s ez|sph|cyl|gr|yee IN.fld OUT.fld NSTEPS [--aux] [--warmup W]\n",
                  argv[0]);
     return 2;
   }
@@ -68,7 +74,8 @@ int main(int argc, char** argv) {
       return 2;
     }
   }
-  if (solver_name != "ez" && solver_name != "sph" && solver_name != "cyl" && solver_name != "gr") {
+  if (solver_name != "ez" && solver_name != "sph" && solver_name != "cyl" && solver_name != "gr" &&
+      solver_name != "yee") {
     std::fprintf(stderr, "unknown solver %s\n", solver_name.c_str());
     return 2;
   }
@@ -99,10 +106,12 @@ int main(int argc, char** argv) {
   }
 
   sim_data data(env);
-  Stagger st[3] = {Stagger(0b111), Stagger(0b111), Stagger(0b111)};
-  data.E.set_stagger(st);
-  data.B.set_stagger(st);
-  data.B0.set_stagger(st);
+  if (solver_name != "yee") {
+    Stagger st[3] = {Stagger(0b111), Stagger(0b111), Stagger(0b111)};
+    data.E.set_stagger(st);
+    data.B.set_stagger(st);
+    data.B0.set_stagger(st);
+  }
 
   // Silence the reference's own prints (block sizes, per-phase timers).
   std::fflush(stdout);
@@ -114,6 +123,7 @@ int main(int argc, char** argv) {
   std::unique_ptr<field_solver_EZ_spherical> s_sph;
   std::unique_ptr<field_solver_EZ_cylindrical> s_cyl;
   std::unique_ptr<field_solver_gr_EZ> s_gr;
+  std::unique_ptr<field_solver> s_yee;
   std::function<void(Scalar)> evolve;
   if (solver_name == "ez") {
     s_ez.reset(new field_solver_EZ(data, env));
@@ -124,9 +134,12 @@ int main(int argc, char** argv) {
   } else if (solver_name == "cyl") {
     s_cyl.reset(new field_solver_EZ_cylindrical(data, env));
     evolve = [&](Scalar t) { s_cyl->evolve_fields(t); };
-  } else {
+  } else if (solver_name == "gr") {
     s_gr.reset(new field_solver_gr_EZ(data, env));
     evolve = [&](Scalar t) { s_gr->evolve_fields(t); };
+  } else {
+    s_yee.reset(new field_solver(data, env));
+    evolve = [&](Scalar t) { s_yee->evolve_fields(t); };
   }
 
   Scalar* dst[7] = {data.E.host_ptr(0), data.E.host_ptr(1), data.E.host_ptr(2),
@@ -134,6 +147,17 @@ int main(int argc, char** argv) {
                     data.P.host_ptr()};
   for (int f = 0; f < 7; ++f)
     std::memcpy(dst[f], payload.data() + f * n * sizeof(Scalar), n * sizeof(Scalar));
+  {
+    // B0 as the user files leave it (data.B0.initialize(): zero), or
+    // arrays 7-9 of IN.fld for the staggered solver
+    Scalar* b0[3] = {data.B0.host_ptr(0), data.B0.host_ptr(1), data.B0.host_ptr(2)};
+    for (int f = 0; f < 3; ++f) {
+      if (solver_name == "yee" && hin.nfields >= 10)
+        std::memcpy(b0[f], payload.data() + (7 + f) * n * sizeof(Scalar), n * sizeof(Scalar));
+      else
+        std::memset(b0[f], 0, n * sizeof(Scalar));
+    }
+  }
   payload.clear();
   payload.shrink_to_fit();
   data.sync_to_device();
