@@ -456,15 +456,21 @@ def run_ours(args):
 
 # ------------------------------------------------- other solvers' workloads
 # Not the headline: measurement lines for the configurations of the other
-# solvers (--workload gr-wald | logsph-batch | logsph | cyl-pulsar).  Their reference
-# implementation exists only as the reference's GPU build, which
-# --impl reference times on the same case.
+# solvers (--workload gr-wald | logsph-batch | logsph | cyl-pulsar | yee-wave |
+# yee-pulsar).  Their reference implementation exists only as the reference's
+# GPU build, which --impl reference times on the same case.
 
-VARIANT_STAGE_BYTES = {"gr-wald": 136, "logsph-batch": 112, "logsph": 112, "cyl-pulsar": 112}
+# Algorithmic bytes per cell of the timed kernel: the LSRK stage kernels of
+# the EZ solvers; for the staggered solver the update pass of substeps 2-3,
+# which reads E, B and their start-of-step copies and writes E*, B'
+# (12 + 6 arrays of 4 bytes).
+VARIANT_STAGE_BYTES = {"gr-wald": 136, "logsph-batch": 112, "logsph": 112, "cyl-pulsar": 112,
+                       "yee-wave": 72, "yee-pulsar": 72}
 
 
-def _variant_cases(workload):
-    """(list of (solver class name, params, FP32 fields), description)."""
+def _variant_cases(workload, n=512):
+    """(list of (solver class name, params, FP32 fields), description); n is
+    the grid side of the staggered workloads (512 is the benchmark)."""
     import numpy as np
 
     from coffee_b200 import problems
@@ -474,6 +480,22 @@ def _variant_cases(workload):
         return [("FieldSolverGrEZ", "gr", p, problems.wald_fields(p, np.float32))], {
             "workload": "gr-wald256", "grid": [256] * 3, "spin": 0.9, "domain": [-20, 20],
             "pml": 16, "note": "Wald field B0 = 1 along the spin axis, E = 0, P = 0"}
+    if workload == "yee-wave":
+        p = problems.alfven_params(N=n, guard=2)
+        p.dt = 0.3 / n
+        return [("FieldSolver", "yee", p,
+                 problems.alfven_plane_wave_fields(p, np.float32, yee=True))], {
+            "workload": f"yee-alfven{n}", "grid": [n] * 3, "guard": 2,
+            "solver": "staggered SSP-RK3 (field_solver)", "cfl": 0.3,
+            "note": "plane Alfven wave on B0 = x-hat, k = 2 pi (2, 0, 1), periodic box"}
+    if workload == "yee-pulsar":
+        p = problems.pulsar_params(N=n, guard=2, half_size=64.0, radius=4.0, omega=0.05,
+                                   pml=n // 16)
+        p.dt = 0.3 * (128.0 / n)
+        return [("FieldSolver", "yee", p, problems.pulsar_fields(p, np.float32, yee=True))], {
+            "workload": f"yee-pulsar{n}", "grid": [n] * 3, "guard": 2,
+            "solver": "staggered SSP-RK3 (field_solver)", "domain": [-64, 64], "radius": 4.0,
+            "omega": 0.05, "pml": n // 16, "note": "rotating dipole star, absorbing layer"}
     if workload == "logsph":
         p = problems.sph_pulsar_params(nr=2048, nth=1024, guard=4, omega=0.2)
         return [("FieldSolverEZSpherical", "sph", p, problems.sph_pulsar_fields(p, np.float32))], {
@@ -507,7 +529,7 @@ def run_variant(args):
 
         if rank != 0:
             return 0
-        runs, cfg = _variant_cases(args.workload)
+        runs, cfg = _variant_cases(args.workload, args.n)
         secs, cells = 0.0, 0
         for _cls, name, p, f in runs:
             oracle.run_reference_gpu(name, p, f, args.warmup)
@@ -533,7 +555,7 @@ def run_variant(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
-    runs, cfg = _variant_cases(args.workload)
+    runs, cfg = _variant_cases(args.workload, args.n)
     objs = []
     cells = 0
     for cls_name, _name, p, f in runs:
@@ -575,15 +597,24 @@ def run_variant(args):
         objs[0][2].set_timing(False)
         n_stage = timing["launches"]["stage"]
         avg = timing["ms"]["stage"] / max(1, n_stage)
-        kname = {"gr-wald": "gr_stage_kernel", "cyl-pulsar": "cyl_stage_kernel",
-                 "logsph": "sph_stage_kernel"}[args.workload]
-        roof = {"kernel": kname + " (LSRK stages 2-5)", "bound": "hbm",
+        kname = {"gr-wald": "gr_stage_kernel (LSRK stages 2-5)",
+                 "cyl-pulsar": "cyl_stage_kernel (LSRK stages 2-5)",
+                 "logsph": "sph_stage_kernel (LSRK stages 2-5)",
+                 "yee-wave": "yee_update_kernel (substeps 2-3)",
+                 "yee-pulsar": "yee_update_kernel (substeps 2-3)"}[args.workload]
+        roof = {"kernel": kname, "bound": "hbm",
                 "achieved": VARIANT_STAGE_BYTES[args.workload] * cells / (avg / 1e3) / 1e9,
                 "peak": peak, "unit": "GB/s", "peak_kind": peak_kind, "traffic": None,
                 "algorithmic_bytes_per_launch": VARIANT_STAGE_BYTES[args.workload] * cells,
                 "avg_launch_ms": avg}
         launches = sum(timing["launches"].values())
         launch_note = "stage + KO kernels counted by the solver's launch hooks"
+        if args.workload.startswith("yee"):
+            per_call = 0 if runs[0][2].problem == 1 else 1
+            launches = objs[0][2].launches_per_step() * args.steps + per_call
+            launch_note = ("per substep: shell copy, update and clamp passes; the star problem "
+                           "adds three star passes and a guard pass (box problem: one guard pass "
+                           "per call)")
     else:
         roof = {"kernel": "whole batched step (stage, axis and KO launches)", "bound": "hbm",
                 "achieved": BYTES_STEP * cells / (step_ms / 1e3) / 1e9, "peak": peak,
@@ -642,9 +673,11 @@ def main():
     ap.add_argument("--no-fp64-check", action="store_true",
                     help="skip the FP32-vs-FP64 error report of the turbulence run")
     ap.add_argument("--n", type=int, default=N_SIDE,
-                    help="grid side of the turbulence workload (512 is the benchmark)")
+                    help="grid side of the turbulence and staggered workloads (512 is the "
+                         "benchmark)")
     ap.add_argument("--workload", default="turbulence",
-                    choices=["turbulence", "gr-wald", "logsph-batch", "logsph", "cyl-pulsar"])
+                    choices=["turbulence", "gr-wald", "logsph-batch", "logsph", "cyl-pulsar",
+                             "yee-wave", "yee-pulsar"])
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

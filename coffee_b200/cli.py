@@ -20,6 +20,9 @@ max_steps, a snapshot every ``snapshot_interval`` steps, an output every
 | gr | main-gr.cpp | any | user_wald2.hpp | field_solver_gr_EZ |
 | pulsar2d-spherical | main-pulsar2d-spherical.cpp | any | user_pulsar_sph.hpp | field_solver_EZ_spherical |
 | pulsar2d-cylindrical | main-pulsar2d-cylindrical.cpp | any | user_pulsar.hpp | field_solver_EZ_cylindrical |
+| wave-yee | main-wave.cpp without EZ | 0 | user_alfven.hpp (staggered branch) | field_solver |
+| pulsar3d-yee | main-pulsar3d.cpp without EZ | 1 | user_pulsar3d.hpp | field_solver |
+| alfven3d-yee | main-alfven3d.cpp without EZ | 2 | user_pulsar3d.hpp | field_solver |
 
 Outputs go to DIR (default ``Data``): ``fld.NNNNN.fld`` holds E, B, P and
 J, div E, div B of the output step on every ``downsample``-th interior point
@@ -27,7 +30,8 @@ J, div E, div B of the output step on every ``downsample``-th interior point
 field-file format since HDF5 is not part of it); ``snapshot.NNNNN.fld`` is a
 full restart state (``coffee_solver_save_snapshot``); ``energy.txt`` gets
 one line ``step time Wb We`` per output (the energy file of
-``main-wave.cpp``), flat solvers only.  Steps between two events run as one
+``main-wave.cpp``), Cartesian solvers only (the staggered solver's energies
+interpolate every component to the vertices, as its total_energy does).  Steps between two events run as one
 ``coffee_solver_step`` call, which advances time exactly as the loop does.
 """
 from __future__ import annotations
@@ -43,7 +47,7 @@ from . import problems
 from .config import SimParams
 from .fld import write_fld
 
-FLAT, GR, SPH, CYL = "flat", "gr", "sph", "cyl"
+FLAT, GR, SPH, CYL, YEE = "flat", "gr", "sph", "cyl", "yee"
 
 
 @dataclass(frozen=True)
@@ -64,6 +68,10 @@ DRIVERS = {d.name: d for d in (
     Driver("pulsar2d-spherical", "main-pulsar2d-spherical.cpp", None, SPH, "sph_pulsar_fields"),
     Driver("pulsar2d-cylindrical", "main-pulsar2d-cylindrical.cpp", None, CYL,
            "cyl_pulsar_fields"),
+    # the same programs built without EZ: the staggered solver field_solver
+    Driver("wave-yee", "main-wave.cpp", 0, YEE, "alfven_plane_wave_fields"),
+    Driver("pulsar3d-yee", "main-pulsar3d.cpp", 1, YEE, "pulsar_fields"),
+    Driver("alfven3d-yee", "main-alfven3d.cpp", 2, YEE, "pulsar_fields"),
 )}
 
 
@@ -115,7 +123,7 @@ def _solver(kind, data, env, sem_gpu):
     if kind == FLAT:
         return sv.FieldSolverEZ(data, env, "gpu" if sem_gpu else "cpu")
     return {GR: sv.FieldSolverGrEZ, SPH: sv.FieldSolverEZSpherical,
-            CYL: sv.FieldSolverEZCylindrical}[kind](data, env)
+            CYL: sv.FieldSolverEZCylindrical, YEE: sv.FieldSolver}[kind](data, env)
 
 
 def _write_output(path, data, s, step, time, ds, guard, flat):
@@ -137,8 +145,10 @@ def run(args) -> int:
     os.makedirs(args.output, exist_ok=True)
     env = SimEnvironment(p, device=args.device)
     data = SimData(env, dtype)
-    data.upload(getattr(problems, d.init)(p, dtype))
+    init = getattr(problems, d.init)
+    data.upload(init(p, dtype, yee=True) if d.kind == YEE else init(p, dtype))
     flat = d.kind == FLAT
+    energies = d.kind in (FLAT, YEE)
     s = _solver(d.kind, data, env, sem_gpu=False)
     if flat:
         s.set_aux(True)  # J, div E, div B for the outputs
@@ -164,7 +174,7 @@ def run(args) -> int:
         if out:
             _write_output(os.path.join(args.output, f"fld.{step:05d}.fld"), data, s, step,
                           float(time), ds, guard, flat)
-            if flat:
+            if energies:
                 wb, we = s.total_energy("B"), s.total_energy("E")
                 with open(os.path.join(args.output, "energy.txt"), "a") as fh:
                     fh.write(f"{step} {float(time):.9g} {wb:.17g} {we:.17g}\n")

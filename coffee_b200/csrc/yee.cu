@@ -193,8 +193,6 @@ int yee_check(const coffee_env* env) {
   const coffee_params& p = env->p;
   if (p.shift_ghost != 0)
     return fail(COFFEE_E_CONFIG, "the staggered solver updates the interior only (shift_ghost 0)");
-  if (p.problem != 0 && p.problem != 1)
-    return fail(COFFEE_E_CONFIG, "problem %d is not supported by the staggered solver", p.problem);
   const coffee_grid& g = env->grid;
   for (int a = 0; a < 3; ++a) {
     if (g.guard[a] < 1) return fail(COFFEE_E_CONFIG, "the staggered solver needs guard[%d] >= 1", a);

@@ -33,6 +33,21 @@
 #include "ez_common.cuh"
 #include "ez_physics.cuh"
 
+// Resident CTAs of 256 threads per SM that the register allocation of the
+// streaming passes must allow (FP32; FP64 builds ask for 1).  The passes are
+// latency bound: 3 CTAs (80 registers) beat 2 (116) by 20% and 4 (64, with
+// spills); the first substep's update, which also writes the start-of-step
+// copies, keeps 2.
+#ifndef COFFEE_YEE_UPDATE_MIN_BLOCKS
+#define COFFEE_YEE_UPDATE_MIN_BLOCKS 3
+#endif
+#ifndef COFFEE_YEE_FIRST_MIN_BLOCKS
+#define COFFEE_YEE_FIRST_MIN_BLOCKS 2
+#endif
+#ifndef COFFEE_YEE_CLAMP_MIN_BLOCKS
+#define COFFEE_YEE_CLAMP_MIN_BLOCKS 3
+#endif
+
 namespace coffee {
 
 constexpr int kStE[3] = {0b110, 0b101, 0b011};
@@ -222,7 +237,9 @@ __device__ __forceinline__ T current(const YeeArgs<T>& a, const Win<kRhoWin, T>&
 // ---------------------------------------------------------------- update
 
 template <typename T, bool FIRST, bool HAS_B0>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? (FIRST ? COFFEE_YEE_FIRST_MIN_BLOCKS
+                                                         : COFFEE_YEE_UPDATE_MIN_BLOCKS)
+                                      : 1)
 yee_update_kernel(const YeeArgs<T> a, const T c1, const T c2, const T c3) {
   const int i = a.g.lo[0] + (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int j = a.g.lo[1] + (int)(blockIdx.y * blockDim.y + threadIdx.y);
@@ -426,7 +443,7 @@ __device__ __forceinline__ T clamp_component(const Win<kClEx, T>& ex, const Win<
 }
 
 template <typename T, bool LAST, bool IMAGES>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? COFFEE_YEE_CLAMP_MIN_BLOCKS : 1)
 yee_clamp_kernel(const YeeArgs<T> a) {
   const int i = a.g.lo[0] + (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int j = a.g.lo[1] + (int)(blockIdx.y * blockDim.y + threadIdx.y);

@@ -81,11 +81,15 @@ def _per_component(fn, p: SimParams, dtype, yee: bool):
 def alfven_plane_wave_fields(p: SimParams, dtype=np.float32, xi0=0.1, yee: bool = False):
     """Plane Alfven wave on B0 = x-hat in a periodic box, the initial
     condition of the reference's wave driver (``src/main-wave.cpp`` with
-    ``src/user_alfven.hpp``, its EZ branch): wave vector
-    k = (2 * 2 pi / Lx, 0, 2 pi / Lz), frequency w = k.B0 / |B0| (c = 1),
-    E along e = (k x B0) x B0 normalised, b = k x e, and
-    E = -xi0 sin(k.x) e, B = B0 - xi0 sin(k.x) b / w, P = 0.  With `yee`
-    each component is evaluated at its staggered position."""
+    ``src/user_alfven.hpp``): wave vector k = (2 * 2 pi / Lx, 0, 2 pi / Lz),
+    frequency w = k.B0 / |B0| (c = 1), E along e = (k x B0) x B0 normalised,
+    b = k x e, E = -xi0 sin(k.x) e, P = 0.  The EZ branch (collocated,
+    every component at the vertices) sets B = B0 - xi0 sin(k.x) b / w.  With
+    `yee`, the staggered branch: each E component at its own position and
+    B = B0 + the staggered curl of A = xi0 cos(k.x) e / w taken at the E
+    positions, so that B is divergence free on the grid
+    (``src/user_alfven.hpp:79-113``; the last point of each axis, which the
+    reference leaves unset, holds B0)."""
     b0 = np.array([1.0, 0.0, 0.0])
     k = np.array([2.0 * 2.0 * math.pi / p.size[0], 0.0, 1.0 * 2.0 * math.pi / p.size[2]])
     w = float(k @ b0) / float(np.linalg.norm(b0))
@@ -98,7 +102,27 @@ def alfven_plane_wave_fields(p: SimParams, dtype=np.float32, xi0=0.1, yee: bool 
             return np.zeros_like(X)
         s = np.sin(k[0] * X + k[1] * Y + k[2] * Z)
         return -xi0 * s * e[c] if c < 3 else b0[c - 3] - xi0 * s * b[c - 3] / w
-    return _per_component(fn, p, dtype, yee)
+    if not yee:
+        return _per_component(fn, p, dtype, False)
+    ft = np.dtype(dtype)
+    out = [np.asarray(fn(*_xyz(p, dtype, YEE_STAGGER[c]), c), dtype=ft) for c in range(3)]
+    A = []
+    for c in range(3):
+        Z, Y, X = _xyz(p, dtype, YEE_STAGGER[c])
+        A.append(xi0 * np.cos(k[0] * X + k[1] * Y + k[2] * Z) * e[c] / w)
+    g = Grid.from_params(p, dtype)
+    inv = g.inv_delta
+    B = [np.full(A[0].shape, b0[c]) for c in range(3)]
+    core = (slice(0, -1),) * 3
+    sh = {0: (slice(0, -1), slice(0, -1), slice(1, None)),   # +x
+          1: (slice(0, -1), slice(1, None), slice(0, -1)),   # +y
+          2: (slice(1, None), slice(0, -1), slice(0, -1))}   # +z
+    B[0][core] = b0[0] + (A[2][sh[1]] - A[2][core]) * inv[1] - (A[1][sh[2]] - A[1][core]) * inv[2]
+    B[1][core] = b0[1] + (A[0][sh[2]] - A[0][core]) * inv[2] - (A[2][sh[0]] - A[2][core]) * inv[0]
+    B[2][core] = b0[2] + (A[1][sh[0]] - A[1][core]) * inv[0] - (A[0][sh[1]] - A[0][core]) * inv[1]
+    out += [np.asarray(a, dtype=ft) for a in B]
+    out.append(np.zeros(A[0].shape, dtype=ft))
+    return out
 
 
 def emwave_fields(p: SimParams, dtype=np.float32, yee: bool = False):

@@ -324,7 +324,8 @@ class FieldSolver(FieldSolverEZ):
     (src/algorithms/field_solver.cu:690-726).  E and B sit on the staggered
     positions of src/data/sim_data.cpp:19-25; sim_data's B0
     (``SimData.upload_background``) is subtracted in curl B.  The reference
-    has it only in its GPU build.  Problems 0 (box) and 1 (rotating star)."""
+    has it only in its GPU build.  Problem 1 adds the rotating star; the
+    reference's solver treats every other problem id as the plain box."""
 
     VARIANT = _lib.VARIANT_YEE
 

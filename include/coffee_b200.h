@@ -70,7 +70,8 @@ enum { /* solver variants */
   COFFEE_VARIANT_GR = 3,     /* Kerr-Schild GR EZ, field_solver_gr_EZ (GPU build); E holds D */
   COFFEE_VARIANT_YEE = 4     /* staggered (Yee) RK3, field_solver (GPU build only): E and B on
                               * the staggered positions of sim_data.cpp:19-25, B0 subtracted
-                              * in curl B; problems 0 and 1, shift_ghost 0 */
+                              * in curl B; the rotating star with problem 1 (any
+                              * other problem: none), shift_ghost 0 */
 };
 enum { /* which reference build the flat solver reproduces */
   COFFEE_SEM_CPU_REF = 0, /* field_solver_EZ.cpp (the parity oracle build) */

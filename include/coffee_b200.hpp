@@ -307,6 +307,7 @@ class sim_data {
   void sync_to_device() {
     E.sync_to_device();
     B.sync_to_device();
+    B0.sync_to_device();
     P.sync_to_device();
   }
   coffee_fields* handle() const { return m_fields; }
@@ -413,6 +414,34 @@ class field_solver_gr_EZ : public gpu_variant_solver {
  public:
   field_solver_gr_EZ(sim_data& mydata, sim_environment& env, void* stream = nullptr)
       : gpu_variant_solver(mydata, env, COFFEE_VARIANT_GR, "field_solver_gr_EZ", stream) {}
+};
+
+// field_solver (src/algorithms/field_solver.h:8-35): the staggered (Yee)
+// RK3 solver.  E and B sit on the staggered positions of
+// src/data/sim_data.cpp:19-25, and sim_data's B0 is the background field
+// subtracted in curl B (the EZ solvers keep J there instead), so this
+// constructor binds data.B0 to the library's B0 arrays.
+class field_solver : public gpu_variant_solver {
+ public:
+  field_solver(sim_data& mydata, sim_environment& env, void* stream = nullptr)
+      : gpu_variant_solver((rebind_background(mydata), mydata), env, COFFEE_VARIANT_YEE,
+                           "field_solver", stream),
+        m_data(mydata) {}
+  // total_energy (field_solver.cu:829-866): each component interpolated to
+  // the vertex, summed in FP64 over the region outside the star and the
+  // absorbing layer.
+  Scalar total_energy(vector_field<Scalar>& f) {
+    const int what = (&f == &m_data.E) ? COFFEE_DIAG_ENERGY_E : COFFEE_DIAG_ENERGY_B;
+    double out = 0;
+    coffee_check(coffee_diag_reduce(handle(), what, &out), "total_energy");
+    return (Scalar)out;
+  }
+
+ private:
+  static void rebind_background(sim_data& d) {
+    for (int i = 0; i < 3; ++i) d.B0.data(i).bind(d.handle(), COFFEE_B0X + i);
+  }
+  sim_data& m_data;
 };
 
 }  // namespace Coffee

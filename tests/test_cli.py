@@ -20,6 +20,12 @@ def _config(tmp_path, p: SimParams, name="config.toml"):
     return str(path)
 
 
+def _with(p, **kw):
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
 def _wave_params(N=16, steps=6):
     p = problems.alfven_params(N)
     p.max_steps = steps
@@ -58,6 +64,26 @@ def test_wave_initial_condition_is_a_force_free_alfven_wave():
     # E = -v x B with v along B0 at the wave speed is not required, but the
     # wave vector is (2 * 2 pi, 0, 2 pi): E varies along x and z only
     assert np.allclose(E[2][:, 0, :], E[2][:, 5, :])
+
+
+def test_staggered_wave_initial_condition_is_divergence_free():
+    """The staggered branch of user_alfven.hpp: B = B0 + the staggered curl of
+    a vector potential, so the cell-centred div B vanishes to rounding, and B
+    matches the collocated wave B0 - xi0 sin(k.x) b / w to O(dx^2)."""
+    p = problems.alfven_params(N=24, guard=2)
+    f = problems.alfven_plane_wave_fields(p, np.float64, yee=True)
+    bx, by, bz = f[3:6]
+    inv = 24.0
+    div = ((bx[:-1, :-1, 1:] - bx[:-1, :-1, :-1]) + (by[:-1, 1:, :-1] - by[:-1, :-1, :-1]) +
+           (bz[1:, :-1, :-1] - bz[:-1, :-1, :-1])) * inv
+    assert np.abs(div[:-1, :-1, :-1]).max() < 1e-12
+    # B_y at its own position (i + 1/2, j, k + 1/2) against the continuum wave
+    k = np.array([4 * math.pi, 0.0, 2 * math.pi])
+    Z, Y, X = problems._xyz(p, np.float64, problems.YEE_STAGGER[4])
+    w = k[0]
+    ref = -0.1 * np.sin(k[0] * X + k[2] * Z) * k[0] / w
+    err = np.abs(by - ref)[:-1, :-1, :-1].max()
+    assert err < 0.1 * (2 * math.pi / 24) ** 2
 
 
 def test_emwave_initial_condition_is_transverse():
@@ -122,6 +148,9 @@ def test_restart_from_snapshot_continues_the_run(tmp_path):
     ("gr", lambda: problems.wald_params(16)),
     ("pulsar2d-spherical", lambda: problems.sph_pulsar_params(nr=32, nth=16, guard=4)),
     ("pulsar2d-cylindrical", lambda: problems.cyl_pulsar_params(nR=16, nz=32)),
+    ("wave-yee", lambda: _wave_params(16)),
+    ("pulsar3d-yee", lambda: problems.pulsar_params(24)),
+    ("alfven3d-yee", lambda: _with(problems.pulsar_params(24), problem=2)),
 ])
 def test_every_driver_runs(tmp_path, driver, make):
     p = make()

@@ -1,5 +1,6 @@
-"""The numpy restatements of the reference's log-spherical, cylindrical and
-GR solvers (oracle/axisym_oracle.py, oracle/gr_oracle.py) against fixtures
+"""The numpy restatements of the reference's log-spherical, cylindrical, GR
+and staggered solvers (oracle/axisym_oracle.py, oracle/gr_oracle.py,
+oracle/yee_oracle.py) against fixtures
 made by the reference's own GPU build in double precision
 (tests/golden/variants/*.npz, written by tests/golden/make_variant_golden.py
 on a GPU).  CPU only."""
@@ -13,7 +14,7 @@ import numpy as np
 import pytest
 
 from helpers import GOLDEN, rel_l2
-from oracle import axisym_oracle, gr_oracle
+from oracle import axisym_oracle, gr_oracle, yee_oracle
 
 VARIANTS = os.path.join(GOLDEN, "variants")
 
@@ -46,6 +47,9 @@ def test_restatement_matches_reference_gpu_double(name):
         out = axisym_oracle.sph_evolve(p, np.stack([a[0] for a in f64]), steps)[:, None]
     elif solver == "cyl":
         out = axisym_oracle.cyl_evolve(p, np.stack([a[0] for a in f64]), steps)[:, None]
+    elif solver == "yee":
+        b0 = np.stack(f64[7:10]) if len(f64) > 7 else None
+        out = yee_oracle.yee_evolve(p, np.stack(f64[:7]), steps, B0=b0)
     else:
         out = gr_oracle.gr_evolve(p, np.stack(f64), steps)
     worst = max(rel_l2(out[f], ref[f]) for f in range(7))
