@@ -464,8 +464,10 @@ def run_ours(args):
 # the EZ solvers; for the staggered solver the update pass of substeps 2-3,
 # which reads E, B and their start-of-step copies and writes E*, B'
 # (12 + 6 arrays of 4 bytes).
+# The Kerr-Schild staggered solver's update pass reads E, H, B, the lowered
+# B, rho, D and the start-of-step copies and writes D*, B' (22 + 6 arrays).
 VARIANT_STAGE_BYTES = {"gr-wald": 136, "logsph-batch": 112, "logsph": 112, "cyl-pulsar": 112,
-                       "yee-wave": 72, "yee-pulsar": 72}
+                       "yee-wave": 72, "yee-pulsar": 72, "gryee-wald": 112}
 
 
 def _variant_cases(workload, n=512):
@@ -496,6 +498,12 @@ def _variant_cases(workload, n=512):
             "workload": f"yee-pulsar{n}", "grid": [n] * 3, "guard": 2,
             "solver": "staggered SSP-RK3 (field_solver)", "domain": [-64, 64], "radius": 4.0,
             "omega": 0.05, "pml": n // 16, "note": "rotating dipole star, absorbing layer"}
+    if workload == "gryee-wald":
+        p = problems.wald_params(N=256, half_size=20.0, a=0.9, pml=16)
+        return [("FieldSolverGr", "gryee", p, problems.wald_fields(p, np.float32, yee=True))], {
+            "workload": "gryee-wald256", "grid": [256] * 3, "spin": 0.9, "domain": [-20, 20],
+            "pml": 16, "solver": "staggered SSP-RK3 in Kerr-Schild coordinates (field_solver_gr)",
+            "note": "Wald field B = curl(x dy - y dx)/2 / sqrt(gamma), D = 0 (user_wald.hpp)"}
     if workload == "logsph":
         p = problems.sph_pulsar_params(nr=2048, nth=1024, guard=4, omega=0.2)
         return [("FieldSolverEZSpherical", "sph", p, problems.sph_pulsar_fields(p, np.float32))], {
@@ -601,7 +609,8 @@ def run_variant(args):
                  "cyl-pulsar": "cyl_stage_kernel (LSRK stages 2-5)",
                  "logsph": "sph_stage_kernel (LSRK stages 2-5)",
                  "yee-wave": "yee_update_kernel (substeps 2-3)",
-                 "yee-pulsar": "yee_update_kernel (substeps 2-3)"}[args.workload]
+                 "yee-pulsar": "yee_update_kernel (substeps 2-3)",
+                 "gryee-wald": "gyee_update_kernel (substeps 2-3)"}[args.workload]
         roof = {"kernel": kname, "bound": "hbm",
                 "achieved": VARIANT_STAGE_BYTES[args.workload] * cells / (avg / 1e3) / 1e9,
                 "peak": peak, "unit": "GB/s", "peak_kind": peak_kind, "traffic": None,
@@ -609,6 +618,10 @@ def run_variant(args):
                 "avg_launch_ms": avg}
         launches = sum(timing["launches"].values())
         launch_note = "stage + KO kernels counted by the solver's launch hooks"
+        if args.workload == "gryee-wald":
+            launches = objs[0][2].launches_per_step() * args.steps
+            launch_note = ("per substep: E/H, rho, shell, update and clamp passes, and the "
+                           "E_par cleaning in the last")
         if args.workload.startswith("yee"):
             per_call = 0 if runs[0][2].problem == 1 else 1
             launches = objs[0][2].launches_per_step() * args.steps + per_call
@@ -677,7 +690,7 @@ def main():
                          "benchmark)")
     ap.add_argument("--workload", default="turbulence",
                     choices=["turbulence", "gr-wald", "logsph-batch", "logsph", "cyl-pulsar",
-                             "yee-wave", "yee-pulsar"])
+                             "yee-wave", "yee-pulsar", "gryee-wald"])
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

@@ -26,6 +26,7 @@ VARIANT_LOGSPH = 1
 VARIANT_CYL = 2
 VARIANT_GR = 3
 VARIANT_YEE = 4
+VARIANT_GRYEE = 5
 KERNEL_STAGE_FIRST, KERNEL_STAGE, KERNEL_KO = 0, 1, 2
 SEM_CPU_REF = 0
 SEM_GPU_REF = 1

@@ -23,6 +23,7 @@ max_steps, a snapshot every ``snapshot_interval`` steps, an output every
 | wave-yee | main-wave.cpp without EZ | 0 | user_alfven.hpp (staggered branch) | field_solver |
 | pulsar3d-yee | main-pulsar3d.cpp without EZ | 1 | user_pulsar3d.hpp | field_solver |
 | alfven3d-yee | main-alfven3d.cpp without EZ | 2 | user_pulsar3d.hpp | field_solver |
+| gr-yee | main-gr-Yee.cpp | any | user_wald.hpp | field_solver_gr |
 
 Outputs go to DIR (default ``Data``): ``fld.NNNNN.fld`` holds E, B, P and
 J, div E, div B of the output step on every ``downsample``-th interior point
@@ -47,7 +48,7 @@ from . import problems
 from .config import SimParams
 from .fld import write_fld
 
-FLAT, GR, SPH, CYL, YEE = "flat", "gr", "sph", "cyl", "yee"
+FLAT, GR, SPH, CYL, YEE, GRYEE = "flat", "gr", "sph", "cyl", "yee", "gryee"
 
 
 @dataclass(frozen=True)
@@ -72,6 +73,7 @@ DRIVERS = {d.name: d for d in (
     Driver("wave-yee", "main-wave.cpp", 0, YEE, "alfven_plane_wave_fields"),
     Driver("pulsar3d-yee", "main-pulsar3d.cpp", 1, YEE, "pulsar_fields"),
     Driver("alfven3d-yee", "main-alfven3d.cpp", 2, YEE, "pulsar_fields"),
+    Driver("gr-yee", "main-gr-Yee.cpp", None, GRYEE, "wald_fields"),
 )}
 
 
@@ -123,7 +125,8 @@ def _solver(kind, data, env, sem_gpu):
     if kind == FLAT:
         return sv.FieldSolverEZ(data, env, "gpu" if sem_gpu else "cpu")
     return {GR: sv.FieldSolverGrEZ, SPH: sv.FieldSolverEZSpherical,
-            CYL: sv.FieldSolverEZCylindrical, YEE: sv.FieldSolver}[kind](data, env)
+            CYL: sv.FieldSolverEZCylindrical, YEE: sv.FieldSolver,
+            GRYEE: sv.FieldSolverGr}[kind](data, env)
 
 
 def _write_output(path, data, s, step, time, ds, guard, flat):
@@ -146,7 +149,7 @@ def run(args) -> int:
     env = SimEnvironment(p, device=args.device)
     data = SimData(env, dtype)
     init = getattr(problems, d.init)
-    data.upload(init(p, dtype, yee=True) if d.kind == YEE else init(p, dtype))
+    data.upload(init(p, dtype, yee=True) if d.kind in (YEE, GRYEE) else init(p, dtype))
     flat = d.kind == FLAT
     energies = d.kind in (FLAT, YEE)
     s = _solver(d.kind, data, env, sem_gpu=False)

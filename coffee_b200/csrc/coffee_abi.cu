@@ -567,7 +567,7 @@ extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int varia
   if (f->env != env) return fail(COFFEE_E_INVALID, "fields belong to another environment");
   if (variant != COFFEE_VARIANT_FLAT && variant != COFFEE_VARIANT_LOGSPH &&
       variant != COFFEE_VARIANT_CYL && variant != COFFEE_VARIANT_GR &&
-      variant != COFFEE_VARIANT_YEE)
+      variant != COFFEE_VARIANT_YEE && variant != COFFEE_VARIANT_GRYEE)
     return fail(COFFEE_E_INVALID, "solver variant %d is not available", variant);
   if (semantics != COFFEE_SEM_CPU_REF && semantics != COFFEE_SEM_GPU_REF)
     return fail(COFFEE_E_INVALID, "unknown semantics %d", semantics);
@@ -581,9 +581,10 @@ extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int varia
                     a);
   } else {
     // the reference has these solvers only in its GPU build
-    int rc = variant == COFFEE_VARIANT_GR    ? gr_check(env)
-             : variant == COFFEE_VARIANT_YEE ? yee_check(env)
-                                             : axisym_check(env, variant);
+    int rc = variant == COFFEE_VARIANT_GR      ? gr_check(env)
+             : variant == COFFEE_VARIANT_YEE   ? yee_check(env)
+             : variant == COFFEE_VARIANT_GRYEE ? gryee_check(env)
+                                               : axisym_check(env, variant);
     if (rc) return rc;
   }
   COFFEE_CUDA_TRY(cudaSetDevice(env->device));
@@ -601,7 +602,7 @@ extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int varia
   // the GR solver's inner absorbing region always needs the start-of-step
   // copy; the staggered solver's substeps read it
   bool abs_any = env->p.shift_ghost > 0 || variant == COFFEE_VARIANT_GR ||
-                 variant == COFFEE_VARIANT_YEE;
+                 variant == COFFEE_VARIANT_YEE || variant == COFFEE_VARIANT_GRYEE;
   for (int a = 0; a < 3; ++a) abs_any = abs_any || env->p.pml[a] > 0;
   s->absorbing = abs_any;
   const size_t bytes = f->n * f->elem;
@@ -628,6 +629,7 @@ extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int varia
   }
   int rc = variant == COFFEE_VARIANT_GR     ? gr_setup(env, f->elem, &s->vtab)
            : variant == COFFEE_VARIANT_YEE  ? COFFEE_OK
+           : variant == COFFEE_VARIANT_GRYEE ? gryee_setup(env, f->elem, &s->vtab)
            : variant != COFFEE_VARIANT_FLAT ? axisym_setup(env, variant, f->elem, &s->vtab)
            : (f->elem == 4)               ? configure_solver<float>(s)
                                           : configure_solver<double>(s);
@@ -674,8 +676,8 @@ extern "C" int coffee_solver_destroy(coffee_solver* s) {
 extern "C" int coffee_solver_set_aux(coffee_solver* s, int enable) {
   clear_error();
   if (!s) return fail(COFFEE_E_INVALID, "coffee_solver_set_aux: null argument");
-  if (enable && s->variant == COFFEE_VARIANT_YEE)
-    return fail(COFFEE_E_INVALID, "the staggered solver writes no J, divE, divB");
+  if (enable && (s->variant == COFFEE_VARIANT_YEE || s->variant == COFFEE_VARIANT_GRYEE))
+    return fail(COFFEE_E_INVALID, "the staggered solvers write no J, divE, divB");
   if (enable)
     for (int id = COFFEE_JX; id <= COFFEE_DIVB; ++id) {
       int rc = ensure_field(s->f, id);
@@ -698,6 +700,9 @@ extern "C" int coffee_solver_launches_per_step(coffee_solver* s) {
     // shell + update + clamp per substep; the star boundary adds its three
     // passes and the guard pass (the box problem: one guard pass per call)
     return s->env->p.problem == 1 ? 21 : 9;
+  if (s && s->variant == COFFEE_VARIANT_GRYEE)
+    // E, H + rho + shell + update + clamp per substep, and the cleaning
+    return 15 + (s->env->p.clean_ep ? 1 : 0);
   return 6;  // 5 stage kernels + 1 KO kernel
 }
 
@@ -754,6 +759,13 @@ static int run_steps(coffee_solver* s, double time, int nsteps) {
   s->events_used = 0;
   EventHook hook(s);
   if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(s->ev_begin, st));
+  if (s->variant == COFFEE_VARIANT_GRYEE) {
+    int rc = gryee_steps(s->env, f->elem, f->d, s->dU, s->Un, s->vtab, nsteps, st,
+                         s->timing ? &hook : nullptr);
+    if (rc) return rc;
+    if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(s->ev_end, st));
+    return COFFEE_OK;
+  }
   if (s->variant == COFFEE_VARIANT_YEE) {
     void* b0[3] = {f->d[COFFEE_B0X], f->d[COFFEE_B0Y], f->d[COFFEE_B0Z]};
     const bool has_b0 = b0[0] && b0[1] && b0[2];
@@ -931,7 +943,7 @@ static int diag_t(coffee_solver* s, int what, double* out) {
     xh[a] = (T)p.lower[a] + (T)p.size[a] - (T)p.pml[a] * c.delta[a];
     xl[a] = (T)p.lower[a] + (T)p.pml[a] * c.delta[a];
   }
-  const int stag = s->variant == COFFEE_VARIANT_YEE ? 1 : 0;
+  const int stag = (s->variant == COFFEE_VARIANT_YEE || s->variant == COFFEE_VARIANT_GRYEE) ? 1 : 0;
   diag_kernel<T><<<s->partial_blocks, 256, 0, s->stream>>>(c, f7c<T>(s->f->d), what, xl[0],
                                                            xl[1], xl[2], xh[0], xh[1], xh[2],
                                                            stag, s->d_partials);

@@ -71,4 +71,11 @@ int yee_steps(const coffee_env* env, int elem, void* const A[7], void* const B0[
               void* const Es[7], void* const Un[7], void* const Tb[7], double time, int nsteps,
               cudaStream_t st, LaunchHook* hook);
 
+// Staggered RK3 solver in Kerr-Schild coordinates (COFFEE_VARIANT_GRYEE):
+// A holds D (in E) and B; scratch from gryee_setup.
+int gryee_check(const coffee_env* env);
+int gryee_setup(const coffee_env* env, int elem, void** scratch);
+int gryee_steps(const coffee_env* env, int elem, void* const A[7], void* const Es[7],
+                void* const Un[7], void* scratch, int nsteps, cudaStream_t st, LaunchHook* hook);
+
 }  // namespace coffee

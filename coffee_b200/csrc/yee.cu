@@ -1,6 +1,8 @@
-// Host side of the staggered (Yee) RK3 solver (COFFEE_VARIANT_YEE):
-// configuration checks, the launch geometry and the step loop of
-// field_solver::evolve_fields (src/algorithms/field_solver.cu:690-726).
+// Host side of the staggered (Yee) RK3 solvers: configuration checks, the
+// launch geometry and the step loops of field_solver::evolve_fields
+// (COFFEE_VARIANT_YEE, src/algorithms/field_solver.cu:690-726) and
+// field_solver_gr::evolve_fields_gr (COFFEE_VARIANT_GRYEE,
+// src/algorithms/field_solver_gr.cu:810-861).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -10,6 +12,7 @@
 #include "coffee_internal.h"
 #include "ez_launch.cuh"
 #include "variants.h"
+#include "gryee_kernels.cuh"
 #include "yee_kernels.cuh"
 
 namespace coffee {
@@ -137,7 +140,7 @@ int yee_steps_t(const coffee_env* env, void* const A[7], void* const B0[3], void
     for (int sub = 0; sub < 3; ++sub) {
       const bool last = sub == 2;
       const T c1 = (T)kC[sub][0], c2 = (T)kC[sub][1], c3 = (T)kC[sub][2];
-      yee_shell_kernel<T><<<gshell, kColBlock, 0, st>>>(a);
+      yee_shell_kernel<T><<<gshell, kColBlock, 0, st>>>(a, 1);
       COFFEE_CUDA_TRY(cudaGetLastError());
       const int kind = sub == 0 ? COFFEE_KERNEL_STAGE_FIRST : COFFEE_KERNEL_STAGE;
       int rc = hook ? hook->before(kind) : COFFEE_OK;
@@ -210,6 +213,119 @@ int yee_steps(const coffee_env* env, int elem, void* const A[7], void* const B0[
               cudaStream_t st, LaunchHook* hook) {
   return elem == 4 ? yee_steps_t<float>(env, A, B0, Es, Un, Tb, time, nsteps, st, hook)
                    : yee_steps_t<double>(env, A, B0, Es, Un, Tb, time, nsteps, st, hook);
+}
+
+// ------------------------------------------------------ Kerr-Schild
+
+namespace {
+
+const dim3 kPointBlock(32, 4, 2);  // one point per thread
+
+template <typename T>
+int gryee_steps_t(const coffee_env* env, void* const A[7], void* const Es[7], void* const Un[7],
+                  void* scratch, int nsteps, cudaStream_t st, LaunchHook* hook) {
+  const coffee_params& p = env->p;
+  GYeeArgs<T> g;
+  fill_args<T>(env, A, nullptr, Es, Un, Es, &g.y);
+  g.y.star = 0;
+  g.spin = (T)p.a;
+  g.calc_current = p.calc_current;
+  g.clean_ep = p.clean_ep;
+  g.check_egb = p.check_egb;
+  // rH = 1 + sqrt(1 - a^2) through double, then 0.8, 0.01, 0.2 rH (field_solver_gr.cu:666-669)
+  const T rH = (T)(1.0 + std::sqrt(1.0 - (double)(g.spin * g.spin)));
+  g.r1 = (T)(0.8 * (double)rH);
+  g.r2 = (T)(0.01 * (double)rH);
+  g.dd = (T)(0.2 * (double)rH);
+  for (int d = 0; d < 3; ++d) {
+    g.half[d] = (T)((double)g.y.c.delta[d] / 2.0);
+    g.upper[d] = (T)((T)p.lower[d] + (T)p.size[d]);
+  }
+  const size_t n = (size_t)g.y.g.dims[0] * g.y.g.dims[1] * g.y.g.dims[2];
+  T* s = static_cast<T*>(scratch);
+  for (int c = 0; c < 3; ++c) {
+    g.Ed[c] = s + (0 + c) * n;
+    g.Hd[c] = s + (3 + c) * n;
+    g.Bd[c] = s + (6 + c) * n;
+    g.Dc[c] = s + (10 + c) * n;
+  }
+  g.rho = s + 9 * n;
+  const YeeArgs<T>& a = g.y;
+  const int nx = a.g.hi[0] - a.g.lo[0], ny = a.g.hi[1] - a.g.lo[1], nz = a.g.hi[2] - a.g.lo[2];
+  const dim3 geh = grid3(kPointBlock, a.g.dims[0] - 2, a.g.dims[1] - 2, a.g.dims[2] - 2);
+  const dim3 gbox = grid3(kPointBlock, nx, ny, nz);
+  const dim3 gface = grid3(kColBlock, std::max(nx + 2, ny), std::max(ny + 2, nz), 1);
+  const dim3 gshell(gface.x, gface.y, 6);
+  for (int step = 0; step < nsteps; ++step) {
+    for (int sub = 0; sub < 3; ++sub) {
+      const bool last = sub == 2;
+      const bool clean = last && g.clean_ep;
+      const T c1 = (T)kC[sub][0], c2 = (T)kC[sub][1], c3 = (T)kC[sub][2];
+      gyee_eh_kernel<T><<<geh, kPointBlock, 0, st>>>(g);
+      gyee_rho_kernel<T><<<gbox, kPointBlock, 0, st>>>(g);
+      // the cleaning reads D* beyond the box where the state's D is; the
+      // rescale reads zeros there (its dD is zero outside the box)
+      yee_shell_kernel<T><<<gshell, kColBlock, 0, st>>>(a, clean ? 1 : 0);
+      COFFEE_CUDA_TRY(cudaGetLastError());
+      const int kind = sub == 0 ? COFFEE_KERNEL_STAGE_FIRST : COFFEE_KERNEL_STAGE;
+      int rc = hook ? hook->before(kind) : COFFEE_OK;
+      if (rc) return rc;
+      if (sub == 0) gyee_update_kernel<T, true><<<gbox, kPointBlock, 0, st>>>(g, c1, c2, c3);
+      else gyee_update_kernel<T, false><<<gbox, kPointBlock, 0, st>>>(g, c1, c2, c3);
+      COFFEE_CUDA_TRY(cudaGetLastError());
+      if (hook && (rc = hook->after(kind))) return rc;
+      if (clean) gyee_clean_kernel<T><<<gbox, kPointBlock, 0, st>>>(g);
+      if ((rc = hook ? hook->before(COFFEE_KERNEL_KO) : COFFEE_OK)) return rc;
+      if (last) gyee_clamp_kernel<T, true><<<gbox, kPointBlock, 0, st>>>(g);
+      else gyee_clamp_kernel<T, false><<<gbox, kPointBlock, 0, st>>>(g);
+      COFFEE_CUDA_TRY(cudaGetLastError());
+      if (hook && (rc = hook->after(COFFEE_KERNEL_KO))) return rc;
+    }
+  }
+  return COFFEE_OK;
+}
+
+}  // namespace
+
+int gryee_check(const coffee_env* env) {
+  const coffee_params& p = env->p;
+  if (p.shift_ghost != 0)
+    return fail(COFFEE_E_CONFIG, "the staggered solver updates the interior only (shift_ghost 0)");
+  for (int a = 0; a < 3; ++a) {
+    if (p.periodic_boundary[a])
+      return fail(COFFEE_E_CONFIG, "the Kerr-Schild solvers have no periodic axis (axis %d)", a);
+    if (env->grid.guard[a] < 1)
+      return fail(COFFEE_E_CONFIG, "the staggered solver needs guard[%d] >= 1", a);
+  }
+  if (!(std::fabs(p.a) < 1.0)) return fail(COFFEE_E_CONFIG, "the spin a must satisfy |a| < 1");
+  const coffee_grid& g = env->grid;
+  const double n = (double)g.dims[0] * g.dims[1] * g.dims[2];
+  if (n >= 2147483648.0)
+    return fail(COFFEE_E_CONFIG, "the staggered solver indexes a rank's arrays in 32 bits");
+  return COFFEE_OK;
+}
+
+// E, H, the lowered B, rho and the cleaned D: 13 arrays, zero outside what
+// the passes write (what the reference's arrays hold there)
+int gryee_setup(const coffee_env* env, int elem, void** scratch) {
+  const coffee_grid& g = env->grid;
+  const size_t bytes = (size_t)g.dims[0] * g.dims[1] * g.dims[2] * (size_t)elem * 13;
+  *scratch = nullptr;
+  cudaError_t err = cudaMalloc(scratch, bytes);
+  if (err == cudaSuccess) err = cudaMemset(*scratch, 0, bytes);
+  if (err != cudaSuccess) {
+    if (*scratch) cudaFree(*scratch);
+    *scratch = nullptr;
+    return fail(COFFEE_E_NOMEM, "staggered Kerr-Schild scratch allocation failed: %s",
+                cudaGetErrorString(err));
+  }
+  return COFFEE_OK;
+}
+
+int gryee_steps(const coffee_env* env, int elem, void* const A[7], void* const Es[7],
+                void* const Un[7], void* scratch, int nsteps, cudaStream_t st, LaunchHook* hook) {
+  return elem == 4 ? gryee_steps_t<float>(env, A, Es, Un, scratch, nsteps, st, hook)
+                   : gryee_steps_t<double>(env, A, Es, Un, scratch, nsteps, st, hook);
 }
 
 }  // namespace coffee

@@ -356,11 +356,13 @@ yee_update_kernel(const YeeArgs<T> a, const T c1, const T c2, const T c3) {
 
 // The clamp pass reads E* and B' one point beyond the box, where the
 // reference reads the state's guard values of before the exchange; this pass
-// copies them into the scratch arrays.  blockIdx.z picks one of the six faces
-// of the box grown by one point (the z faces whole, the y faces between
-// them, the x faces between those); (x, y) threads cover the face.
+// copies them into the scratch arrays (with e_state 0 the E* shell is 0
+// instead: what the Kerr-Schild solver's rescale reads there, its dD being
+// zero outside the box).  blockIdx.z picks one of the six faces of the box
+// grown by one point (the z faces whole, the y faces between them, the x
+// faces between those); (x, y) threads cover the face.
 template <typename T>
-__global__ void yee_shell_kernel(const YeeArgs<T> a) {
+__global__ void yee_shell_kernel(const YeeArgs<T> a, const int e_state) {
   const int u = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   const int v = (int)(blockIdx.y * blockDim.y + threadIdx.y);
   const int face = (int)blockIdx.z;
@@ -381,7 +383,7 @@ __global__ void yee_shell_kernel(const YeeArgs<T> a) {
   const uint32_t o = (uint32_t)k * (uint32_t)a.g.sz + (uint32_t)j * (uint32_t)a.g.sy + (uint32_t)i;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    a.Es[c][o] = a.E[c][o];
+    a.Es[c][o] = e_state ? a.E[c][o] : (T)0;
     a.Bs[c][o] = a.B[c][o];
   }
 }

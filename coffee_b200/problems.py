@@ -429,14 +429,46 @@ def cks_sqrt_gamma(a, x, y, z, tiny):
     return np.sqrt(1.0 + 2.0 * r ** 3 / np.maximum(r ** 4 + a * a * z * z, tiny))
 
 
-def wald_fields(p: SimParams, dtype=np.float32):
+def wald_fields(p: SimParams, dtype=np.float32, yee: bool = False):
     """Uniform asymptotic field along the spin axis: B^z = 1 / sqrt(gamma),
-    D = 0, P = 0 (``src/user_wald2.hpp``)."""
+    D = 0, P = 0 (``src/user_wald2.hpp``).  With `yee`, the staggered
+    solver's initial condition (``src/user_wald.hpp``): B = curl A / sqrt(gamma)
+    with A = (-y/2, x/2, 0) (its vector potential at a = 0) taken at the E
+    positions and the staggered curl, each component divided by sqrt(gamma)
+    at its own position; D = 0."""
     g = Grid.from_params(p, dtype)
     tiny = 1e-7 if np.dtype(dtype) == np.float32 else 1e-11
-    x, y, z = (g.coords(a, np.float64) for a in range(3))
-    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
-    bz = 1.0 / cks_sqrt_gamma(p.a, X, Y, Z, tiny)
-    zeros = np.zeros_like(X)
-    arrs = [zeros, zeros, zeros, zeros, zeros, bz, zeros]
-    return [np.asarray(a, dtype=dtype).copy() for a in arrs]
+    if not yee:
+        x, y, z = (g.coords(a, np.float64) for a in range(3))
+        Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+        bz = 1.0 / cks_sqrt_gamma(p.a, X, Y, Z, tiny)
+        zeros = np.zeros_like(X)
+        arrs = [zeros, zeros, zeros, zeros, zeros, bz, zeros]
+        return [np.asarray(a, dtype=dtype).copy() for a in arrs]
+    A = []
+    for c, f in enumerate((lambda X, Y: -0.5 * Y, lambda X, Y: 0.5 * X, lambda X, Y: 0.0 * X)):
+        Z, Y, X = _xyz(p, dtype, YEE_STAGGER[c])
+        A.append(f(X, Y))
+    inv = g.inv_delta
+    ext = lambda f, ax: np.concatenate([f, f[tuple(slice(-1, None) if i == 2 - ax else
+                                                    slice(None) for i in range(3))]],
+                                       axis=2 - ax)
+    d = lambda f, ax: np.diff(ext(f, ax), axis=2 - ax)
+    curl = [d(A[2], 1) * inv[1] - d(A[1], 2) * inv[2],
+            d(A[0], 2) * inv[2] - d(A[2], 0) * inv[0],
+            d(A[1], 0) * inv[0] - d(A[0], 1) * inv[1]]
+    B = []
+    for c in range(3):
+        Z, Y, X = _xyz(p, dtype, YEE_STAGGER[3 + c])
+        B.append(curl[c] / cks_sqrt_gamma(p.a, X, Y, Z, tiny))
+    # the last point of each axis has no forward difference: continue the
+    # field from the point before it
+    for c in range(3):
+        for ax in range(3):
+            sl = [slice(None)] * 3
+            sl[2 - ax] = slice(-1, None)
+            src = [slice(None)] * 3
+            src[2 - ax] = slice(-2, -1)
+            B[c][tuple(sl)] = B[c][tuple(src)]
+    zeros = np.zeros_like(B[0])
+    return [np.asarray(a, dtype=dtype).copy() for a in (zeros, zeros, zeros, *B, zeros)]

@@ -333,6 +333,19 @@ class FieldSolver(FieldSolverEZ):
         super().__init__(data, env, semantics="gpu", stream=stream)
 
 
+class FieldSolverGr(FieldSolverEZ):
+    """``field_solver_gr(sim_data&, sim_environment&)`` (src/algorithms/field_solver_gr.h:6-29):
+    the staggered solver in Cartesian Kerr-Schild coordinates around a hole
+    of spin ``params.a`` (evolve_fields_gr, src/algorithms/field_solver_gr.cu:810-861).
+    sim_data's E holds D on the E positions; B on the B positions.  The
+    reference has it only in its GPU build.  ``step``'s time is not used."""
+
+    VARIANT = _lib.VARIANT_GRYEE
+
+    def __init__(self, data: SimData, env: SimEnvironment, stream: int | None = None):
+        super().__init__(data, env, semantics="gpu", stream=stream)
+
+
 class SphBatch:
     """Independent log-spherical runs advanced together, one kernel launch
     per phase for all of them (``coffee_batch_*``; no counterpart in the

@@ -15,7 +15,9 @@
  *   field_solver_EZ  (src/algorithms/field_solver_EZ.h:6-33) -> coffee_solver
  * The reference's staggered RK3 solver, Coffee::field_solver::evolve_fields
  * (src/algorithms/field_solver.h:8-35, src/algorithms/field_solver.cu:690-726),
- * is the variant COFFEE_VARIANT_YEE of the same handle.
+ * is the variant COFFEE_VARIANT_YEE of the same handle, and its Kerr-Schild
+ * counterpart Coffee::field_solver_gr::evolve_fields_gr
+ * (src/algorithms/field_solver_gr.cu:810-861) the variant COFFEE_VARIANT_GRYEE.
  * include/coffee_b200.hpp re-creates the reference's C++ classes on top of
  * these calls.
  *
@@ -68,10 +70,14 @@ enum { /* solver variants */
   COFFEE_VARIANT_LOGSPH = 1, /* 2D log-spherical EZ, field_solver_EZ_spherical (GPU build) */
   COFFEE_VARIANT_CYL = 2,    /* 2D cylindrical EZ, field_solver_EZ_cylindrical (GPU build) */
   COFFEE_VARIANT_GR = 3,     /* Kerr-Schild GR EZ, field_solver_gr_EZ (GPU build); E holds D */
-  COFFEE_VARIANT_YEE = 4     /* staggered (Yee) RK3, field_solver (GPU build only): E and B on
+  COFFEE_VARIANT_YEE = 4,    /* staggered (Yee) RK3, field_solver (GPU build only): E and B on
                               * the staggered positions of sim_data.cpp:19-25, B0 subtracted
                               * in curl B; the rotating star with problem 1 (any
                               * other problem: none), shift_ghost 0 */
+  COFFEE_VARIANT_GRYEE = 5   /* staggered RK3 in Kerr-Schild coordinates, field_solver_gr
+                              * (GPU build only; evolve_fields_gr): E holds D, staggered as
+                              * above; no periodic axis, shift_ghost 0; the time argument of
+                              * coffee_solver_step is not used */
 };
 enum { /* which reference build the flat solver reproduces */
   COFFEE_SEM_CPU_REF = 0, /* field_solver_EZ.cpp (the parity oracle build) */

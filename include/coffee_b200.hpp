@@ -444,6 +444,15 @@ class field_solver : public gpu_variant_solver {
   sim_data& m_data;
 };
 
+// field_solver_gr (src/algorithms/field_solver_gr.h:6-29): the staggered
+// solver in Kerr-Schild coordinates; sim_data's E holds D.
+class field_solver_gr : public gpu_variant_solver {
+ public:
+  field_solver_gr(sim_data& mydata, sim_environment& env, void* stream = nullptr)
+      : gpu_variant_solver(mydata, env, COFFEE_VARIANT_GRYEE, "field_solver_gr", stream) {}
+  void evolve_fields_gr() { evolve_fields((Scalar)0); }
+};
+
 }  // namespace Coffee
 
 #endif  // COFFEE_B200_HPP

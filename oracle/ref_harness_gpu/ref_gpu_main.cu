@@ -10,6 +10,9 @@
 //                staggered RK3 solver; keeps sim_data's Yee staggering
 //                (src/data/sim_data.cpp:19-25) and, when IN.fld holds 10
 //                arrays, loads arrays 7-9 as the background field B0
+//           gryee field_solver_gr           (src/algorithms/field_solver_gr.cu), the
+//                staggered solver in Kerr-Schild coordinates
+//                (evolve_fields_gr(); Yee staggering; E holds D)
 //
 // The config is read by the reference's parse_config through the single-rank
 // environment double (ref_gpu_env.cu), which also fills the reference's
@@ -49,6 +52,7 @@
 #include "algorithms/field_solver_EZ_spherical.h"
 #include "algorithms/field_solver_gr_EZ.h"
 #include "algorithms/field_solver.h"
+#include "algorithms/field_solver_gr.h"
 #include "coffee_fld.h"
 #include "data/sim_data.h"
 #include "sim_env.h"
@@ -57,7 +61,7 @@ using namespace Coffee;
 
 int main(int argc, char** argv) {
   if (argc < 5) {
-    std::fprintf(stderr, "usage: %s ez|sph|cyl|gr|yee IN.fld OUT.fld NSTEPS [--aux] [--warmup W]\n",
+    std::fprintf(stderr, "usage: %s ez|sph|cyl|gr|yee|gryee IN.fld OUT.fld NSTEPS [--aux] [--warmup W]\n",
                  argv[0]);
     return 2;
   }
@@ -75,7 +79,7 @@ int main(int argc, char** argv) {
     }
   }
   if (solver_name != "ez" && solver_name != "sph" && solver_name != "cyl" && solver_name != "gr" &&
-      solver_name != "yee") {
+      solver_name != "yee" && solver_name != "gryee") {
     std::fprintf(stderr, "unknown solver %s\n", solver_name.c_str());
     return 2;
   }
@@ -106,7 +110,8 @@ int main(int argc, char** argv) {
   }
 
   sim_data data(env);
-  if (solver_name != "yee") {
+  const bool staggered = solver_name == "yee" || solver_name == "gryee";
+  if (!staggered) {
     Stagger st[3] = {Stagger(0b111), Stagger(0b111), Stagger(0b111)};
     data.E.set_stagger(st);
     data.B.set_stagger(st);
@@ -124,6 +129,7 @@ int main(int argc, char** argv) {
   std::unique_ptr<field_solver_EZ_cylindrical> s_cyl;
   std::unique_ptr<field_solver_gr_EZ> s_gr;
   std::unique_ptr<field_solver> s_yee;
+  std::unique_ptr<field_solver_gr> s_gryee;
   std::function<void(Scalar)> evolve;
   if (solver_name == "ez") {
     s_ez.reset(new field_solver_EZ(data, env));
@@ -137,9 +143,12 @@ int main(int argc, char** argv) {
   } else if (solver_name == "gr") {
     s_gr.reset(new field_solver_gr_EZ(data, env));
     evolve = [&](Scalar t) { s_gr->evolve_fields(t); };
-  } else {
+  } else if (solver_name == "yee") {
     s_yee.reset(new field_solver(data, env));
     evolve = [&](Scalar t) { s_yee->evolve_fields(t); };
+  } else {
+    s_gryee.reset(new field_solver_gr(data, env));
+    evolve = [&](Scalar) { s_gryee->evolve_fields_gr(); };
   }
 
   Scalar* dst[7] = {data.E.host_ptr(0), data.E.host_ptr(1), data.E.host_ptr(2),
@@ -157,6 +166,10 @@ int main(int argc, char** argv) {
       else
         std::memset(b0[f], 0, n * sizeof(Scalar));
     }
+    // divE holds the staggered GR solver's rho, which it writes only inside
+    // the update box and reads one point beyond it: start it at zero
+    std::memset(data.divE.host_ptr(), 0, n * sizeof(Scalar));
+    std::memset(data.divB.host_ptr(), 0, n * sizeof(Scalar));
   }
   payload.clear();
   payload.shrink_to_fit();

@@ -11,6 +11,8 @@ coffee_b200.  Nothing in the library imports this module.
   _pulsar_b/_e kernel_boundary_pulsar_{B,E}_thread (:344-638)
   _absorbing   kernel_boundary_absorbing_thread (src/algorithms/boundary.cu:18-78)
   interp       interpolate (src/algorithms/interpolation.h:9-33)
+  gryee_evolve field_solver_gr::evolve_fields_gr, the staggered solver in
+               Cartesian Kerr-Schild coordinates (src/algorithms/field_solver_gr.cu:810-861)
 
 Layout (src/data/sim_data.cpp:19-25): Stagger bit a set means "on the grid
 vertex along axis a", clear means "half a cell above it" (Grid::pos,
@@ -40,8 +42,10 @@ import numpy as np
 
 try:
     from .axisym_oracle import as_dict, tiny
+    from .gr_oracle import Cks
 except ImportError:  # imported as a top-level module
     from axisym_oracle import as_dict, tiny
+    from gr_oracle import Cks
 
 ST_E = (0b110, 0b101, 0b011)
 ST_B = (0b001, 0b010, 0b100)
@@ -68,6 +72,13 @@ class Geo:
         self.lo = [self.g[a] - s for a in range(3)]
         self.hi = [self.d[a] - self.g[a] + s for a in range(3)]
         self.periodic = [bool(x) for x in p["periodic_boundary"]]
+
+    def boxed(self, lo, hi):
+        """The same grid with another box (e.g. the E, H box [1, dims - 1))."""
+        g = Geo.__new__(Geo)
+        g.__dict__.update(self.__dict__)
+        g.lo, g.hi = list(lo), list(hi)
+        return g
 
     def S(self, f, dz=0, dy=0, dx=0):
         """f over the box shifted by (dz, dy, dx)."""
@@ -373,4 +384,218 @@ def yee_evolve(p, U: np.ndarray, nsteps: int, time0: float = 0.0, B0=None):
                 _absorbing(G, p, U[0:6], np.concatenate([En, Bn]))
             _exchange(G, list(E) + list(B))
         t = ft(t + dt)
+    return U
+
+
+# ----------------------------------------------------------------- GR (Kerr-Schild)
+# sim_data's E holds the densitised D.  E = alpha D_i + sqrt(gamma) (beta x B)_i
+# and H = alpha B_i - sqrt(gamma) (beta x D)_i at the E and B positions, the
+# lowered B (kept in sim_data's B0 by the reference) at the B positions.
+
+def _cks_at(G: Geo, a, st, T):
+    return Cks(a, G.pos(0, st & 1), G.pos(1, (st >> 1) & 1), G.pos(2, (st >> 2) & 1), T)
+
+
+def _gr_eh(GE: Geo, a, T, D, B, Ed, Hd, Bd):
+    """kernel_compute_E_gr_thread / kernel_compute_H_gr_thread
+    (field_solver_gr.cu:81-225) over [1, dims - 1)."""
+    for A in range(3):
+        st = ST_E[A]
+        m = _cks_at(GE, a, st, T)
+        iD = [GE.S(D[c]) if c == A else interp(GE, D[c], ST_E[c], st) for c in range(3)]
+        iB = [None if c == A else interp(GE, B[c], ST_B[c], st) for c in range(3)]
+        dd = m.lower(iD)[A]
+        b, c = (A + 1) % 3, (A + 2) % 3
+        GE.S(Ed[A])[...] = m.alpha * dd + m.sqrt_gamma * (m.beta_u[b] * iB[c] -
+                                                          m.beta_u[c] * iB[b])
+    for A in range(3):
+        st = ST_B[A]
+        m = _cks_at(GE, a, st, T)
+        iB = [GE.S(B[c]) if c == A else interp(GE, B[c], ST_B[c], st) for c in range(3)]
+        iD = [None if c == A else interp(GE, D[c], ST_E[c], st) for c in range(3)]
+        bd = m.lower(iB)[A]
+        b, c = (A + 1) % 3, (A + 2) % 3
+        GE.S(Hd[A])[...] = m.alpha * bd - m.sqrt_gamma * (m.beta_u[b] * iD[c] -
+                                                          m.beta_u[c] * iD[b])
+        GE.S(Bd[A])[...] = bd
+
+
+def _gr_rho(G: Geo, a, T, D, rho):
+    """kernel_compute_rho_gr_thread (field_solver_gr.cu:29-53): the
+    sqrt(gamma)-weighted divergence of D at the vertices."""
+    ft = G.ft
+    x, y, z = (G.pos(c, 1) for c in range(3))
+    h = [ft(G.delta[c] / 2.0) for c in range(3)]
+
+    def sg(xx, yy, zz):
+        return Cks(a, xx, yy, zz, T).sqrt_gamma
+    rho[:] = 0
+    G.S(rho)[...] = (G.inv[0] * (G.S(D[0]) * sg(x + h[0], y, z) - G.S(D[0], 0, 0, -1) *
+                                 sg(x - h[0], y, z)) +
+                     G.inv[1] * (G.S(D[1]) * sg(x, y + h[1], z) - G.S(D[1], 0, -1, 0) *
+                                 sg(x, y - h[1], z)) +
+                     G.inv[2] * (G.S(D[2]) * sg(x, y, z + h[2]) - G.S(D[2], -1, 0, 0) *
+                                 sg(x, y, z - h[2]))) / sg(x, y, z)
+
+
+def _gr_push(G: Geo, p, a, T, Ed, Hd, B, Bd, rho, dD, dB):
+    """kernel_rk_push_gr_thread (field_solver_gr.cu:227-378)."""
+    ft = G.ft
+    S = G.S
+    dt = ft(p["dt"])
+    CCx, CCy, CCz = (dt * G.inv[c] for c in range(3))
+    ex, ey, ez = Ed
+    hx, hy, hz = Hd
+    sgB = [_cks_at(G, a, ST_B[c], T).sqrt_gamma for c in range(3)]
+    sgE = [_cks_at(G, a, ST_E[c], T).sqrt_gamma for c in range(3)]
+    S(dB[0])[...] = (CCz * (S(ey, 1) - S(ey)) - CCy * (S(ez, 0, 1) - S(ez))) / sgB[0]
+    S(dB[1])[...] = (CCx * (S(ez, 0, 0, 1) - S(ez)) - CCz * (S(ex, 1) - S(ex))) / sgB[1]
+    S(dB[2])[...] = (CCy * (S(ex, 0, 1) - S(ex)) - CCx * (S(ey, 0, 0, 1) - S(ey))) / sgB[2]
+    S(dD[0])[...] = (CCz * (S(hy, -1) - S(hy)) - CCy * (S(hz, 0, -1) - S(hz))) / sgE[0]
+    S(dD[1])[...] = (CCx * (S(hz, 0, 0, -1) - S(hz)) - CCz * (S(hx, -1) - S(hx))) / sgE[1]
+    S(dD[2])[...] = (CCy * (S(hx, 0, -1) - S(hx)) - CCx * (S(hy, 0, 0, -1) - S(hy))) / sgE[2]
+    if not p.get("calc_current", True):
+        return
+    for A in range(3):
+        out = ST_E[A]
+        ir = interp(G, rho, ST_RHO, out)
+        ie = [interp(G, Ed[c], ST_E[c], out) for c in range(3)]
+        ib = [interp(G, B[c], ST_B[c], out) for c in range(3)]
+        ibd = [interp(G, Bd[c], ST_B[c], out) for c in range(3)]
+        b, c = (A + 1) % 3, (A + 2) % 3
+        cross = ie[b] * ibd[c] - ibd[b] * ie[c]
+        den = ib[0] * ibd[0] + ib[1] * ibd[1] + ib[2] * ibd[2] + T
+        S(dD[A])[...] = S(dD[A]) - dt * ir * cross / sgE[A] / den
+
+
+def _gr_clean(G: Geo, a, T, D, B, dD):
+    """kernel_clean_epar_gr_thread (field_solver_gr.cu:416-517)."""
+    for A in range(3):
+        st = ST_E[A]
+        m = _cks_at(G, a, st, T)
+        iD = [G.S(D[c]) if c == A else interp(G, D[c], ST_E[c], st) for c in range(3)]
+        iB = [interp(G, B[c], ST_B[c], st) for c in range(3)]
+        bd = m.lower(iB)
+        dot = iD[0] * bd[0] + iD[1] * bd[1] + iD[2] * bd[2]
+        den = iB[0] * bd[0] + iB[1] * bd[1] + iB[2] * bd[2] + T
+        G.S(dD[A])[...] = G.S(D[A]) - dot * iB[A] / den
+
+
+def _gr_check(G: Geo, a, T, dD, B, D):
+    """kernel_check_eGTb_gr_thread (field_solver_gr.cu:519-647): reads dD
+    and B, writes D, so it is free of the flat solver's race."""
+    ft = G.ft
+    out = []
+    for A in range(3):
+        st = ST_E[A]
+        m = _cks_at(G, a, st, T)
+        iD = [G.S(dD[c]) if c == A else interp(G, dD[c], ST_E[c], st) for c in range(3)]
+        dd = m.lower(iD)
+        emag = iD[0] * dd[0] + iD[1] * dd[1] + iD[2] * dd[2] + T
+        iB = [interp(G, B[c], ST_B[c], st) for c in range(3)]
+        bd = m.lower(iB)
+        bmag = iB[0] * bd[0] + iB[1] * bd[1] + iB[2] * bd[2] + T
+        with np.errstate(invalid="ignore", divide="ignore"):
+            temp = np.where(emag > bmag, np.sqrt(bmag / emag), ft(1.0)).astype(ft)
+        out.append(temp * G.S(dD[A]))
+    for A in range(3):
+        G.S(D[A])[...] = out[A]
+
+
+def _gr_absorbing(G: Geo, p, a, T, U, Un):
+    """kernel_absorbing_boundary_gr_thread (field_solver_gr.cu:661-775): the
+    damping layer inside 0.8 r_H (rate sig0 cube((r1 - r) / (0.2 r_H)) dt at
+    each component's position), zero inside 0.01 r_H, the outer layer
+    (pmlsigma_gr), and the start-of-step values on and beyond the box edge."""
+    ft = G.ft
+    f8 = np.float64
+    x, y, z = (G.pos(c, 1) for c in range(3))
+    shape = G.S(U[0]).shape
+    rH = ft(1.0 + np.sqrt(1.0 - f8(a * a)))
+    r1, r2, dd = ft(0.8 * f8(rH)), ft(0.01 * f8(rH)), ft(0.2 * f8(rH))
+    sig0 = ft(p["sigpml"])
+    dt = ft(p["dt"])
+    h = [ft(G.delta[c] / 2.0) for c in range(3)]
+    r = np.broadcast_to(Cks(a, x, y, z, T).r, shape)
+    off = [(h[0], 0, 0), (0, h[1], 0), (0, 0, h[2]), (0, h[1], h[2]), (h[0], 0, h[2]),
+           (h[0], h[1], 0)]
+    for c in range(6):
+        u, un = G.S(U[c]), G.S(Un[c])
+        rc = Cks(a, x + ft(off[c][0]), y + ft(off[c][1]), z + ft(off[c][2]), T).r
+        q = (r1 - rc) / dd
+        sig = np.broadcast_to((sig0 * (q * q * q)) * dt, shape)
+        act = (r < r1) & (sig > T)
+        s = np.where(act, sig, ft(1.0))
+        e = np.exp(-s)
+        new = ((e * un).astype(f8) + (1.0 - e.astype(f8)) / s.astype(f8) *
+               (u - un).astype(f8)).astype(ft)
+        u[...] = np.where(act, new, u)
+    for c in range(6):
+        u = G.S(U[c])
+        u[...] = np.where(r < r2, ft(0), u)
+    pml = p["pml"]
+    hi = [G.lower[c] + G.size[c] - ft(pml[c]) * G.delta[c] for c in range(3)]
+    lo = [G.lower[c] + ft(pml[c]) * G.delta[c] for c in range(3)]
+    scale = ft(p["pmllen"]) * G.delta[0]
+
+    def ps(v, vl, vh):
+        qh = ((v - vh) / scale).astype(f8)
+        ql = ((vl - v) / scale).astype(f8)
+        return np.where(v > vh, (f8(sig0) * qh ** 3.0).astype(ft),
+                        np.where(v < vl, (f8(sig0) * ql ** 3.0).astype(ft), ft(0)))
+    outside = np.broadcast_to((x > hi[0]) | (x < lo[0]) | (y > hi[1]) | (y < lo[1]) |
+                              (z > hi[2]) | (z < lo[2]), shape)
+    sig = np.broadcast_to((ps(x, lo[0], hi[0]) + ps(y, lo[1], hi[1]) + ps(z, lo[2], hi[2])
+                           ).astype(ft), shape)
+    act = outside & (sig > T)
+    if act.any():
+        s = np.where(act, sig, ft(1.0))
+        e = np.exp(-s)
+        for c in range(6):
+            u, un = G.S(U[c]), G.S(Un[c])
+            new = ((e * un).astype(f8) + (1.0 - e.astype(f8)) / s.astype(f8) *
+                   (u - un).astype(f8)).astype(ft)
+            u[...] = np.where(act, new, u)
+    up = [G.lower[c] + G.size[c] for c in range(3)]
+    edge = np.broadcast_to((x <= G.lower[0]) | (x >= up[0]) | (y <= G.lower[1]) |
+                           (y >= up[1]) | (z <= G.lower[2]) | (z >= up[2]), shape)
+    for c in range(6):
+        u, un = G.S(U[c]), G.S(Un[c])
+        u[...] = np.where(edge, un, u)
+
+
+def gryee_evolve(p, U: np.ndarray, nsteps: int):
+    """Advance U = (Dx, Dy, Dz, Bx, By, Bz[, P]) by nsteps
+    field_solver_gr::evolve_fields_gr calls (field_solver_gr.cu:810-861):
+    per substep E and H over [1, dims - 1), rho, push, update, then the
+    E_par cleaning (last substep, clean_ep), the rescale (check_egb) and the
+    absorbing layers (last substep).  The axes are not periodic."""
+    p = as_dict(p)
+    U = np.array(U, copy=True)
+    ft = U.dtype.type
+    T = ft(tiny(ft))
+    G = Geo(p, U.dtype)
+    GE = G.boxed([1, 1, 1], [d - 1 for d in G.d])
+    a = ft(p["a"])
+    D, B = U[0:3], U[3:6]
+    Ed, Hd, Bd = np.zeros_like(D), np.zeros_like(B), np.zeros_like(B)
+    rho = np.zeros_like(D[0])
+    for _ in range(nsteps):
+        Dn, Bn = D.copy(), B.copy()
+        dD, dB = np.zeros_like(D), np.zeros_like(B)
+        for sub, (c1, c2, c3, _tf) in enumerate(RK3):
+            last = sub == 2
+            _gr_eh(GE, a, T, D, B, Ed, Hd, Bd)
+            _gr_rho(G, a, T, D, rho)
+            _gr_push(G, p, a, T, Ed, Hd, B, Bd, rho, dD, dB)
+            _update(G, D, Dn, dD, c1, c2, c3)
+            for c in range(3):
+                G.S(dD[c])[...] = G.S(D[c])
+            _update(G, B, Bn, dB, c1, c2, c3)
+            if last and p.get("clean_ep", True):
+                _gr_clean(G, a, T, D, B, dD)
+            if p.get("check_egb", True):
+                _gr_check(G, a, T, dD, B, D)
+            if last:
+                _gr_absorbing(G, p, a, T, U[0:6], np.concatenate([Dn, Bn]))
     return U

@@ -7,7 +7,7 @@ the reference sources).  Needs a GPU:
 
 Each fixture ``<name>.npz`` holds
   params_toml  the config.toml the reference read,
-  solver       "sph", "cyl", "gr" or "yee",
+  solver       "sph", "cyl", "gr", "yee" or "gryee",
   steps,
   out_f64      the double build's E (D for GR), B, P after `steps`
                evolve_fields calls, arrays of shape (d2, d1, d0).
@@ -56,6 +56,10 @@ def variant_cases():
     out.append(("yee16", "yee", p, problems.alfven_plane_wave_fields(p, np.float64, yee=True), 6))
     p, f = yee_mixed_case()
     out.append(("yee_mixed16", "yee", p, f, 6))
+
+    # staggered solver in Kerr-Schild coordinates (field_solver_gr)
+    p = problems.wald_params(N=12, half_size=3.0, a=0.9, pml=2)
+    out.append(("gryee12", "gryee", p, problems.wald_fields(p, np.float64, yee=True), 3))
     return out
 
 

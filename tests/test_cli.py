@@ -151,6 +151,7 @@ def test_restart_from_snapshot_continues_the_run(tmp_path):
     ("wave-yee", lambda: _wave_params(16)),
     ("pulsar3d-yee", lambda: problems.pulsar_params(24)),
     ("alfven3d-yee", lambda: _with(problems.pulsar_params(24), problem=2)),
+    ("gr-yee", lambda: problems.wald_params(16)),
 ])
 def test_every_driver_runs(tmp_path, driver, make):
     p = make()

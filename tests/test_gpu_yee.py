@@ -235,3 +235,48 @@ def test_yee_rejects_unsupported_configurations():
     s.close()
     data.close()
     env.close()
+
+
+# ------------------------------------------------------ Kerr-Schild (field_solver_gr)
+
+GR_CASES = {
+    # Wald field around a spin-0.9 hole: inner and outer absorbing layers
+    "gryee_wald": dict(),
+    # no E_par cleaning, no rescale: the current and the layers alone
+    "gryee_wald_noclamps": dict(clean_ep=False, check_egb=False),
+    # rescale without cleaning: the cleaned D is never stored
+    "gryee_wald_check_only": dict(clean_ep=False),
+}
+
+
+@pytest.mark.parametrize("case", sorted(GR_CASES))
+def test_gryee_matches_reference_gpu_build(case):
+    """field_solver_gr (evolve_fields_gr) against the reference's float and
+    double GPU builds; its rescale reads dD and writes D, so it has no race
+    and the whole grid is compared."""
+    from coffee_b200.solver import FieldSolverGr
+    _need_refgpu()
+    p = problems.wald_params(N=24, half_size=4.0, a=0.9, pml=4)
+    for k, v in GR_CASES[case].items():
+        setattr(p, k, v)
+    nsteps = 8
+    f64 = problems.wald_fields(p, np.float64, yee=True)
+    f32 = [a.astype(np.float32) for a in f64]
+    r64, _, _ = oracle.run_reference_gpu("gryee", p, f64, nsteps)
+    r32, _, _ = oracle.run_reference_gpu("gryee", p, f32, nsteps)
+    env = SimEnvironment(p)
+    data = SimData(env, np.float32)
+    data.upload(f32)
+    s = FieldSolverGr(data, env)
+    s.step(0.0, nsteps)
+    out = data.download()
+    s.close()
+    data.close()
+    env.close()
+    ok, rep = fp32_parity(out, r32, r64)
+    print(f"--- {case}\n{rep}")
+    assert ok, f"{case}: FP32 parity with the reference GPU build failed\n{rep}"
+    np64 = yo.gryee_evolve(p, np.stack(f64), nsteps)
+    worst = max(rel_l2(np64[f], r64[f]) for f in range(6))
+    print(f"numpy restatement vs reference double build: {worst:.2e}")
+    assert worst < 1e-9, f"{case}: numpy restatement departs from the reference ({worst:.2e})"

@@ -47,6 +47,8 @@ def test_restatement_matches_reference_gpu_double(name):
         out = axisym_oracle.sph_evolve(p, np.stack([a[0] for a in f64]), steps)[:, None]
     elif solver == "cyl":
         out = axisym_oracle.cyl_evolve(p, np.stack([a[0] for a in f64]), steps)[:, None]
+    elif solver == "gryee":
+        out = yee_oracle.gryee_evolve(p, np.stack(f64), steps)
     elif solver == "yee":
         b0 = np.stack(f64[7:10]) if len(f64) > 7 else None
         out = yee_oracle.yee_evolve(p, np.stack(f64[:7]), steps, B0=b0)
