@@ -112,6 +112,25 @@ SIGNATURES = {
     "coffee_batch_info": (_i, [_vp, _P(_i), _P(_i), _P(_i), _P(_d)]),
     "coffee_batch_destroy": (_i, [_vp]),
     "coffee_evolve_noalloc": (_i, [_P(CoffeeParams), _i, _P(_vp), _d, _i, _vp]),
+    # learned warm start (include/coffee_surrogate.h); all pointers are device pointers
+    "coffee_conv3d_forward": (_i, [_vp, _i, _i, _i, _i, _i, _vp, _i, _vp, _vp, _vp, _i,
+                                   ctypes.c_float, _vp]),
+    "coffee_conv3d_flip_weights": (_i, [_vp, _i, _i, _vp, _vp]),
+    "coffee_conv3d_backward_data": (_i, [_vp, _i, _i, _i, _i, _i, _vp, _i, _vp, _vp]),
+    "coffee_conv3d_backward_weight_workspace": (ctypes.c_size_t, [_i, _i]),
+    "coffee_conv3d_backward_weight": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp]),
+    "coffee_bias_grad": (_i, [_vp, ctypes.c_longlong, _i, _vp, _vp]),
+    "coffee_leaky_backward": (_i, [_vp, _vp, ctypes.c_longlong, ctypes.c_float, _vp, _vp, _vp]),
+    "coffee_pool2_forward": (_i, [_vp, _i, _i, _i, _i, _i, _vp, _vp]),
+    "coffee_pool2_backward_add": (_i, [_vp, _i, _i, _i, _i, _i, _vp, _vp]),
+    "coffee_up2_forward": (_i, [_vp, _i, _i, _i, _i, _i, _vp, _i, _i, _vp]),
+    "coffee_up2_backward": (_i, [_vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp]),
+    "coffee_channels_copy": (_i, [_vp, ctypes.c_longlong, _i, _vp, _i, _i, _vp]),
+    "coffee_channels_add": (_i, [_vp, ctypes.c_longlong, _i, _i, _i, _vp, _vp]),
+    "coffee_mse": (_i, [_vp, _vp, _vp, ctypes.c_longlong, _i, _d, _vp, _vp, _vp]),
+    "coffee_adam": (_i, [_vp, _vp, _vp, _vp, ctypes.c_longlong, ctypes.c_float, ctypes.c_float,
+                         ctypes.c_float, ctypes.c_float, _i, _vp, _vp]),
+    "coffee_to_bf16": (_i, [_vp, ctypes.c_longlong, _vp, _vp]),
 }
 
 _lib = None

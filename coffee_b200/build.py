@@ -19,7 +19,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libcoffee_b200.so")
 
 SOURCES = ["coffee_abi.cu", "coffee_params.cpp", "axisym.cu", "gr.cu", "yee.cu",
-           "coffee_noalloc.cu"]
+           "coffee_noalloc.cu", "surrogate.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1,0 +1,177 @@
+"""The learned warm start (coffee_b200/surrogate.py, include/coffee_surrogate.h).
+
+CPU: the FP64 convolution restatement (oracle/conv_oracle.py) against
+finite differences.  GPU: the BF16 tensor-core convolution kernels and their
+gradients against the restatement on the same BF16-rounded operands, the
+whole network's gradients against the restatement of the network, training
+that lowers the loss, and the warm start's gain on the rotating star."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import conv_oracle as co
+
+
+def _fd(f, a, idx, eps=1e-6):
+    ap, am = a.copy(), a.copy()
+    ap[idx] += eps
+    am[idx] -= eps
+    return (f(ap) - f(am)) / (2 * eps)
+
+
+def test_oracle_gradients_match_finite_differences():
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((2, 4, 3, 5, 3))
+    w = rng.standard_normal((4, 27, 3))
+    b = rng.standard_normal(4)
+    dy = rng.standard_normal((2, 4, 3, 5, 4))
+    gx = co.conv3d_grad_input(dy, w)
+    gw = co.conv3d_grad_weight(dy, x)
+    for idx in [(0, 0, 0, 0, 0), (1, 3, 2, 4, 2), (0, 2, 1, 3, 1)]:
+        fd = _fd(lambda xx: float((co.conv3d(xx, w, b) * dy).sum()), x, idx)
+        assert abs(fd - gx[idx]) < 1e-6 * max(1.0, abs(fd))
+    for idx in [(0, 0, 0), (3, 13, 2), (2, 26, 1)]:
+        fd = _fd(lambda ww: float((co.conv3d(x, ww, b) * dy).sum()), w, idx)
+        assert abs(fd - gw[idx]) < 1e-6 * max(1.0, abs(fd))
+
+
+def test_oracle_network_gradients_match_finite_differences():
+    """The restated network's backward pass (bf16 rounding off: identity)."""
+    rng = np.random.default_rng(1)
+    shapes = [(16, 16), (16, 16), (32, 16), (32, 32), (16, 48), (16, 16)]
+    ws = [rng.standard_normal((k, 27, c)) * 0.1 for k, c in shapes]
+    bs = [rng.standard_normal(k) * 0.1 for k, _ in shapes]
+    x = rng.standard_normal((1, 4, 4, 4, 16))
+    tgt = rng.standard_normal((1, 4, 4, 4, 16))
+    mask = (rng.random((1, 4, 4, 4)) > 0.3).astype(float)
+    saved = co.bf16
+    co.bf16 = lambda a: np.asarray(a, np.float64)
+    try:
+        _, dws, dbs, _ = co.unet_forward_backward(ws, bs, x, tgt, mask)
+        for layer, idx in [(0, (3, 5, 7)), (2, (10, 20, 4)), (4, (2, 13, 40)), (5, (7, 26, 9))]:
+            def f(wl):
+                w2 = list(ws)
+                w2[layer] = wl
+                return co.unet_forward_backward(w2, bs, x, tgt, mask)[0]
+            fd = _fd(f, ws[layer], idx)
+            assert abs(fd - dws[layer][idx]) < 1e-5 * max(1e-3, abs(fd)), (layer, fd, dws[layer][idx])
+    finally:
+        co.bf16 = saved
+
+
+# ------------------------------------------------------------------ GPU
+
+def _torch():
+    import torch
+    return torch
+
+
+def _bf16_tensor(a):
+    torch = _torch()
+    return torch.from_numpy(np.asarray(a, np.float32)).cuda().to(torch.bfloat16)
+
+
+def _np(t):
+    torch = _torch()
+    return t.to(torch.float32).cpu().numpy().astype(np.float64)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("c,k", [(16, 16), (16, 32), (48, 16), (32, 64)])
+def test_conv_kernels_match_oracle(c, k):
+    from coffee_b200 import surrogate as sg
+    torch = _torch()
+    rng = np.random.default_rng(c + k)
+    shape = (2, 6, 5, 7)
+    x = co.bf16(rng.standard_normal(shape + (c,)))
+    w = co.bf16(rng.standard_normal((k, 27, c)) * 0.2)
+    b = rng.standard_normal(k).astype(np.float32)
+    xt, wt = _bf16_tensor(x), _bf16_tensor(w)
+    bt = torch.from_numpy(b).cuda()
+    z = torch.empty(shape + (k,), dtype=torch.float32, device="cuda")
+    a = torch.empty(shape + (k,), dtype=torch.bfloat16, device="cuda")
+    sg.conv_forward(xt, wt, bt, k, True, z, a)
+    ref = co.conv3d(x, w, b)
+    assert _rel(_np(z), ref) < 1e-5
+    # the BF16 activation is the rounded leaky(z) of the kernel's own z
+    assert np.array_equal(_np(a), co.bf16(co.leaky(_np(z))))
+    # gradients for a BF16 dy
+    dy = co.bf16(rng.standard_normal(shape + (k,)))
+    dyt = _bf16_tensor(dy)
+    wflip = torch.empty((c, 27, k), dtype=torch.bfloat16, device="cuda")
+    sg.flip_weights(wt, wflip)
+    dx = torch.empty(shape + (c,), dtype=torch.float32, device="cuda")
+    sg.conv_backward_data(dyt, wflip, c, dx)
+    assert _rel(_np(dx), co.conv3d_grad_input(dy, w)) < 1e-5
+    dw = torch.empty((k, 27, c), dtype=torch.float32, device="cuda")
+    ws = torch.empty(sg.workspace_bytes(k, c), dtype=torch.uint8, device="cuda")
+    sg.conv_backward_weight(dyt, xt, dw, ws)
+    assert _rel(_np(dw), co.conv3d_grad_weight(dy, x)) < 1e-5
+
+
+@pytest.mark.gpu
+def test_network_gradients_match_oracle():
+    """Loss and every layer's gradients of the U-Net on the library's kernels
+    against the FP64 restatement with the same BF16 rounding points."""
+    from coffee_b200 import surrogate as sg
+    torch = _torch()
+    rng = np.random.default_rng(3)
+    net = sg.UNet(seed=5)
+    shape = (2, 8, 8, 6)
+    x = co.bf16(rng.standard_normal(shape + (16,)))
+    tgt = rng.standard_normal(shape + (16,)).astype(np.float32)
+    mask = (rng.random(shape) > 0.2).astype(np.float32)
+    out = net.forward(_bf16_tensor(x))
+    loss, dout = net.loss(out, torch.from_numpy(tgt).cuda(), torch.from_numpy(mask).cuda())
+    net.backward(dout)
+    torch.cuda.synchronize()
+    ws = [L.w.cpu().numpy().astype(np.float64) for L in net.layers]
+    bs = [L.b.cpu().numpy().astype(np.float64) for L in net.layers]
+    rloss, dws, dbs, rout = co.unet_forward_backward(ws, bs, x, tgt.astype(np.float64),
+                                                     mask.astype(np.float64))
+    assert _rel(out.cpu().numpy(), rout) < 1e-3
+    assert abs(float(loss) - rloss) < 1e-3 * rloss
+    for i, L in enumerate(net.layers):
+        gw = L.gw.cpu().numpy()
+        gb = L.gb.cpu().numpy()
+        print(i, _rel(gw, dws[i]), _rel(gb, dbs[i]))
+        assert _rel(gw, dws[i]) < 2e-2, i
+        assert _rel(gb, dbs[i]) < 2e-2, i
+
+
+@pytest.mark.gpu
+def test_training_lowers_the_loss():
+    """Adam on the library's kernels fits a smooth synthetic map."""
+    from coffee_b200 import surrogate as sg
+    torch = _torch()
+    rng = np.random.default_rng(4)
+    net = sg.UNet(seed=1)
+    shape = (2, 16, 16, 16)
+    zz, yy, xx = np.meshgrid(*[np.linspace(-1, 1, 16)] * 3, indexing="ij")
+    x = np.zeros(shape + (16,), np.float32)
+    tgt = np.zeros(shape + (16,), np.float32)
+    for n in range(2):
+        ph = rng.uniform(0, 6.3, 3)
+        x[n, ..., 0] = np.sin(3 * xx + ph[0])
+        x[n, ..., 1] = np.cos(2 * yy + ph[1]) * zz
+        x[n, ..., 2] = xx * yy
+        tgt[n, ..., 0] = 0.5 * x[n, ..., 0] * x[n, ..., 1]
+        tgt[n, ..., 1] = np.roll(x[n, ..., 2], 1, axis=0)
+    xt = _bf16_tensor(x)
+    tt = torch.from_numpy(tgt).cuda()
+    mt = torch.ones(shape, device="cuda")
+    losses = []
+    for it in range(300):
+        out = net.forward(xt)
+        loss, dout = net.loss(out, tt, mt)
+        net.backward(dout)
+        net.step(3e-3)
+        if it % 50 == 0 or it == 299:
+            losses.append(float(loss))
+    print(losses)
+    assert losses[-1] < 0.1 * losses[0]
