@@ -676,6 +676,97 @@ def run_variant(args):
     return 0
 
 
+# ------------------------------------------------------ learned warm start
+# --workload surrogate: training steps of the 3D U-Net (coffee_b200/surrogate.py)
+# on the library's BF16 tensor-core kernels: 8 samples of 64^3, forward +
+# masked MSE + backward + Adam per step.  The roofline line is the largest
+# convolution's forward kernel (48 -> 16 channels) against the measured
+# dense BF16 tensor peak; --study adds the warm-start study.
+
+def run_surrogate(args):
+    import numpy as np
+    import torch
+
+    from coffee_b200 import surrogate as sg
+
+    ws, rank, local = _dist()
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the learned warm start has no "
+                              "counterpart in the reference"}), flush=True)
+        return 0
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n, side = 8, 64
+    rng = np.random.default_rng(0)
+    x = torch.from_numpy(rng.standard_normal((n, side, side, side, sg.CIN)).astype(np.float32))
+    x = x.to(dev).to(torch.bfloat16)
+    tgt = torch.from_numpy(rng.standard_normal((n, side, side, side, sg.COUT)).astype(np.float32))
+    tgt = tgt.to(dev)
+    mask = torch.ones((n, side, side, side), device=dev)
+    net = sg.UNet(seed=0, device=str(dev))
+
+    def train_step():
+        out = net.forward(x)
+        _, dout = net.loss(out, tgt, mask)
+        net.backward(dout)
+        net.step(1e-3)
+
+    for _ in range(args.warmup):
+        train_step()
+    torch.cuda.synchronize(dev)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    w0 = time.time()
+    e0.record(stream)
+    for _ in range(args.steps):
+        train_step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop(w0, time.time())
+    ms = e0.elapsed_time(e1) / args.steps
+    vox = n * side ** 3
+    # the largest convolution alone: layer 5, 48 -> 16 channels at full size
+    L = net.layers[4]
+    cat = net._saved["cat"]
+    z = torch.empty(cat.shape[:4] + (L.cout,), dtype=torch.float32, device=dev)
+    a = torch.empty(cat.shape[:4] + (L.cout,), dtype=torch.bfloat16, device=dev)
+    for _ in range(3):
+        sg.conv_forward(cat, L.wb, L.b, L.cout, True, z, a)
+    e0.record(stream)
+    reps = 10
+    for _ in range(reps):
+        sg.conv_forward(cat, L.wb, L.b, L.cout, True, z, a)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    conv_ms = e0.elapsed_time(e1) / reps
+    flops = 2.0 * 27 * L.cin * L.cout * vox
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, kind = float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        peak, kind = 1590.0, "fallback"
+    achieved = flops / (conv_ms / 1e3) / 1e12
+    line = {"metric": "training voxels/s", "value": vox / (ms / 1e3), "unit": "voxels/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+            "data": "synthetic (random inputs and targets)",
+            "config": {"workload": "surrogate-unet64", "samples": n, "grid": [side] * 3,
+                       "channels": [sg.CIN, sg.C1, sg.C2, sg.COUT],
+                       "step": "forward + masked MSE + backward + Adam, all on the library's kernels"},
+            "roofline": {"kernel": "conv3d_fwd_kernel (48 -> 16 channels, 64^3 x 8)",
+                         "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "peak_kind": kind, "frac": achieved / peak, "traffic": None,
+                         "avg_launch_ms": conv_ms, "flops_per_launch": flops},
+            "gpu_launches": None, "clocks": clk}
+    if args.study:
+        line["warm_start_study"] = sg.warm_start_study()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -690,10 +781,14 @@ def main():
                          "benchmark)")
     ap.add_argument("--workload", default="turbulence",
                     choices=["turbulence", "gr-wald", "logsph-batch", "logsph", "cyl-pulsar",
-                             "yee-wave", "yee-pulsar", "gryee-wald"])
+                             "yee-wave", "yee-pulsar", "gryee-wald", "surrogate"])
+    ap.add_argument("--study", action="store_true",
+                    help="with --workload surrogate: also run the warm-start study")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.workload == "surrogate":
+        return run_surrogate(args)
     if args.workload != "turbulence":
         return run_variant(args)
     if args.impl == "reference":

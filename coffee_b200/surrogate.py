@@ -309,3 +309,148 @@ def apply_prediction(p, start, pred):
         full[g:-g, g:-g, g:-g] = pred[..., c]
         out[c] = np.where(keep, start[c] + full / scale, start[c]).astype(start[c].dtype)
     return out
+
+
+# --------------------------------------------------------- warm-start study
+
+def star_run(p, fields, steps, lum_radius, every=10):
+    """Run the flat solver (GPU build's arithmetic) from `fields` for
+    `steps` steps; returns the final fields and the luminosity through the
+    sphere r = lum_radius every `every` steps: [(step, L), ...]."""
+    from .solver import FieldSolverEZ, SimData, SimEnvironment
+    env = SimEnvironment(p)
+    data = SimData(env, np.float32)
+    data.upload(fields)
+    s = FieldSolverEZ(data, env, "gpu")
+    dt = np.float32(p.dt)
+    t = np.float32(0.0)
+    hist = [(0, s.luminosity(lum_radius))]
+    done = 0
+    while done < steps:
+        n = min(every, steps - done)
+        s.step(float(t), n)
+        for _ in range(n):
+            t = np.float32(t + dt)
+        done += n
+        hist.append((done, s.luminosity(lum_radius)))
+    out = data.download()
+    s.close()
+    data.close()
+    env.close()
+    return out, hist
+
+
+def rotation_mean(hist, period):
+    """The luminosity averaged over the last rotation period at every
+    recorded step that has a full period behind it.  The flux of an oblique
+    rotator through a sphere is steady only on average: on a Cartesian grid
+    it is modulated at the rotation period."""
+    steps = np.array([s for s, _ in hist], float)
+    lums = np.array([l for _, l in hist], float)
+    out = []
+    for s in steps:
+        if s < period:
+            continue
+        sel = (steps > s - period) & (steps <= s)
+        out.append((int(s), float(lums[sel].mean())))
+    return out
+
+
+def settle_step(series, l_ref, tol=0.02):
+    """The first step of `series` [(step, value)] from which the value stays
+    within tol of l_ref to the end."""
+    settled = series[-1][0]
+    for step, lum in reversed(series):
+        if abs(lum - l_ref) > tol * abs(l_ref):
+            break
+        settled = step
+    return settled
+
+
+def _batch(p, samples):
+    torch = _torch()
+    xs, ts, ms = [], [], []
+    for incl, start, steady in samples:
+        xs.append(features(p, start, incl))
+        t, m = target_and_mask(p, start, steady)
+        ts.append(t)
+        ms.append(m)
+    x = torch.from_numpy(np.stack(xs)).cuda().to(torch.bfloat16)
+    return x, torch.from_numpy(np.stack(ts)).cuda(), torch.from_numpy(np.stack(ms)).cuda()
+
+
+def train(net, p, samples, iters, lr=2e-3, log_every=50):
+    """Full-batch Adam on the library's kernels; returns the loss history."""
+    x, tgt, mask = _batch(p, samples)
+    losses = []
+    for it in range(iters):
+        out = net.forward(x)
+        loss, dout = net.loss(out, tgt, mask)
+        net.backward(dout)
+        rate = lr * (0.1 ** (it / max(1, iters)))
+        net.step(rate)
+        if it % log_every == 0 or it == iters - 1:
+            losses.append((it, float(loss)))
+    return losses
+
+
+def predict(net, p, start, incl):
+    torch = _torch()
+    x = torch.from_numpy(features(p, start, incl)[None]).cuda().to(torch.bfloat16)
+    out = net.forward(x)
+    return apply_prediction(p, start, out[0].cpu().numpy())
+
+
+def warm_start_study(N=64, train_incl=(0, 15, 30, 45, 60, 75, 90), test_incl=(38, 68),
+                     periods=4.0, iters=2000, lum_radius=4.5, seed=0):
+    """Train the network on rotating-star runs at `train_incl` (degrees),
+    each run `periods` rotation periods from its dipole; then for every
+    held-out inclination run the plain cold start and the warm start for the
+    same number of steps and compare when their spindown luminosity (the
+    mean over the last rotation period) settles within 2% of the cold run's
+    final value."""
+    import time
+    p0 = star_params(N, 0.0)
+    period = int(round(2 * math.pi / (p0.omega * float(np.float32(p0.dt)))))
+    steps = int(round(periods * period))
+    every = max(1, period // 20)
+    t0 = time.time()
+    samples = []
+    for incl in train_incl:
+        p = star_params(N, incl)
+        start = problems.pulsar_fields(p, np.float32)
+        steady, _ = star_run(p, start, steps, lum_radius, every)
+        samples.append((float(incl), start, steady))
+    t_gen = time.time() - t0
+    net = UNet(seed=seed)
+    t1 = time.time()
+    losses = train(net, p0, samples, iters)
+    _torch().cuda.synchronize()
+    t_train = time.time() - t1
+    results = []
+    for incl in test_incl:
+        p = star_params(N, incl)
+        start = problems.pulsar_fields(p, np.float32)
+        cold, hist_c = star_run(p, start, steps, lum_radius, every)
+        t2 = time.time()
+        warm0 = predict(net, p, start, incl)
+        t_infer = time.time() - t2
+        _, hist_w = star_run(p, warm0, steps, lum_radius, every)
+        mean_c, mean_w = rotation_mean(hist_c, period), rotation_mean(hist_w, period)
+        l_ref = mean_c[-1][1]
+        g = p.guard[0]
+        sl = (slice(g, -g),) * 3
+        _, mask = target_and_mask(p, start, cold)
+
+        def err(f):
+            num = sum(float(((f[c] - cold[c])[sl] ** 2 * mask).sum()) for c in range(6))
+            den = sum(float((cold[c][sl] ** 2 * mask).sum()) for c in range(6))
+            return math.sqrt(num / den)
+        sc, sw = settle_step(mean_c, l_ref), settle_step(mean_w, l_ref)
+        results.append({"inclination": incl, "L_steady": l_ref, "period_steps": period,
+                        "settle_step_cold": sc, "settle_step_warm": sw, "gain": sc / max(sw, 1),
+                        "L_first_period_cold": mean_c[0][1], "L_first_period_warm": mean_w[0][1],
+                        "field_error_dipole": err(start), "field_error_warm": err(warm0),
+                        "seconds_inference": t_infer})
+    return {"N": N, "steps": steps, "period_steps": period, "train_inclinations": list(train_incl),
+            "test": results, "loss": losses, "seconds_generate": t_gen, "seconds_train": t_train}
