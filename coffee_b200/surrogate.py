@@ -244,11 +244,11 @@ class UNet:
 
 # ------------------------------------------------------ the star problem
 
-def star_params(N=64, inclination_deg=30.0):
+def star_params(N=64, inclination_deg=30.0, omega=0.15):
     """The rotating-star configuration of the warm-start study: an inclined
-    dipole star of radius 1.5 turning at 0.15 (light cylinder 6.7) in a box of
-    half size 12 with an absorbing layer."""
-    p = problems.pulsar_params(N=N, guard=3, half_size=12.0, radius=1.5, omega=0.15, pml=8)
+    dipole star of radius 1.5 turning at omega (0.15: light cylinder 6.7) in a
+    box of half size 12 with an absorbing layer."""
+    p = problems.pulsar_params(N=N, guard=3, half_size=12.0, radius=1.5, omega=omega, pml=8)
     a = math.radians(inclination_deg)
     p.p1, p.p2, p.p3 = math.sin(a), 0.0, math.cos(a)
     return p
@@ -262,7 +262,7 @@ def _coords(p):
 def features(p, fields, inclination_deg):
     """Input channels (D, H, W, 16) of the interior: B r^3 / R^3 of the
     dipole state, x, y, z / half size, the star mask, sin and cos of the
-    inclination, zeros."""
+    inclination, the spin omega / 0.15, zeros."""
     g = p.guard[0]
     X, Y, Z = (c[g:-g, g:-g, g:-g] for c in _coords(p))
     R = np.sqrt(X * X + Y * Y + Z * Z)
@@ -275,6 +275,7 @@ def features(p, fields, inclination_deg):
     out[..., 6] = (R < p.radius).astype(np.float32)
     a = math.radians(inclination_deg)
     out[..., 7], out[..., 8] = math.sin(a), math.cos(a)
+    out[..., 9] = p.omega / 0.15
     return out
 
 
@@ -367,10 +368,10 @@ def settle_step(series, l_ref, tol=0.02):
     return settled
 
 
-def _batch(p, samples):
+def _batch(samples):
     torch = _torch()
     xs, ts, ms = [], [], []
-    for incl, start, steady in samples:
+    for p, incl, start, steady in samples:
         xs.append(features(p, start, incl))
         t, m = target_and_mask(p, start, steady)
         ts.append(t)
@@ -379,9 +380,11 @@ def _batch(p, samples):
     return x, torch.from_numpy(np.stack(ts)).cuda(), torch.from_numpy(np.stack(ms)).cuda()
 
 
-def train(net, p, samples, iters, lr=2e-3, log_every=50):
-    """Full-batch Adam on the library's kernels; returns the loss history."""
-    x, tgt, mask = _batch(p, samples)
+def train(net, samples, iters, lr=2e-3, log_every=50):
+    """Full-batch Adam on the library's kernels over samples
+    [(params, inclination, start fields, target fields)]; returns the loss
+    history."""
+    x, tgt, mask = _batch(samples)
     losses = []
     for it in range(iters):
         out = net.forward(x)
@@ -401,35 +404,42 @@ def predict(net, p, start, incl):
     return apply_prediction(p, start, out[0].cpu().numpy())
 
 
-def warm_start_study(N=64, train_incl=(0, 15, 30, 45, 60, 75, 90), test_incl=(38, 68),
-                     periods=4.0, iters=2000, lum_radius=4.5, seed=0):
-    """Train the network on rotating-star runs at `train_incl` (degrees),
-    each run `periods` rotation periods from its dipole; then for every
-    held-out inclination run the plain cold start and the warm start for the
-    same number of steps and compare when their spindown luminosity (the
-    mean over the last rotation period) settles within 2% of the cold run's
-    final value."""
+def warm_start_study(N=64, train_set=((0, 0.15), (15, 0.15), (30, 0.15), (45, 0.15), (60, 0.15),
+                                   (75, 0.15), (90, 0.15)),
+                     test_set=((38, 0.15), (68, 0.15)), periods=4.0, iters=2000, lum_radius=4.5,
+                     seed=0):
+    """Train the network on rotating-star runs at the (inclination in
+    degrees, spin) pairs of `train_set`, each run `periods` rotation periods from
+    its dipole; then for every held-out pair of `test_set` run the plain cold
+    start and the warm start for as long and compare when their spindown
+    luminosity (the mean over the last rotation period) settles within 2% of
+    the cold run's final value, and how far each start is from the cold
+    run's final fields."""
     import time
-    p0 = star_params(N, 0.0)
-    period = int(round(2 * math.pi / (p0.omega * float(np.float32(p0.dt)))))
-    steps = int(round(periods * period))
-    every = max(1, period // 20)
+
+    def period_steps(p):
+        return int(round(2 * math.pi / (p.omega * float(np.float32(p.dt)))))
     t0 = time.time()
     samples = []
-    for incl in train_incl:
-        p = star_params(N, incl)
+    for incl, om in train_set:
+        p = star_params(N, incl, om)
+        period = period_steps(p)
         start = problems.pulsar_fields(p, np.float32)
-        steady, _ = star_run(p, start, steps, lum_radius, every)
-        samples.append((float(incl), start, steady))
+        steady, _ = star_run(p, start, int(round(periods * period)), lum_radius,
+                             max(1, period // 20))
+        samples.append((p, float(incl), start, steady))
     t_gen = time.time() - t0
     net = UNet(seed=seed)
     t1 = time.time()
-    losses = train(net, p0, samples, iters)
+    losses = train(net, samples, iters)
     _torch().cuda.synchronize()
     t_train = time.time() - t1
     results = []
-    for incl in test_incl:
-        p = star_params(N, incl)
+    for incl, om in test_set:
+        p = star_params(N, incl, om)
+        period = period_steps(p)
+        steps = int(round(periods * period))
+        every = max(1, period // 20)
         start = problems.pulsar_fields(p, np.float32)
         cold, hist_c = star_run(p, start, steps, lum_radius, every)
         t2 = time.time()
@@ -447,10 +457,19 @@ def warm_start_study(N=64, train_incl=(0, 15, 30, 45, 60, 75, 90), test_incl=(38
             den = sum(float((cold[c][sl] ** 2 * mask).sum()) for c in range(6))
             return math.sqrt(num / den)
         sc, sw = settle_step(mean_c, l_ref), settle_step(mean_w, l_ref)
-        results.append({"inclination": incl, "L_steady": l_ref, "period_steps": period,
+        # the instantaneous luminosity (steady for an aligned rotator; an
+        # oblique one's is modulated at the rotation period)
+        ic, iw = settle_step(hist_c, l_ref), settle_step(hist_w, l_ref)
+        results.append({"inclination": incl, "omega": om, "L_steady": l_ref,
+                        "period_steps": period, "steps": steps,
                         "settle_step_cold": sc, "settle_step_warm": sw, "gain": sc / max(sw, 1),
+                        "settle_step_cold_instantaneous": ic,
+                        "settle_step_warm_instantaneous": iw,
+                        "gain_instantaneous": ic / max(iw, 1),
+                        "L_cold_history": [round(l, 6) for _, l in hist_c[:40]],
+                        "L_warm_history": [round(l, 6) for _, l in hist_w[:40]],
                         "L_first_period_cold": mean_c[0][1], "L_first_period_warm": mean_w[0][1],
                         "field_error_dipole": err(start), "field_error_warm": err(warm0),
                         "seconds_inference": t_infer})
-    return {"N": N, "steps": steps, "period_steps": period, "train_inclinations": list(train_incl),
-            "test": results, "loss": losses, "seconds_generate": t_gen, "seconds_train": t_train}
+    return {"N": N, "periods": periods, "train": [list(x) for x in train_set], "test": results,
+            "loss": losses, "seconds_generate": t_gen, "seconds_train": t_train}

@@ -186,8 +186,8 @@ def test_warm_start_is_closer_to_the_steady_state_than_the_dipole():
     not asserted: on this small box neither start settles within 2% in
     three periods.)"""
     from coffee_b200 import surrogate as sg
-    res = sg.warm_start_study(N=48, train_incl=(0, 20, 45, 70, 90), test_incl=(30,), periods=3.0,
-                              iters=600)
+    res = sg.warm_start_study(N=48, train_set=((0, 0.15), (20, 0.15), (45, 0.15), (70, 0.15),
+                                           (90, 0.15)), test_set=((30, 0.15),), periods=3.0, iters=600)
     print(res["test"], res["loss"][-1], res["seconds_train"])
     r = res["test"][0]
     assert r["field_error_warm"] < 0.8 * r["field_error_dipole"]
