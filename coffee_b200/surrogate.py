@@ -32,6 +32,9 @@ from ._lib import check
 
 SLOPE = 0.1
 CIN, C1, C2, COUT = 16, 16, 32, 16
+# the prediction is trained and applied outside STAR_EDGE star radii; inside,
+# the star's own boundary condition sets the fields
+STAR_EDGE = 1.5
 
 
 def _torch():
@@ -291,7 +294,7 @@ def target_and_mask(p, start, steady):
     for c in range(7):
         out[..., c] = (steady[c] - start[c])[g:-g, g:-g, g:-g] * scale
     edge = p.size[0] / 2 - p.pml[0] * p.size[0] / p.N[0]
-    mask = ((R > 1.5 * p.radius) & (np.abs(X) < edge) & (np.abs(Y) < edge) &
+    mask = ((R > STAR_EDGE * p.radius) & (np.abs(X) < edge) & (np.abs(Y) < edge) &
             (np.abs(Z) < edge)).astype(np.float32)
     return out, mask
 
@@ -303,7 +306,7 @@ def apply_prediction(p, start, pred):
     X, Y, Z = _coords(p)
     R = np.sqrt(X * X + Y * Y + Z * Z)
     scale = np.minimum((np.maximum(R, p.radius) / p.radius) ** 3, 1e4).astype(np.float32)
-    keep = R > 1.5 * p.radius
+    keep = R > STAR_EDGE * p.radius
     out = [a.copy() for a in start]
     for c in range(7):
         full = np.zeros_like(start[c])
