@@ -280,3 +280,59 @@ def test_gryee_matches_reference_gpu_build(case):
     worst = max(rel_l2(np64[f], r64[f]) for f in range(6))
     print(f"numpy restatement vs reference double build: {worst:.2e}")
     assert worst < 1e-9, f"{case}: numpy restatement departs from the reference ({worst:.2e})"
+
+
+def _run_ours64(cls, p, f64, nsteps, b0=None):
+    env = SimEnvironment(p)
+    data = SimData(env, np.float64)
+    data.upload(f64)
+    if b0 is not None:
+        data.upload_background(b0)
+    s = cls(data, env)
+    s.step(0.0, nsteps)
+    out = data.download()
+    s.close()
+    data.close()
+    env.close()
+    return out
+
+
+def test_yee_fp64_matches_reference_double_build():
+    """The FP64 build of the staggered solver (the two passes) against the
+    reference's double build: the same arithmetic in the same precision."""
+    _need_refgpu()
+    p, f64, b0 = _mixed_case()
+    nsteps = 6
+    r64, _, _ = oracle.run_reference_gpu("yee", p, list(f64) + list(b0), nsteps)
+    out = _run_ours64(FieldSolver, p, f64, nsteps, b0=b0)
+    worst = max(rel_l2(out[f], r64[f]) for f in range(6))
+    print(f"FP64 library vs reference double build: {worst:.2e}")
+    assert worst < 1e-10
+
+
+def test_gryee_fp64_matches_reference_double_build():
+    from coffee_b200.solver import FieldSolverGr
+    _need_refgpu()
+    p = problems.wald_params(N=16, half_size=3.0, a=0.9, pml=2)
+    f64 = problems.wald_fields(p, np.float64, yee=True)
+    nsteps = 4
+    r64, _, _ = oracle.run_reference_gpu("gryee", p, f64, nsteps)
+    out = _run_ours64(FieldSolverGr, p, f64, nsteps)
+    worst = max(rel_l2(out[f], r64[f]) for f in range(6))
+    print(f"FP64 library vs reference double build: {worst:.2e}")
+    assert worst < 1e-10
+
+
+def test_yee_one_guard_point():
+    """guard = 1, the least the staggered stencils need, against the
+    restatement."""
+    p = problems.alfven_params(N=16, guard=1)
+    p.dt = 0.3 / 16
+    f64 = problems.alfven_plane_wave_fields(p, np.float64, yee=True)
+    nsteps = 6
+    np64 = yo.yee_evolve(p, np.stack(f64), nsteps)
+    np32 = yo.yee_evolve(p, np.stack([a.astype(np.float32) for a in f64]), nsteps)
+    out = _run_ours(p, [a.astype(np.float32) for a in f64], nsteps)
+    ok, rep = fp32_parity(out, list(np32), list(np64))
+    print(rep)
+    assert ok, rep
