@@ -115,6 +115,9 @@ SIGNATURES = {
     # learned warm start (include/coffee_surrogate.h); all pointers are device pointers
     "coffee_conv3d_forward": (_i, [_vp, _i, _i, _i, _i, _i, _vp, _i, _vp, _vp, _vp, _i,
                                    ctypes.c_float, _vp]),
+    "coffee_conv3d_forward_tc": (_i, [_vp, _i, _i, _i, _i, _i, _vp, _i, _vp, _vp, _vp, _i,
+                                      ctypes.c_float, _vp]),
+    "coffee_conv3d_tc_fault": (_i, [_P(_i), _i]),
     "coffee_conv3d_flip_weights": (_i, [_vp, _i, _i, _vp, _vp]),
     "coffee_conv3d_backward_data": (_i, [_vp, _i, _i, _i, _i, _i, _vp, _i, _vp, _vp]),
     "coffee_conv3d_backward_weight_workspace": (ctypes.c_size_t, [_i, _i]),

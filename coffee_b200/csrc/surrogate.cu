@@ -440,6 +440,252 @@ int check_grid(int n, int d, int h, int w) {
   return COFFEE_OK;
 }
 
+// ------------------------------------------- forward on tcgen05 (sm_100a)
+// The same "same" 3x3x3 convolution as conv3d_fwd_kernel on the fifth-
+// generation tensor cores: D (128 points x N output channels, FP32) lives in
+// tensor memory and is built by 27 C / 16 tcgen05.mma steps of K = 16 (one
+// tap, 16 input channels each), issued by one thread.  Both operands come
+// from shared memory in the K-major, unswizzled canonical layout: 8-row core
+// matrices of 16 bytes per row (128 bytes each), the two 8-channel halves of
+// a K step LBO bytes apart and consecutive 8-row groups SBO = 128 bytes
+// apart.  A CTA is persistent: it stages the whole weight tensor once, then
+// walks its share of 128-point tiles.  Per K step the 128 threads gather
+// their point's 16 channels (two 16-byte loads, zeros outside the grid) into
+// one of kTcStages A buffers; tcgen05.commit arrives on that buffer's
+// mbarrier when the MMA reading it is done, which is what a later step
+// waits for before refilling it.  The epilogue reads D back with
+// tcgen05.ld (warp w owns points 32 w .. 32 w + 31, one per lane).
+//
+// Every wait is bounded (kTcWaitCycles); a wait that runs out sets
+// g_tc_fault, the block stops issuing work, waits (bounded) for what it has
+// in flight, frees its tensor memory and returns.
+constexpr int kTcM = 128;                // points per tile = MMA M
+constexpr int kTcStages = 4;             // A buffers
+constexpr int kTcATile = kTcM * 32;      // bytes of one A buffer (128 x 16 BF16)
+constexpr long long kTcWaitCycles = 4000000000LL;  // about 2 s at 1.9 GHz
+
+__device__ int g_tc_fault;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// shared-memory matrix descriptor: start, LBO, SBO (all >> 4), version 1
+// (bits 46-47), base offset 0, no swizzle (bits 61-63 = 0)
+__device__ __forceinline__ uint64_t tc_sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor of kind::f16: D FP32 (bits 4-5 = 1), A and B BF16
+// (bits 7-9 and 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
+__host__ __device__ constexpr uint32_t tc_idesc(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_st16(uint32_t addr, uint4 v) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v.x), "r"(v.y), "r"(v.z),
+               "r"(v.w)
+               : "memory");
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (true) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > kTcWaitCycles) return false;
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(128) conv3d_fwd_tc_kernel(const bf16* __restrict__ x, Grid4 g,
+                                                            int C, const bf16* __restrict__ w,
+                                                            const float* __restrict__ bias,
+                                                            float* __restrict__ z,
+                                                            bf16* __restrict__ a, int act,
+                                                            float slope) {
+  static_assert(N % 16 == 0 && N >= 16 && N <= 64, "N = 16, 32, 48 or 64");
+  constexpr int NCOLS = N <= 32 ? 32 : 64;  // tensor-memory columns (a power of two >= 32)
+  constexpr uint32_t kIdesc = tc_idesc(kTcM, N);
+  extern __shared__ __align__(128) unsigned char tc_smem[];
+  __shared__ __align__(8) unsigned long long mbar_s[kTcStages];
+  __shared__ uint32_t tmem_s;
+
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int cchunks = C / 16, nks = 27 * cchunks;
+  const uint32_t wbase = smem_addr(tc_smem);
+  const uint32_t abase = wbase + (uint32_t)(nks * N * 32);
+  const uint32_t mbar0 = smem_addr(mbar_s);
+
+  // weights (N, 27, C) -> per K step s = tap * cchunks + chunk: row n, half h
+  // at s * N * 32 + h * (N / 8) * 128 + (n / 8) * 128 + (n % 8) * 16
+  for (int e = tid; e < nks * N * 2; e += blockDim.x) {
+    const int s = e / (N * 2), r = e - s * (N * 2), n = r >> 1, h = r & 1;
+    const int tap = s / cchunks, c0 = (s - tap * cchunks) * 16;
+    const uint4 v =
+        __ldg(reinterpret_cast<const uint4*>(w + ((long long)n * 27 + tap) * C + c0 + 8 * h));
+    tc_st16(wbase + (uint32_t)(s * N * 32 + h * (N / 8) * 128 + (n / 8) * 128 + (n % 8) * 16), v);
+  }
+  if (tid == 0) {
+    for (int b = 0; b < kTcStages; ++b)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar0 + 8 * b) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(&tmem_s)),
+                 "r"(NCOLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_s;
+
+  const long long M = g.npts();
+  const long long ntiles = (M + kTcM - 1) / kTcM;
+  uint32_t step = 0;  // K steps issued by this CTA so far (buffer step % kTcStages)
+  bool failed = false;
+  const uint32_t a_row = (uint32_t)((tid >> 3) * 128 + (tid & 7) * 16);
+  for (long long tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+    const long long m = tile * kTcM + tid;
+    const bool valid = m < M;
+    int pn = 0, pz = 0, py = 0, px = 0;
+    if (valid) decompose(g, m, pn, pz, py, px);
+    auto gather = [&](int s, uint4& v0, uint4& v1) {
+      const int tap = s / cchunks, c0 = (s - tap * cchunks) * 16;
+      v0 = make_uint4(0u, 0u, 0u, 0u);
+      v1 = v0;
+      if (valid) {
+        const long long q =
+            neighbour(g, pn, pz, py, px, tap / 9 - 1, (tap / 3) % 3 - 1, tap % 3 - 1);
+        if (q >= 0) {
+          const uint4* p = reinterpret_cast<const uint4*>(x + q * C + c0);
+          v0 = __ldg(p);
+          v1 = __ldg(p + 1);
+        }
+      }
+    };
+    uint4 v0, v1;
+    gather(0, v0, v1);
+    for (int s = 0; s < nks; ++s, ++step) {
+      uint4 n0 = v0, n1 = v1;
+      if (s + 1 < nks) gather(s + 1, n0, n1);  // the next step's loads overlap this one
+      const uint32_t buf = step % kTcStages;
+      bool bad = false;
+      if (step >= (uint32_t)kTcStages)  // the MMA that last read this buffer is done
+        bad = !tc_wait(mbar0 + 8 * buf, ((step / kTcStages) - 1) & 1);
+      const uint32_t ab = abase + buf * kTcATile;
+      if (!bad) {
+        tc_st16(ab + a_row, v0);
+        tc_st16(ab + 2048 + a_row, v1);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      if (__syncthreads_or(bad)) {
+        failed = true;
+        break;
+      }
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint64_t ad = tc_sdesc(ab, 2048, 128);
+        const uint64_t bd = tc_sdesc(wbase + (uint32_t)(s * N * 32), (N / 8) * 128, 128);
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(kIdesc), "r"(s > 0 ? 1 : 0)
+            : "memory");
+        asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                mbar0 + 8 * buf)
+            : "memory");
+      }
+      v0 = n0;
+      v1 = n1;
+    }
+    if (failed) break;
+    const uint32_t last = step - 1;  // its commit covers every MMA of the tile
+    const bool bad = !tc_wait(mbar0 + 8 * (last % kTcStages), (last / kTcStages) & 1);
+    if (__syncthreads_or(bad)) {
+      failed = true;
+      break;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+    for (int c16 = 0; c16 < N / 16; ++c16) {
+      uint32_t r[16];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c16 * 16);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+          "%11, %12, %13, %14, %15}, [%16];\n"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+            "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+            "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(taddr)
+          : "memory");
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (valid) {
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+          const int k = c16 * 16 + e;
+          const float v = __uint_as_float(r[e]) + (bias ? bias[k] : 0.f);
+          const long long o = m * N + k;
+          if (z) z[o] = v;
+          if (a) a[o] = __float2bfloat16_rn(act ? (v > 0.f ? v : slope * v) : v);
+        }
+      }
+    }
+    // every thread's reads of D are complete before the next tile's first
+    // MMA overwrites it (that MMA is issued after the next step's barrier)
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  }
+  if (failed) {
+    if (tid == 0) atomicExch(&g_tc_fault, 1);
+    // whatever was committed last must finish before the memory is freed
+    if (step > 0) (void)tc_wait(mbar0 + 8 * ((step - 1) % kTcStages), ((step - 1) / kTcStages) & 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOLS)
+                 : "memory");
+  }
+}
+
+template <int N>
+int launch_fwd_tc(const bf16* x, Grid4 g, int C, const bf16* w, const float* bias, float* z,
+                  bf16* a, int act, float slope, cudaStream_t st) {
+  const size_t smem = (size_t)27 * C * N * 2 + (size_t)kTcStages * kTcATile;
+  if (smem > 200 * 1024)
+    return fail(COFFEE_E_INVALID, "tcgen05 convolution: %d x %d weights exceed shared memory", N,
+                C);
+  auto kern = conv3d_fwd_tc_kernel<N>;
+  COFFEE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int dev = 0, sms = 0, per_sm = 0;
+  COFFEE_CUDA_TRY(cudaGetDevice(&dev));
+  COFFEE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  COFFEE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem));
+  // resident CTAs of one SM must fit its 512 tensor-memory columns together,
+  // so that no tcgen05.alloc waits
+  per_sm = std::max(1, std::min(per_sm, 512 / (N <= 32 ? 32 : 64)));
+  const long long ntiles = (g.npts() + kTcM - 1) / kTcM;
+  const unsigned blocks = (unsigned)std::min<long long>(ntiles, (long long)sms * per_sm);
+  kern<<<blocks, 128, smem, st>>>(x, g, C, w, bias, z, a, act, slope);
+  COFFEE_CUDA_TRY(cudaGetLastError());
+  return COFFEE_OK;
+}
+
 }  // namespace
 }  // namespace coffee
 
@@ -455,6 +701,40 @@ extern "C" int coffee_conv3d_forward(const void* x, int n, int d, int h, int w, 
   return fwd_dispatch(static_cast<const bf16*>(x), Grid4{n, d, h, w}, c,
                       static_cast<const bf16*>(weight), k, bias, z, static_cast<bf16*>(a), act,
                       slope, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int coffee_conv3d_forward_tc(const void* x, int n, int d, int h, int w, int c,
+                                        const void* weight, int k, const float* bias, float* z,
+                                        void* a, int act, float slope, void* stream) {
+  clear_error();
+  if (!x || !weight) return fail(COFFEE_E_INVALID, "coffee_conv3d_forward_tc: null argument");
+  if (int rc = check_grid(n, d, h, w)) return rc;
+  if (c <= 0 || c % 16) return fail(COFFEE_E_INVALID, "input channels must be a multiple of 16");
+  if (reinterpret_cast<uintptr_t>(x) % 16 || reinterpret_cast<uintptr_t>(weight) % 16)
+    return fail(COFFEE_E_INVALID, "coffee_conv3d_forward_tc: x and weight must be 16-byte aligned");
+  const Grid4 g{n, d, h, w};
+  const bf16* xb = static_cast<const bf16*>(x);
+  const bf16* wb = static_cast<const bf16*>(weight);
+  bf16* ab = static_cast<bf16*>(a);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  switch (k) {
+    case 16: return launch_fwd_tc<16>(xb, g, c, wb, bias, z, ab, act, slope, st);
+    case 32: return launch_fwd_tc<32>(xb, g, c, wb, bias, z, ab, act, slope, st);
+    case 48: return launch_fwd_tc<48>(xb, g, c, wb, bias, z, ab, act, slope, st);
+    case 64: return launch_fwd_tc<64>(xb, g, c, wb, bias, z, ab, act, slope, st);
+    default: return fail(COFFEE_E_INVALID, "output channels must be 16, 32, 48 or 64 (%d)", k);
+  }
+}
+
+extern "C" int coffee_conv3d_tc_fault(int* fault, int clear) {
+  clear_error();
+  if (!fault) return fail(COFFEE_E_INVALID, "coffee_conv3d_tc_fault: null argument");
+  COFFEE_CUDA_TRY(cudaMemcpyFromSymbol(fault, g_tc_fault, sizeof(int)));
+  if (clear) {
+    const int zero = 0;
+    COFFEE_CUDA_TRY(cudaMemcpyToSymbol(g_tc_fault, &zero, sizeof(int)));
+  }
+  return COFFEE_OK;
 }
 
 extern "C" int coffee_conv3d_flip_weights(const void* weight, int k, int c, void* wt,

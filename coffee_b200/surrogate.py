@@ -61,6 +61,22 @@ def conv_forward(x, w_bf16, bias, k, act, z=None, a=None):
     return z, a
 
 
+def conv_forward_tc(x, w_bf16, bias, k, act, z=None, a=None):
+    """conv_forward on the tcgen05 tensor cores (K = 16, 32, 48 or 64)."""
+    n, d, h, ww, c = x.shape
+    check(_lib.load().coffee_conv3d_forward_tc(_ptr(x), n, d, h, ww, c, _ptr(w_bf16), k,
+                                               _ptr(bias), _ptr(z), _ptr(a), int(act), SLOPE,
+                                               _stream()))
+    return z, a
+
+
+def tc_fault(clear=True):
+    """True if a wait of the tcgen05 convolution ran out of time (results invalid)."""
+    flag = ctypes.c_int(0)
+    check(_lib.load().coffee_conv3d_tc_fault(ctypes.byref(flag), int(clear)))
+    return bool(flag.value)
+
+
 def conv_backward_data(dy, wt_bf16, c, dx):
     n, d, h, w, k = dy.shape
     check(_lib.load().coffee_conv3d_backward_data(_ptr(dy), n, d, h, w, k, _ptr(wt_bf16), c,

@@ -30,6 +30,19 @@ extern "C" {
 COFFEE_API int coffee_conv3d_forward(const void* x, int n, int d, int h, int w, int c,
                                      const void* weight, int k, const float* bias, float* z,
                                      void* a, int act, float slope, void* stream);
+/* The same convolution on the tcgen05 tensor cores (sm_100a): the
+ * accumulator in tensor memory, both operands staged in shared memory, one
+ * persistent CTA per resident slot.  K = 16, 32, 48 or 64; C % 16 == 0 with
+ * 54 K C bytes of weights fitting shared memory (K C <= 3500); x and weight
+ * 16-byte aligned.  Results equal coffee_conv3d_forward's up to the order of
+ * the FP32 additions.  Also the input gradient: call it on dy with the
+ * flipped weights (coffee_conv3d_flip_weights), bias NULL, act 0. */
+COFFEE_API int coffee_conv3d_forward_tc(const void* x, int n, int d, int h, int w, int c,
+                                        const void* weight, int k, const float* bias, float* z,
+                                        void* a, int act, float slope, void* stream);
+/* *fault = 1 if a wait of the tcgen05 kernel ran out of time since the last
+ * clear (its results are then invalid); clear != 0 resets it.  Synchronous. */
+COFFEE_API int coffee_conv3d_tc_fault(int* fault, int clear);
 /* wt (C, 27, K) = w (K, 27, C) with the taps reversed: the weights of the
  * transposed convolution. */
 COFFEE_API int coffee_conv3d_flip_weights(const void* weight, int k, int c, void* wt,

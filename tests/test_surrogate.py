@@ -115,6 +115,48 @@ def test_conv_kernels_match_oracle(c, k):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("c,k,shape", [(16, 16, (2, 6, 5, 7)), (16, 32, (1, 9, 4, 5)),
+                                       (48, 16, (2, 6, 5, 7)), (32, 64, (1, 4, 4, 9)),
+                                       (16, 48, (2, 6, 5, 7)), (32, 32, (2, 24, 40, 40))])
+def test_tcgen05_forward_matches_oracle_and_mma_sync(c, k, shape):
+    """The tcgen05 convolution against the FP64 restatement on the same BF16
+    operands and against the mma.sync kernel; ragged last tiles (420, 180,
+    144 points) and a grid of 600 tiles, more than one per CTA."""
+    from coffee_b200 import surrogate as sg
+    torch = _torch()
+    rng = np.random.default_rng(7 * c + k)
+    x = co.bf16(rng.standard_normal(shape + (c,)))
+    w = co.bf16(rng.standard_normal((k, 27, c)) * 0.2)
+    b = rng.standard_normal(k).astype(np.float32)
+    xt, wt = _bf16_tensor(x), _bf16_tensor(w)
+    bt = torch.from_numpy(b).cuda()
+    sg.tc_fault(clear=True)
+    z = torch.full(shape + (k,), float("nan"), dtype=torch.float32, device="cuda")
+    a = torch.empty(shape + (k,), dtype=torch.bfloat16, device="cuda")
+    sg.conv_forward_tc(xt, wt, bt, k, True, z, a)
+    z_ref = torch.empty_like(z)
+    sg.conv_forward(xt, wt, bt, k, True, z_ref, None)
+    torch.cuda.synchronize()
+    assert not sg.tc_fault()
+    got = _np(z)
+    assert np.isfinite(got).all()
+    assert _rel(got, _np(z_ref)) < 1e-5
+    if np.prod(shape) <= 1000:
+        assert _rel(got, co.conv3d(x, w, b)) < 1e-5
+    assert np.array_equal(_np(a), co.bf16(co.leaky(got)))
+    # the input gradient: the same kernel on dy with the tap-reversed weights
+    if c in (16, 32, 48, 64) and k % 16 == 0 and np.prod(shape) <= 1000:
+        dy = co.bf16(rng.standard_normal(shape + (k,)))
+        wflip = torch.empty((c, 27, k), dtype=torch.bfloat16, device="cuda")
+        sg.flip_weights(wt, wflip)
+        dx = torch.empty(shape + (c,), dtype=torch.float32, device="cuda")
+        sg.conv_forward_tc(_bf16_tensor(dy), wflip, None, c, False, dx, None)
+        torch.cuda.synchronize()
+        assert not sg.tc_fault()
+        assert _rel(_np(dx), co.conv3d_grad_input(dy, w)) < 1e-5
+
+
+@pytest.mark.gpu
 def test_network_gradients_match_oracle():
     """Loss and every layer's gradients of the U-Net on the library's kernels
     against the FP64 restatement with the same BF16 rounding points."""
