@@ -10,6 +10,7 @@
 // its B fragments are 16 channels x 8 output channels of that tap's
 // weights.  The network is small (16-48 channels), so the kernels are
 // bound by these gathers through L1, not by the tensor pipe.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -442,27 +443,35 @@ int check_grid(int n, int d, int h, int w) {
 
 // ------------------------------------------- forward on tcgen05 (sm_100a)
 // The same "same" 3x3x3 convolution as conv3d_fwd_kernel on the fifth-
-// generation tensor cores: D (128 points x N output channels, FP32) lives in
-// tensor memory and is built by 27 C / 16 tcgen05.mma steps of K = 16 (one
-// tap, 16 input channels each), issued by one thread.  Both operands come
-// from shared memory in the K-major, unswizzled canonical layout: 8-row core
-// matrices of 16 bytes per row (128 bytes each), the two 8-channel halves of
-// a K step LBO bytes apart and consecutive 8-row groups SBO = 128 bytes
-// apart.  A CTA is persistent: it stages the whole weight tensor once, then
-// walks its share of 128-point tiles.  Per K step the 128 threads gather
-// their point's 16 channels (two 16-byte loads, zeros outside the grid) into
-// one of kTcStages A buffers; tcgen05.commit arrives on that buffer's
-// mbarrier when the MMA reading it is done, which is what a later step
-// waits for before refilling it.  The epilogue reads D back with
-// tcgen05.ld (warp w owns points 32 w .. 32 w + 31, one per lane).
+// generation tensor cores, as an implicit GEMM whose A operand is fetched by
+// the tensor memory accelerator:
 //
-// Every wait is bounded (kTcWaitCycles); a wait that runs out sets
-// g_tc_fault, the block stops issuing work, waits (bounded) for what it has
-// in flight, frees its tensor memory and returns.
-constexpr int kTcM = 128;                // points per tile = MMA M
-constexpr int kTcStages = 4;             // A buffers
-constexpr int kTcATile = kTcM * 32;      // bytes of one A buffer (128 x 16 BF16)
-constexpr long long kTcWaitCycles = 4000000000LL;  // about 2 s at 1.9 GHz
+//   * A tile is a box of BX x BY x BZ = 128 points of one sample.  For each
+//     K step (one tap, 16 input channels) one thread issues a 5D TMA load of
+//     the box shifted by the tap's offset, {c0, x0 + dx, y0 + dy, z0 + dz, n};
+//     the TMA unit writes zeros where the shifted box leaves the grid (the
+//     convolution's padding) and lays the 128 rows of 32 bytes out with the
+//     32-byte swizzle that the MMA's K-major SWIZZLE_32B descriptor reads.
+//   * The weights (N, 27, C) are staged once per persistent CTA in the
+//     unswizzled K-major layout: 8-row core matrices of 16-byte rows, the two
+//     8-channel halves of a K step LBO bytes apart, 8-row groups 128 apart.
+//   * Warp 4 produces (TMA into a kTcStages-deep ring, "full" mbarriers with
+//     the expected byte count), warp 5 issues tcgen05.mma (M 128, N, K 16,
+//     BF16 in, FP32 accumulate) and commits each step to the ring slot's
+//     "empty" mbarrier and each tile to its accumulator's "ready" mbarrier;
+//     warps 0-3 read the accumulator back with tcgen05.ld (warp w owns rows
+//     32 w .. 32 w + 31) and store.  Two accumulators in tensor memory let
+//     the epilogue of one tile overlap the MMAs of the next.
+//
+// Every wait is bounded (kTcWaitCycles) and also ends when another role of
+// the CTA has given up: a wait that runs out sets g_tc_fault, the roles stop
+// issuing work, the MMA thread waits (bounded) for what it committed, and
+// the CTA frees its tensor memory and returns.
+constexpr int kTcM = 128;                         // points per tile = MMA M
+constexpr int kTcStages = 8;                      // A ring slots
+constexpr int kTcATile = kTcM * 32;               // bytes of one A slot (128 x 16 BF16)
+constexpr int kTcThreads = 192;                   // 4 epilogue warps, producer, MMA
+constexpr long long kTcWaitCycles = 4000000000LL; // about 2 s at 1.9 GHz
 
 __device__ int g_tc_fault;
 
@@ -471,10 +480,11 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) {
 }
 
 // shared-memory matrix descriptor: start, LBO, SBO (all >> 4), version 1
-// (bits 46-47), base offset 0, no swizzle (bits 61-63 = 0)
-__device__ __forceinline__ uint64_t tc_sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+// (bits 46-47), base offset 0, layout type at bits 61-63 (0 none, 6 32B swizzle)
+__device__ __forceinline__ uint64_t tc_sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo,
+                                             uint32_t layout) {
   return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) | ((uint64_t)layout << 61);
 }
 
 // instruction descriptor of kind::f16: D FP32 (bits 4-5 = 1), A and B BF16
@@ -490,7 +500,9 @@ __device__ __forceinline__ void tc_st16(uint32_t addr, uint4 v) {
                : "memory");
 }
 
-__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
+// Wait for the phase of parity `parity` of the mbarrier at `mbar`; false if
+// it did not complete within kTcWaitCycles or another role gave up (*abort).
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity, volatile int* abort) {
   const long long t0 = clock64();
   while (true) {
     uint32_t done;
@@ -501,32 +513,44 @@ __device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity) {
         : "r"(mbar), "r"(parity)
         : "memory");
     if (done) return true;
-    if (clock64() - t0 > kTcWaitCycles) return false;
+    if (*abort) return false;
+    if (clock64() - t0 > kTcWaitCycles) {
+      *abort = 1;
+      atomicExch(&g_tc_fault, 1);
+      return false;
+    }
   }
 }
 
+struct TcBox {
+  int bx, by, bz;     // box extent (bx * by * bz = 128)
+  int tx, ty, tz;     // boxes per sample along x, y, z
+};
+
 template <int N>
-__global__ void __launch_bounds__(128) conv3d_fwd_tc_kernel(const bf16* __restrict__ x, Grid4 g,
-                                                            int C, const bf16* __restrict__ w,
-                                                            const float* __restrict__ bias,
-                                                            float* __restrict__ z,
-                                                            bf16* __restrict__ a, int act,
-                                                            float slope) {
+__global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
+    const __grid_constant__ CUtensorMap xmap, Grid4 g, int C, const bf16* __restrict__ w,
+    const float* __restrict__ bias, float* __restrict__ z, bf16* __restrict__ a, int act,
+    float slope, TcBox box) {
   static_assert(N % 16 == 0 && N >= 16 && N <= 64, "N = 16, 32, 48 or 64");
-  constexpr int NCOLS = N <= 32 ? 32 : 64;  // tensor-memory columns (a power of two >= 32)
+  constexpr int NCOLS = N <= 32 ? 32 : 64;  // columns of one accumulator (power of two >= 32)
   constexpr uint32_t kIdesc = tc_idesc(kTcM, N);
-  extern __shared__ __align__(128) unsigned char tc_smem[];
-  __shared__ __align__(8) unsigned long long mbar_s[kTcStages];
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  __shared__ __align__(8) unsigned long long full_s[kTcStages], empty_s[kTcStages];
+  __shared__ __align__(8) unsigned long long ready_s[2], free_s[2];
   __shared__ uint32_t tmem_s;
+  __shared__ int abort_s;
 
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int cchunks = C / 16, nks = 27 * cchunks;
-  const uint32_t wbase = smem_addr(tc_smem);
-  const uint32_t abase = wbase + (uint32_t)(nks * N * 32);
-  const uint32_t mbar0 = smem_addr(mbar_s);
+  // A ring at the first 1024-byte boundary (the swizzle atoms repeat every
+  // 256 bytes), the weights after it
+  const uint32_t abase = (smem_addr(tc_smem) + 1023u) & ~1023u;
+  const uint32_t wbase = abase + (uint32_t)(kTcStages * kTcATile);
+  const uint32_t full0 = smem_addr(full_s), empty0 = smem_addr(empty_s);
+  const uint32_t ready0 = smem_addr(ready_s), free0 = smem_addr(free_s);
+  volatile int* abort = &abort_s;
 
-  // weights (N, 27, C) -> per K step s = tap * cchunks + chunk: row n, half h
-  // at s * N * 32 + h * (N / 8) * 128 + (n / 8) * 128 + (n % 8) * 16
   for (int e = tid; e < nks * N * 2; e += blockDim.x) {
     const int s = e / (N * 2), r = e - s * (N * 2), n = r >> 1, h = r & 1;
     const int tap = s / cchunks, c0 = (s - tap * cchunks) * 16;
@@ -535,14 +559,21 @@ __global__ void __launch_bounds__(128) conv3d_fwd_tc_kernel(const bf16* __restri
     tc_st16(wbase + (uint32_t)(s * N * 32 + h * (N / 8) * 128 + (n / 8) * 128 + (n % 8) * 16), v);
   }
   if (tid == 0) {
-    for (int b = 0; b < kTcStages; ++b)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar0 + 8 * b) : "memory");
+    abort_s = 0;
+    for (int b = 0; b < kTcStages; ++b) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full0 + 8 * b) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(empty0 + 8 * b) : "memory");
+    }
+    for (int b = 0; b < 2; ++b) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(ready0 + 8 * b) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(free0 + 8 * b) : "memory");
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_addr(&tmem_s)),
-                 "r"(NCOLS)
+                 "r"(2 * NCOLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -552,136 +583,248 @@ __global__ void __launch_bounds__(128) conv3d_fwd_tc_kernel(const bf16* __restri
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_s;
 
-  const long long M = g.npts();
-  const long long ntiles = (M + kTcM - 1) / kTcM;
-  uint32_t step = 0;  // K steps issued by this CTA so far (buffer step % kTcStages)
-  bool failed = false;
-  const uint32_t a_row = (uint32_t)((tid >> 3) * 128 + (tid & 7) * 16);
-  for (long long tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
-    const long long m = tile * kTcM + tid;
-    const bool valid = m < M;
-    int pn = 0, pz = 0, py = 0, px = 0;
-    if (valid) decompose(g, m, pn, pz, py, px);
-    auto gather = [&](int s, uint4& v0, uint4& v1) {
-      const int tap = s / cchunks, c0 = (s - tap * cchunks) * 16;
-      v0 = make_uint4(0u, 0u, 0u, 0u);
-      v1 = v0;
-      if (valid) {
-        const long long q =
-            neighbour(g, pn, pz, py, px, tap / 9 - 1, (tap / 3) % 3 - 1, tap % 3 - 1);
-        if (q >= 0) {
-          const uint4* p = reinterpret_cast<const uint4*>(x + q * C + c0);
-          v0 = __ldg(p);
-          v1 = __ldg(p + 1);
+  const long long per_n = (long long)box.tx * box.ty * box.tz;
+  const long long ntiles = (long long)g.n * per_n;
+  auto tile_origin = [&](long long t, int& n, int& x0, int& y0, int& z0) {
+    n = (int)(t / per_n);
+    long long r = t - (long long)n * per_n;
+    z0 = (int)(r / ((long long)box.tx * box.ty)) * box.bz;
+    r %= (long long)box.tx * box.ty;
+    y0 = (int)(r / box.tx) * box.by;
+    x0 = (int)(r % box.tx) * box.bx;
+  };
+
+  if (warp == 4) {
+    // ---- producer: one TMA load per K step into the ring
+    if (lane == 0) {
+      uint32_t step = 0;
+      const uint64_t map = reinterpret_cast<uint64_t>(&xmap);
+      for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        int n, x0, y0, z0;
+        tile_origin(t, n, x0, y0, z0);
+        bool ok = true;
+        for (int s = 0; s < nks && ok; ++s, ++step) {
+          const uint32_t b = step % kTcStages;
+          if (step >= (uint32_t)kTcStages && !tc_wait(empty0 + 8 * b, ((step / kTcStages) - 1) & 1, abort)) {
+            ok = false;
+            break;
+          }
+          const int tap = s / cchunks, c0 = (s - tap * cchunks) * 16;
+          const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full0 + 8 * b),
+                       "r"(kTcATile)
+                       : "memory");
+          asm volatile(
+              "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+              "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(abase + b * kTcATile),
+              "l"(map), "r"(c0), "r"(x0 + dx), "r"(y0 + dy), "r"(z0 + dz), "r"(n),
+              "r"(full0 + 8 * b)
+              : "memory");
+        }
+        if (!ok) break;
+      }
+      if (*abort && step > 0) {
+        // the loads already issued must land before the CTA's memory goes away
+        const uint32_t last = step - 1;
+        const long long t0 = clock64();
+        while (clock64() - t0 < kTcWaitCycles) {
+          uint32_t done;
+          asm volatile(
+              "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+              " selp.u32 %0, 1, 0, p;\n}\n"
+              : "=r"(done)
+              : "r"(full0 + 8 * (last % kTcStages)), "r"((last / kTcStages) & 1)
+              : "memory");
+          if (done) break;
         }
       }
-    };
-    uint4 v0, v1;
-    gather(0, v0, v1);
-    for (int s = 0; s < nks; ++s, ++step) {
-      uint4 n0 = v0, n1 = v1;
-      if (s + 1 < nks) gather(s + 1, n0, n1);  // the next step's loads overlap this one
-      const uint32_t buf = step % kTcStages;
-      bool bad = false;
-      if (step >= (uint32_t)kTcStages)  // the MMA that last read this buffer is done
-        bad = !tc_wait(mbar0 + 8 * buf, ((step / kTcStages) - 1) & 1);
-      const uint32_t ab = abase + buf * kTcATile;
-      if (!bad) {
-        tc_st16(ab + a_row, v0);
-        tc_st16(ab + 2048 + a_row, v1);
-      }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      if (__syncthreads_or(bad)) {
-        failed = true;
-        break;
-      }
-      if (tid == 0) {
+    }
+  } else if (warp == 5) {
+    // ---- MMA issuer
+    if (lane == 0) {
+      uint32_t step = 0, tiles = 0;
+      bool ok = true;
+      for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++tiles) {
+        const uint32_t acc = tiles & 1, use = tiles >> 1;
+        if (tiles >= 2 && !tc_wait(free0 + 8 * acc, (use - 1) & 1, abort)) {
+          ok = false;
+          break;
+        }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint64_t ad = tc_sdesc(ab, 2048, 128);
-        const uint64_t bd = tc_sdesc(wbase + (uint32_t)(s * N * 32), (N / 8) * 128, 128);
-        asm volatile(
-            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-            "l"(ad), "l"(bd), "r"(kIdesc), "r"(s > 0 ? 1 : 0)
-            : "memory");
+        const uint32_t d = tmem + acc * NCOLS;
+        for (int s = 0; s < nks; ++s, ++step) {
+          const uint32_t b = step % kTcStages;
+          if (!tc_wait(full0 + 8 * b, (step / kTcStages) & 1, abort)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint64_t ad = tc_sdesc(abase + b * kTcATile, 16, 256, 6);
+          const uint64_t bd = tc_sdesc(wbase + (uint32_t)(s * N * 32), (N / 8) * 128, 128, 0);
+          asm volatile(
+              "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+              "l"(ad), "l"(bd), "r"(kIdesc), "r"(s > 0 ? 1 : 0)
+              : "memory");
+          asm volatile(
+              "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                  empty0 + 8 * b)
+              : "memory");
+        }
+        if (!ok) break;
         asm volatile(
             "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                mbar0 + 8 * buf)
+                ready0 + 8 * acc)
             : "memory");
       }
-      v0 = n0;
-      v1 = n1;
-    }
-    if (failed) break;
-    const uint32_t last = step - 1;  // its commit covers every MMA of the tile
-    const bool bad = !tc_wait(mbar0 + 8 * (last % kTcStages), (last / kTcStages) & 1);
-    if (__syncthreads_or(bad)) {
-      failed = true;
-      break;
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-    for (int c16 = 0; c16 < N / 16; ++c16) {
-      uint32_t r[16];
-      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c16 * 16);
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-          "%11, %12, %13, %14, %15}, [%16];\n"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-            "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-            "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-          : "r"(taddr)
-          : "memory");
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (valid) {
-#pragma unroll
-        for (int e = 0; e < 16; ++e) {
-          const int k = c16 * 16 + e;
-          const float v = __uint_as_float(r[e]) + (bias ? bias[k] : 0.f);
-          const long long o = m * N + k;
-          if (z) z[o] = v;
-          if (a) a[o] = __float2bfloat16_rn(act ? (v > 0.f ? v : slope * v) : v);
+      if (!ok && step > 0) {
+        // what was committed must finish before the tensor memory is freed
+        const uint32_t last = step - 1;
+        const long long t0 = clock64();
+        while (clock64() - t0 < kTcWaitCycles) {
+          uint32_t done;
+          asm volatile(
+              "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+              " selp.u32 %0, 1, 0, p;\n}\n"
+              : "=r"(done)
+              : "r"(empty0 + 8 * (last % kTcStages)), "r"((last / kTcStages) & 1)
+              : "memory");
+          if (done) break;
         }
       }
     }
-    // every thread's reads of D are complete before the next tile's first
-    // MMA overwrites it (that MMA is issued after the next step's barrier)
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  }
-  if (failed) {
-    if (tid == 0) atomicExch(&g_tc_fault, 1);
-    // whatever was committed last must finish before the memory is freed
-    if (step > 0) (void)tc_wait(mbar0 + 8 * ((step - 1) % kTcStages), ((step - 1) / kTcStages) & 1);
+  } else {
+    // ---- epilogue: warps 0-3, row r = tid of the tile's box
+    const int bx = tid % box.bx, by = (tid / box.bx) % box.by, bz = tid / (box.bx * box.by);
+    uint32_t tiles = 0;
+    for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, ++tiles) {
+      const uint32_t acc = tiles & 1;
+      if (!tc_wait(ready0 + 8 * acc, (tiles >> 1) & 1, abort)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      uint32_t r[N];
+#pragma unroll
+      for (int c16 = 0; c16 < N / 16; ++c16) {
+        const uint32_t taddr =
+            tmem + ((uint32_t)(warp * 32) << 16) + acc * NCOLS + (uint32_t)(c16 * 16);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
+            "%10, %11, %12, %13, %14, %15}, [%16];\n"
+            : "=r"(r[c16 * 16 + 0]), "=r"(r[c16 * 16 + 1]), "=r"(r[c16 * 16 + 2]),
+              "=r"(r[c16 * 16 + 3]), "=r"(r[c16 * 16 + 4]), "=r"(r[c16 * 16 + 5]),
+              "=r"(r[c16 * 16 + 6]), "=r"(r[c16 * 16 + 7]), "=r"(r[c16 * 16 + 8]),
+              "=r"(r[c16 * 16 + 9]), "=r"(r[c16 * 16 + 10]), "=r"(r[c16 * 16 + 11]),
+              "=r"(r[c16 * 16 + 12]), "=r"(r[c16 * 16 + 13]), "=r"(r[c16 * 16 + 14]),
+              "=r"(r[c16 * 16 + 15])
+            : "r"(taddr)
+            : "memory");
+      }
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(free0 + 8 * acc) : "memory");
+      int n, x0, y0, z0;
+      tile_origin(t, n, x0, y0, z0);
+      const int px = x0 + bx, py = y0 + by, pz = z0 + bz;
+      if (px < g.w && py < g.h && pz < g.d) {
+        const long long m = (((long long)n * g.d + pz) * g.h + py) * g.w + px;
+#pragma unroll
+        for (int k4 = 0; k4 < N; k4 += 4) {
+          float v[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) v[e] = __uint_as_float(r[k4 + e]) + (bias ? bias[k4 + e] : 0.f);
+          if (z) *reinterpret_cast<float4*>(z + m * N + k4) = make_float4(v[0], v[1], v[2], v[3]);
+          if (a) {
+            __nv_bfloat162 lo, hi;
+            lo.x = __float2bfloat16_rn(act ? (v[0] > 0.f ? v[0] : slope * v[0]) : v[0]);
+            lo.y = __float2bfloat16_rn(act ? (v[1] > 0.f ? v[1] : slope * v[1]) : v[1]);
+            hi.x = __float2bfloat16_rn(act ? (v[2] > 0.f ? v[2] : slope * v[2]) : v[2]);
+            hi.y = __float2bfloat16_rn(act ? (v[3] > 0.f ? v[3] : slope * v[3]) : v[3]);
+            uint2 pk;
+            pk.x = *reinterpret_cast<uint32_t*>(&lo);
+            pk.y = *reinterpret_cast<uint32_t*>(&hi);
+            *reinterpret_cast<uint2*>(a + m * N + k4) = pk;
+          }
+        }
+      }
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOLS)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(2 * NCOLS)
                  : "memory");
   }
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int encode_fn(EncodeTiledFn* fn) {
+  static EncodeTiledFn cached = nullptr;
+  if (!cached) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    const cudaError_t err = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+    if (err != cudaSuccess || q != cudaDriverEntryPointSuccess || !p)
+      return fail(COFFEE_E_CUDA, "cuTensorMapEncodeTiled is not available");
+    cached = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  *fn = cached;
+  return COFFEE_OK;
+}
+
+int pow2_at_least(int v) {
+  int p = 1;
+  while (p < v) p <<= 1;
+  return p;
 }
 
 template <int N>
 int launch_fwd_tc(const bf16* x, Grid4 g, int C, const bf16* w, const float* bias, float* z,
                   bf16* a, int act, float slope, cudaStream_t st) {
-  const size_t smem = (size_t)27 * C * N * 2 + (size_t)kTcStages * kTcATile;
+  const size_t smem = 1024 + (size_t)kTcStages * kTcATile + (size_t)27 * C * N * 2;
   if (smem > 200 * 1024)
     return fail(COFFEE_E_INVALID, "tcgen05 convolution: %d x %d weights exceed shared memory", N,
                 C);
+  // the box: x extent a power of two in [8, 128], then y, then z
+  TcBox box;
+  box.bx = std::min(128, std::max(8, pow2_at_least(g.w)));
+  box.by = std::min(128 / box.bx, pow2_at_least(g.h));
+  box.bz = 128 / (box.bx * box.by);
+  box.tx = (g.w + box.bx - 1) / box.bx;
+  box.ty = (g.h + box.by - 1) / box.by;
+  box.tz = (g.d + box.bz - 1) / box.bz;
+  if (box.bz > 256) return fail(COFFEE_E_INVALID, "tcgen05 convolution: box too deep");
+  EncodeTiledFn enc;
+  if (int rc = encode_fn(&enc)) return rc;
+  CUtensorMap map;
+  const cuuint64_t dims[5] = {(cuuint64_t)C, (cuuint64_t)g.w, (cuuint64_t)g.h, (cuuint64_t)g.d,
+                              (cuuint64_t)g.n};
+  const cuuint64_t strides[4] = {(cuuint64_t)C * 2, (cuuint64_t)C * 2 * g.w,
+                                 (cuuint64_t)C * 2 * g.w * g.h, (cuuint64_t)C * 2 * g.w * g.h * g.d};
+  const cuuint32_t boxdim[5] = {16, (cuuint32_t)box.bx, (cuuint32_t)box.by, (cuuint32_t)box.bz, 1};
+  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  const CUresult cr = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16*>(x), dims,
+                          strides, boxdim, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (cr != CUDA_SUCCESS)
+    return fail(COFFEE_E_INVALID, "tcgen05 convolution: tensor map rejected (%d)", (int)cr);
   auto kern = conv3d_fwd_tc_kernel<N>;
   COFFEE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev = 0, sms = 0, per_sm = 0;
   COFFEE_CUDA_TRY(cudaGetDevice(&dev));
   COFFEE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  COFFEE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem));
-  // resident CTAs of one SM must fit its 512 tensor-memory columns together,
-  // so that no tcgen05.alloc waits
-  per_sm = std::max(1, std::min(per_sm, 512 / (N <= 32 ? 32 : 64)));
-  const long long ntiles = (g.npts() + kTcM - 1) / kTcM;
+  COFFEE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTcThreads, smem));
+  // the resident CTAs of one SM must fit its 512 tensor-memory columns
+  // together, so that no tcgen05.alloc waits
+  per_sm = std::max(1, std::min(per_sm, 512 / (2 * (N <= 32 ? 32 : 64))));
+  const long long ntiles = (long long)g.n * box.tx * box.ty * box.tz;
   const unsigned blocks = (unsigned)std::min<long long>(ntiles, (long long)sms * per_sm);
-  kern<<<blocks, 128, smem, st>>>(x, g, C, w, bias, z, a, act, slope);
+  kern<<<blocks, kTcThreads, smem, st>>>(map, g, C, w, bias, z, a, act, slope, box);
   COFFEE_CUDA_TRY(cudaGetLastError());
   return COFFEE_OK;
 }
@@ -712,6 +855,8 @@ extern "C" int coffee_conv3d_forward_tc(const void* x, int n, int d, int h, int 
   if (c <= 0 || c % 16) return fail(COFFEE_E_INVALID, "input channels must be a multiple of 16");
   if (reinterpret_cast<uintptr_t>(x) % 16 || reinterpret_cast<uintptr_t>(weight) % 16)
     return fail(COFFEE_E_INVALID, "coffee_conv3d_forward_tc: x and weight must be 16-byte aligned");
+  if (reinterpret_cast<uintptr_t>(z) % 16 || reinterpret_cast<uintptr_t>(a) % 8)
+    return fail(COFFEE_E_INVALID, "coffee_conv3d_forward_tc: z must be 16-byte, a 8-byte aligned");
   const Grid4 g{n, d, h, w};
   const bf16* xb = static_cast<const bf16*>(x);
   const bf16* wb = static_cast<const bf16*>(weight);

@@ -30,8 +30,9 @@ extern "C" {
 COFFEE_API int coffee_conv3d_forward(const void* x, int n, int d, int h, int w, int c,
                                      const void* weight, int k, const float* bias, float* z,
                                      void* a, int act, float slope, void* stream);
-/* The same convolution on the tcgen05 tensor cores (sm_100a): the
- * accumulator in tensor memory, both operands staged in shared memory, one
+/* The same convolution on the tcgen05 tensor cores (sm_100a): A fetched by
+ * TMA (one shifted box per tap, zero fill at the edges), weights staged once
+ * per CTA, the accumulator in tensor memory (two, so the epilogue overlaps), one
  * persistent CTA per resident slot.  K = 16, 32, 48 or 64; C % 16 == 0 with
  * 54 K C bytes of weights fitting shared memory (K C <= 3500); x and weight
  * 16-byte aligned.  Results equal coffee_conv3d_forward's up to the order of
