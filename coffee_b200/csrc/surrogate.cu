@@ -815,6 +815,10 @@ int launch_fwd_tc(const bf16* x, Grid4 g, int C, const bf16* w, const float* bia
     return fail(COFFEE_E_INVALID, "tcgen05 convolution: tensor map rejected (%d)", (int)cr);
   auto kern = conv3d_fwd_tc_kernel<N>;
   COFFEE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // all of the unified L1 / shared memory as shared memory, so that the
+  // occupancy below counts every CTA that fits
+  COFFEE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared));
   int dev = 0, sms = 0, per_sm = 0;
   COFFEE_CUDA_TRY(cudaGetDevice(&dev));
   COFFEE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
