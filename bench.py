@@ -728,21 +728,22 @@ def run_surrogate(args):
     clk = clocks.stop(w0, time.time())
     ms = e0.elapsed_time(e1) / args.steps
     vox = n * side ** 3
-    # the largest convolution alone: layer 5, 48 -> 16 channels at full size
-    L = net.layers[4]
-    cat = net._saved["cat"]
-    z = torch.empty(cat.shape[:4] + (L.cout,), dtype=torch.float32, device=dev)
-    a = torch.empty(cat.shape[:4] + (L.cout,), dtype=torch.bfloat16, device=dev)
-    for _ in range(3):
-        sg.conv_forward(cat, L.wb, L.b, L.cout, True, z, a)
-    e0.record(stream)
-    reps = 10
-    for _ in range(reps):
-        sg.conv_forward(cat, L.wb, L.b, L.cout, True, z, a)
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    conv_ms = e0.elapsed_time(e1) / reps
-    flops = 2.0 * 27 * L.cin * L.cout * vox
+    def conv_time(fn, L, xin):
+        z = torch.empty(xin.shape[:4] + (L.cout,), dtype=torch.float32, device=dev)
+        a = torch.empty(xin.shape[:4] + (L.cout,), dtype=torch.bfloat16, device=dev)
+        for _ in range(3):
+            fn(xin, L.wb, L.b, L.cout, True, z, a)
+        e0.record(stream)
+        for _ in range(10):
+            fn(xin, L.wb, L.b, L.cout, True, z, a)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / 10, 2.0 * 27 * L.cin * L.cout * xin[..., 0].numel()
+
+    # the tcgen05 convolution of layer 4 (32 -> 32 channels, 32^3 x 8), and
+    # the largest one, layer 5 (48 -> 16 channels at full size, mma.sync)
+    conv_ms, flops = conv_time(sg.conv_forward_tc, net.layers[3], net._saved["a3"])
+    mma_ms, mma_flops = conv_time(sg.conv_forward, net.layers[4], net._saved["cat"])
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             peak, kind = float(json.load(f)["bf16_tflops"]), "measured"
@@ -756,10 +757,12 @@ def run_surrogate(args):
             "config": {"workload": "surrogate-unet64", "samples": n, "grid": [side] * 3,
                        "channels": [sg.CIN, sg.C1, sg.C2, sg.COUT],
                        "step": "forward + masked MSE + backward + Adam, all on the library's kernels"},
-            "roofline": {"kernel": "conv3d_fwd_kernel (48 -> 16 channels, 64^3 x 8)",
+            "roofline": {"kernel": "conv3d_fwd_tc_kernel (tcgen05 + TMA, 32 -> 32 channels, "
+                                   "32^3 x 8)",
                          "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "peak_kind": kind, "frac": achieved / peak, "traffic": None,
                          "avg_launch_ms": conv_ms, "flops_per_launch": flops},
+            "conv_48_16_mma_sync": {"ms": mma_ms, "tflops": mma_flops / (mma_ms / 1e3) / 1e12},
             "gpu_launches": None, "clocks": clk}
     if args.study:
         line["warm_start_study"] = sg.warm_start_study()

@@ -447,11 +447,13 @@ int check_grid(int n, int d, int h, int w) {
 // the tensor memory accelerator:
 //
 //   * A tile is a box of BX x BY x BZ = 128 points of one sample.  For each
-//     K step (one tap, 16 input channels) one thread issues a 5D TMA load of
-//     the box shifted by the tap's offset, {c0, x0 + dx, y0 + dy, z0 + dz, n};
-//     the TMA unit writes zeros where the shifted box leaves the grid (the
-//     convolution's padding) and lays the 128 rows of 32 bytes out with the
-//     32-byte swizzle that the MMA's K-major SWIZZLE_32B descriptor reads.
+//     stage (one tap, cb = 16, 32 or 64 input channels, the widest that
+//     divides C) one thread issues a 5D TMA load of the box shifted by the
+//     tap's offset, {c0, x0 + dx, y0 + dy, z0 + dz, n}; the TMA unit writes
+//     zeros where the shifted box leaves the grid (the convolution's padding)
+//     and lays the 128 rows of 2 cb bytes out with the swizzle of that width,
+//     which the MMA's K-major SWIZZLE_32B / 64B / 128B descriptor reads; the
+//     stage's cb / 16 MMAs (K 16 each) start 32 bytes apart along the rows.
 //   * The weights (N, 27, C) are staged once per persistent CTA in the
 //     unswizzled K-major layout: 8-row core matrices of 16-byte rows, the two
 //     8-channel halves of a K step LBO bytes apart, 8-row groups 128 apart.
@@ -468,8 +470,8 @@ int check_grid(int n, int d, int h, int w) {
 // issuing work, the MMA thread waits (bounded) for what it committed, and
 // the CTA frees its tensor memory and returns.
 constexpr int kTcM = 128;                         // points per tile = MMA M
-constexpr int kTcStages = 8;                      // A ring slots
-constexpr int kTcATile = kTcM * 32;               // bytes of one A slot (128 x 16 BF16)
+constexpr int kTcStages = 8;                      // A ring slots at most (32 KB of ring)
+constexpr int kTcRing = 32768;                    // bytes of the A ring
 constexpr int kTcThreads = 192;                   // 4 epilogue warps, producer, MMA
 constexpr long long kTcWaitCycles = 4000000000LL; // about 2 s at 1.9 GHz
 
@@ -527,12 +529,13 @@ struct TcBox {
   int tx, ty, tz;     // boxes per sample along x, y, z
 };
 
-template <int N>
+template <int N, int CB>
 __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
     const __grid_constant__ CUtensorMap xmap, Grid4 g, int C, const bf16* __restrict__ w,
     const float* __restrict__ bias, float* __restrict__ z, bf16* __restrict__ a, int act,
     float slope, TcBox box) {
   static_assert(N % 16 == 0 && N >= 16 && N <= 64, "N = 16, 32, 48 or 64");
+  static_assert(CB == 16 || CB == 32 || CB == 64, "boxes of 16, 32 or 64 channels");
   constexpr int NCOLS = N <= 32 ? 32 : 64;  // columns of one accumulator (power of two >= 32)
   constexpr uint32_t kIdesc = tc_idesc(kTcM, N);
   extern __shared__ __align__(1024) unsigned char tc_smem[];
@@ -543,10 +546,17 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int cchunks = C / 16, nks = 27 * cchunks;
+  // A stage: one box of cb channels (16, 32 or 64: rows of 32, 64 or 128
+  // bytes under the swizzle of that width), cb / 16 MMAs
+  constexpr int sub = CB / 16;
+  constexpr uint32_t slot = (uint32_t)(kTcM * CB * 2);
+  constexpr uint32_t stages = (uint32_t)(kTcRing / (kTcM * CB * 2));
+  constexpr uint32_t layout = CB == 16 ? 6u : (CB == 32 ? 4u : 2u);  // 32B / 64B / 128B swizzle
+  const int bchunks = C / CB, nstage = 27 * bchunks;
   // A ring at the first 1024-byte boundary (the swizzle atoms repeat every
-  // 256 bytes), the weights after it
+  // 256 to 1024 bytes), the weights after it
   const uint32_t abase = (smem_addr(tc_smem) + 1023u) & ~1023u;
-  const uint32_t wbase = abase + (uint32_t)(kTcStages * kTcATile);
+  const uint32_t wbase = abase + (uint32_t)kTcRing;
   const uint32_t full0 = smem_addr(full_s), empty0 = smem_addr(empty_s);
   const uint32_t ready0 = smem_addr(ready_s), free0 = smem_addr(free_s);
   volatile int* abort = &abort_s;
@@ -603,23 +613,28 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
         int n, x0, y0, z0;
         tile_origin(t, n, x0, y0, z0);
         bool ok = true;
-        for (int s = 0; s < nks && ok; ++s, ++step) {
-          const uint32_t b = step % kTcStages;
-          if (step >= (uint32_t)kTcStages && !tc_wait(empty0 + 8 * b, ((step / kTcStages) - 1) & 1, abort)) {
+        int tap = 0, q = 0;
+        for (int s = 0; s < nstage && ok; ++s, ++step) {
+          const uint32_t b = step % stages;
+          if (step >= stages && !tc_wait(empty0 + 8 * b, ((step / stages) - 1) & 1, abort)) {
             ok = false;
             break;
           }
-          const int tap = s / cchunks, c0 = (s - tap * cchunks) * 16;
+          const int c0 = q * CB;
           const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
           asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full0 + 8 * b),
-                       "r"(kTcATile)
+                       "r"(slot)
                        : "memory");
           asm volatile(
               "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
-              "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(abase + b * kTcATile),
+              "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(abase + b * slot),
               "l"(map), "r"(c0), "r"(x0 + dx), "r"(y0 + dy), "r"(z0 + dz), "r"(n),
               "r"(full0 + 8 * b)
               : "memory");
+          if (++q == bchunks) {
+            q = 0;
+            ++tap;
+          }
         }
         if (!ok) break;
       }
@@ -633,7 +648,7 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
               "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
               " selp.u32 %0, 1, 0, p;\n}\n"
               : "=r"(done)
-              : "r"(full0 + 8 * (last % kTcStages)), "r"((last / kTcStages) & 1)
+              : "r"(full0 + 8 * (last % stages)), "r"((last / stages) & 1)
               : "memory");
           if (done) break;
         }
@@ -652,20 +667,25 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t d = tmem + acc * NCOLS;
-        for (int s = 0; s < nks; ++s, ++step) {
-          const uint32_t b = step % kTcStages;
-          if (!tc_wait(full0 + 8 * b, (step / kTcStages) & 1, abort)) {
+        int s16 = 0;  // 16-channel K step of the stage's first MMA
+        for (int s = 0; s < nstage; ++s, ++step) {
+          const uint32_t b = step % stages;
+          if (!tc_wait(full0 + 8 * b, (step / stages) & 1, abort)) {
             ok = false;
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          const uint64_t ad = tc_sdesc(abase + b * kTcATile, 16, 256, 6);
-          const uint64_t bd = tc_sdesc(wbase + (uint32_t)(s * N * 32), (N / 8) * 128, 128, 0);
-          asm volatile(
-              "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
-              "l"(ad), "l"(bd), "r"(kIdesc), "r"(s > 0 ? 1 : 0)
-              : "memory");
+#pragma unroll
+          for (int j = 0; j < sub; ++j, ++s16) {
+            // K slice j of the swizzled rows: the descriptor start moves 32 bytes
+            const uint64_t ad = tc_sdesc(abase + b * slot + 32u * j, 16, 8u * CB * 2, layout);
+            const uint64_t bd = tc_sdesc(wbase + (uint32_t)(s16 * N * 32), (N / 8) * 128, 128, 0);
+            asm volatile(
+                "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+                "l"(ad), "l"(bd), "r"(kIdesc), "r"((s > 0 || j > 0) ? 1 : 0)
+                : "memory");
+          }
           asm volatile(
               "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                   empty0 + 8 * b)
@@ -687,7 +707,7 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
               "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
               " selp.u32 %0, 1, 0, p;\n}\n"
               : "=r"(done)
-              : "r"(empty0 + 8 * (last % kTcStages)), "r"((last / kTcStages) & 1)
+              : "r"(empty0 + 8 * (last % stages)), "r"((last / stages) & 1)
               : "memory");
           if (done) break;
         }
@@ -785,7 +805,8 @@ int pow2_at_least(int v) {
 template <int N>
 int launch_fwd_tc(const bf16* x, Grid4 g, int C, const bf16* w, const float* bias, float* z,
                   bf16* a, int act, float slope, cudaStream_t st) {
-  const size_t smem = 1024 + (size_t)kTcStages * kTcATile + (size_t)27 * C * N * 2;
+  const size_t smem = 1024 + (size_t)kTcRing + (size_t)27 * C * N * 2;
+  const int cb = C % 64 == 0 ? 64 : (C % 32 == 0 ? 32 : 16);  // channels per TMA box
   if (smem > 200 * 1024)
     return fail(COFFEE_E_INVALID, "tcgen05 convolution: %d x %d weights exceed shared memory", N,
                 C);
@@ -805,15 +826,20 @@ int launch_fwd_tc(const bf16* x, Grid4 g, int C, const bf16* w, const float* bia
                               (cuuint64_t)g.n};
   const cuuint64_t strides[4] = {(cuuint64_t)C * 2, (cuuint64_t)C * 2 * g.w,
                                  (cuuint64_t)C * 2 * g.w * g.h, (cuuint64_t)C * 2 * g.w * g.h * g.d};
-  const cuuint32_t boxdim[5] = {16, (cuuint32_t)box.bx, (cuuint32_t)box.by, (cuuint32_t)box.bz, 1};
+  const cuuint32_t boxdim[5] = {(cuuint32_t)cb, (cuuint32_t)box.bx, (cuuint32_t)box.by,
+                                (cuuint32_t)box.bz, 1};
   const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
   const CUresult cr = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16*>(x), dims,
                           strides, boxdim, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                          CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          cb == 16 ? CU_TENSOR_MAP_SWIZZLE_32B
+                                   : (cb == 32 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                               : CU_TENSOR_MAP_SWIZZLE_128B),
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (cr != CUDA_SUCCESS)
     return fail(COFFEE_E_INVALID, "tcgen05 convolution: tensor map rejected (%d)", (int)cr);
-  auto kern = conv3d_fwd_tc_kernel<N>;
+  auto kern = cb == 64 ? conv3d_fwd_tc_kernel<N, 64>
+                       : (cb == 32 ? conv3d_fwd_tc_kernel<N, 32> : conv3d_fwd_tc_kernel<N, 16>);
   COFFEE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   // all of the unified L1 / shared memory as shared memory, so that the
   // occupancy below counts every CTA that fits

@@ -70,6 +70,13 @@ def conv_forward_tc(x, w_bf16, bias, k, act, z=None, a=None):
     return z, a
 
 
+def use_tc(c, k):
+    """True where the tcgen05 convolution is the faster one: inputs of 16, 32
+    or 64 channels (one TMA box of 16, 32 or 64 channels per tap); the results
+    are those of the mma.sync kernel."""
+    return c in (16, 32, 64) and k in (16, 32, 48, 64)
+
+
 def tc_fault(clear=True):
     """True if a wait of the tcgen05 convolution ran out of time (results invalid)."""
     flag = ctypes.c_int(0)
@@ -157,7 +164,8 @@ class UNet:
         shape = x.shape[:4] + (L.cout,)
         z = torch.empty(shape, dtype=torch.float32, device=self.dev)
         a = torch.empty(shape, dtype=torch.bfloat16, device=self.dev) if act else None
-        conv_forward(x, L.wb, L.b, L.cout, act, z, a)
+        fwd = conv_forward_tc if use_tc(L.cin, L.cout) else conv_forward
+        fwd(x, L.wb, L.b, L.cout, act, z, a)
         return z, a
 
     def forward(self, x):
@@ -218,6 +226,8 @@ class UNet:
         def dgrad(i, dzb, like):
             L = self.layers[i]
             dx = torch.empty(like.shape[:4] + (L.cin,), dtype=torch.float32, device=self.dev)
+            if use_tc(L.cout, L.cin):
+                return conv_forward_tc(dzb, L.wt, None, L.cin, False, dx, None)[0]
             return conv_backward_data(dzb, L.wt, L.cin, dx)
 
         dzb6 = bf(dout)
