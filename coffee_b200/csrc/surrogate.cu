@@ -552,7 +552,9 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
   constexpr uint32_t slot = (uint32_t)(kTcM * CB * 2);
   constexpr uint32_t stages = (uint32_t)(kTcRing / (kTcM * CB * 2));
   constexpr uint32_t layout = CB == 16 ? 6u : (CB == 32 ? 4u : 2u);  // 32B / 64B / 128B swizzle
-  const int bchunks = C / CB, nstage = 27 * bchunks;
+  // boxes per tap; a box may reach past C (C = 48 in 64-channel boxes): the
+  // TMA unit fills those channels with zeros and no MMA reads them
+  const int bchunks = (C + CB - 1) / CB, nstage = 27 * bchunks;
   // A ring at the first 1024-byte boundary (the swizzle atoms repeat every
   // 256 to 1024 bytes), the weights after it
   const uint32_t abase = (smem_addr(tc_smem) + 1023u) & ~1023u;
@@ -668,6 +670,7 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t d = tmem + acc * NCOLS;
         int s16 = 0;  // 16-channel K step of the stage's first MMA
+        int cq = 0;   // first channel of the stage's box
         for (int s = 0; s < nstage; ++s, ++step) {
           const uint32_t b = step % stages;
           if (!tc_wait(full0 + 8 * b, (step / stages) & 1, abort)) {
@@ -677,6 +680,7 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
           for (int j = 0; j < sub; ++j, ++s16) {
+            if (cq + 16 * j >= C) break;  // past the tensor's channels
             // K slice j of the swizzled rows: the descriptor start moves 32 bytes
             const uint64_t ad = tc_sdesc(abase + b * slot + 32u * j, 16, 8u * CB * 2, layout);
             const uint64_t bd = tc_sdesc(wbase + (uint32_t)(s16 * N * 32), (N / 8) * 128, 128, 0);
@@ -690,6 +694,8 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
               "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                   empty0 + 8 * b)
               : "memory");
+          cq += CB;
+          if (cq >= C) cq = 0;
         }
         if (!ok) break;
         asm volatile(
@@ -806,7 +812,9 @@ template <int N>
 int launch_fwd_tc(const bf16* x, Grid4 g, int C, const bf16* w, const float* bias, float* z,
                   bf16* a, int act, float slope, cudaStream_t st) {
   const size_t smem = 1024 + (size_t)kTcRing + (size_t)27 * C * N * 2;
-  const int cb = C % 64 == 0 ? 64 : (C % 32 == 0 ? 32 : 16);  // channels per TMA box
+  // channels per TMA box: the widest that divides C; 48 channels in one
+  // 64-channel box (the last 16 zero-filled, not multiplied)
+  const int cb = (C % 64 == 0 || C == 48) ? 64 : (C % 32 == 0 ? 32 : 16);
   if (smem > 200 * 1024)
     return fail(COFFEE_E_INVALID, "tcgen05 convolution: %d x %d weights exceed shared memory", N,
                 C);
