@@ -221,6 +221,169 @@ static void FN(rk_step)(const oracle_params* p, const FN(grid_t) * g, REAL* cons
   }
 }
 
+/* ---- The CPU build in its own arithmetic ------------------------------
+ * The reference's CPU build is compiled by g++ -O3 for x86-64-v4, whose
+ * default -ffp-contract=fast fuses a product into the add or subtract that
+ * consumes it (one rounding).  The functions below write each of those
+ * fused multiply-adds as an explicit FMAR and every other operation as one
+ * correctly rounded IEEE operation, in the reference's order, so that with
+ * this file compiled with -ffp-contract=off the float restatement is the
+ * float build operation for operation.  Which products are fused was read
+ * from the compiler's dump of its own FMA formation pass
+ * (-fdump-tree-widening_mul) on field_solver_EZ.cpp.  The rule it follows:
+ * in a left-to-right sum a*b + c*d + e*f the first product is rounded and
+ * each later one is fused into the running sum; a product subtracted from a
+ * rounded value is a fused negative multiply-add. */
+
+/* diff1_4 of finite_diff_simd.h:15-25 before its inv_delta factor:
+ * (((f-2 - 8 f-1) + 8 f+1) - f+2) / 12, the multiplications by 8 fused
+ * (they are exact, so fused or not gives the same value). */
+static inline REAL FN(dq)(const REAL* f, size_t ijk, size_t s) {
+  REAL t = FMAR(-f[ijk - s], (REAL)8, f[ijk - 2 * s]);
+  t = FMAR(f[ijk + s], (REAL)8, t);
+  t = t - f[ijk + 2 * s];
+  return t / (REAL)12;
+}
+
+/* diff6_2 of finite_diff_simd.h:41-58, each weighted term fused into the
+ * running sum, f+3 added last */
+static inline REAL FN(d6x)(const REAL* f, size_t ijk, size_t s) {
+  REAL t = FMAR(-f[ijk - 2 * s], (REAL)6, f[ijk - 3 * s]);
+  t = FMAR(f[ijk - s], (REAL)15, t);
+  t = FMAR(-f[ijk], (REAL)20, t);
+  t = FMAR(f[ijk + s], (REAL)15, t);
+  t = FMAR(-f[ijk + 2 * s], (REAL)6, t);
+  return f[ijk + 3 * s] + t;
+}
+
+/* B2 floored at TINY as vectorclass max(B2, TINY) (x86 maxps: the second
+ * operand unless the first is greater, NaN included) */
+static inline REAL FN(floor_tiny)(REAL b2) { return b2 > TINYR ? b2 : TINYR; }
+
+/* rk_step of the CPU build (field_solver_EZ.cpp:105-322). */
+static void FN(rk_step_cpu)(const oracle_params* p, const FN(grid_t) * g, REAL* const* U,
+                            REAL* const* dU, REAL* const* aux, REAL As, REAL Bs) {
+  const int sh = p->shift_ghost;
+  const size_t s0 = 1, s1 = (size_t)g->d0, s2 = (size_t)g->d0 * g->d1;
+  REAL *Ex = U[0], *Ey = U[1], *Ez = U[2], *Bx = U[3], *By = U[4], *Bz = U[5], *P = U[6];
+  const REAL dt = (REAL)p->dt, ch2 = (REAL)p->ch2, tau = (REAL)p->tau;
+  const REAL gam_dt = (REAL)p->damp_gamma / dt;
+  const int lanes = p->taper_lanes > 0 ? p->taper_lanes : 1;
+  const REAL ix = g->inv_delta[0], iy = g->inv_delta[1], iz = g->inv_delta[2];
+  LOOP_BOX(g, sh) {
+    size_t ijk = (size_t)i + ((size_t)j + (size_t)k * g->d1) * g->d0;
+    /* dfdy(Bz) - dfdz(By): the first product rounded, the second fused */
+    const REAL rotBx = FMAR(-iz, FN(dq)(By, ijk, s2), iy * FN(dq)(Bz, ijk, s1));
+    const REAL rotBy = FMAR(-ix, FN(dq)(Bz, ijk, s0), iz * FN(dq)(Bx, ijk, s2));
+    const REAL rotBz = FMAR(-iy, FN(dq)(Bx, ijk, s1), ix * FN(dq)(By, ijk, s0));
+    const REAL rotEx = FMAR(-iz, FN(dq)(Ey, ijk, s2), iy * FN(dq)(Ez, ijk, s1));
+    const REAL rotEy = FMAR(-ix, FN(dq)(Ez, ijk, s0), iz * FN(dq)(Ex, ijk, s2));
+    const REAL rotEz = FMAR(-iy, FN(dq)(Ex, ijk, s1), ix * FN(dq)(Ey, ijk, s0));
+    const REAL divE =
+        FMAR(iz, FN(dq)(Ez, ijk, s2), FMAR(iy, FN(dq)(Ey, ijk, s1), ix * FN(dq)(Ex, ijk, s0)));
+    const REAL divB =
+        FMAR(iz, FN(dq)(Bz, ijk, s2), FMAR(iy, FN(dq)(By, ijk, s1), ix * FN(dq)(Bx, ijk, s0)));
+    const REAL ex = Ex[ijk], ey = Ey[ijk], ez = Ez[ijk], bx = Bx[ijk], by = By[ijk], bz = Bz[ijk];
+    const REAL B2 = FN(floor_tiny)(FMAR(bz, bz, FMAR(by, by, bx * bx)));
+    const REAL BrotB = FMAR(bz, rotBz, FMAR(by, rotBy, bx * rotBx));
+    const REAL ErotE = FMAR(ez, rotEz, FMAR(ey, rotEy, ex * rotEx));
+    const REAL cx = FMAR(-by, ez, bz * ey), cy = FMAR(-bz, ex, bx * ez), cz = FMAR(-bx, ey, by * ex);
+    REAL Jx, Jy, Jz;
+    if (p->use_edotb_damping) {
+      const REAL E2 = FMAR(ez, ez, FMAR(ey, ey, ex * ex));
+      const REAL chi2 = B2 - E2;
+      const REAL EdotB = FMAR(bz, ez, FMAR(by, ey, bx * ex));
+      const REAL E02 = FMAR(SQRTR(FMAR(EdotB * (REAL)4, EdotB, chi2 * chi2)) - chi2, (REAL)0.5, B2);
+      const REAL Jp = FMAR(EdotB, gam_dt, BrotB - ErotE);
+      Jx = (divE * cx) / E02 + (bx * Jp) / B2;
+      Jy = (divE * cy) / E02 + (by * Jp) / B2;
+      Jz = (divE * cz) / E02 + (bz * Jp) / B2;
+    } else {
+      const REAL Jp = BrotB - ErotE;
+      Jx = FMAR(bx, Jp, divE * cx) / B2;
+      Jy = FMAR(by, Jp, divE * cy) / B2;
+      Jz = FMAR(bz, Jp, divE * cz) / B2;
+    }
+    if (aux) {
+      aux[0][ijk] = Jx; aux[1][ijk] = Jy; aux[2][ijk] = Jz;
+      aux[3][ijk] = divE; aux[4][ijk] = divB;
+    }
+    REAL Px = 0, Py = 0, Pz = 0;
+    if (p->divB_clean) {
+      Px = ix * FN(dq)(P, ijk, s0);
+      Py = iy * FN(dq)(P, ijk, s1);
+      Pz = iz * FN(dq)(P, ijk, s2);
+    }
+    /* the taper, lane by lane: x, y and z each offset by lane * delta, with
+     * Grid::pos(axis, n, 1) = fma(delta, n - guard + 0, lower) */
+    const int lane = (i - (g->g[0] - sh)) % lanes;
+    const int ibase = i - lane;
+    const REAL fl = (REAL)lane;
+    const REAL x = FMAR(g->delta[0], fl, FMAR(g->delta[0], (REAL)(ibase - g->g[0]), g->lower[0]));
+    const REAL y = FMAR(g->delta[1], fl, FMAR(g->delta[1], (REAL)(j - g->g[1]), g->lower[1]));
+    const REAL z = FMAR(g->delta[2], fl, FMAR(g->delta[2], (REAL)(k - g->g[2]), g->lower[2]));
+    const REAL r = SQRTR(FMAR(z, z, FMAR(y, y, x * x)));
+    /* (r - 3) / 0.5 is compiled as (r + -3) * 2, exact either way */
+    const REAL s = ((REAL)1 - TANHX((r - (REAL)3) * (REAL)2)) * (REAL)0.5;
+    dU[3][ijk] = FMAR(-dt, FMAR(Px, s, rotEx), dU[3][ijk] * As);
+    dU[4][ijk] = FMAR(-dt, FMAR(Py, s, rotEy), dU[4][ijk] * As);
+    dU[5][ijk] = FMAR(-dt, FMAR(Pz, s, rotEz), dU[5][ijk] * As);
+    dU[0][ijk] = FMAR(dt, rotBx - Jx, dU[0][ijk] * As);
+    dU[1][ijk] = FMAR(dt, rotBy - Jy, dU[1][ijk] * As);
+    dU[2][ijk] = FMAR(dt, rotBz - Jz, dU[2][ijk] * As);
+    dU[6][ijk] = FMAR(-dt, divB * ch2, FMAR(dU[6][ijk], As, -(P[ijk] / tau)));
+  }
+  LOOP_BOX(g, sh) {
+    size_t ijk = (size_t)i + ((size_t)j + (size_t)k * g->d1) * g->d0;
+    /* mul_add(dU, Bs, U) */
+    for (int f = 0; f < 7; ++f) U[f][ijk] = FMAR(dU[f][ijk], Bs, U[f][ijk]);
+  }
+}
+
+/* clean_epar_check_eGTb of the CPU build (field_solver_EZ.cpp:552-634) */
+static void FN(clamps_cpu)(const oracle_params* p, const FN(grid_t) * g, REAL* const* U) {
+  const int sh = p->shift_ghost;
+  REAL *Ex = U[0], *Ey = U[1], *Ez = U[2], *Bx = U[3], *By = U[4], *Bz = U[5];
+  LOOP_BOX(g, sh) {
+    size_t ijk = (size_t)i + ((size_t)j + (size_t)k * g->d1) * g->d0;
+    const REAL bx = Bx[ijk], by = By[ijk], bz = Bz[ijk];
+    REAL ex = Ex[ijk], ey = Ey[ijk], ez = Ez[ijk];
+    const REAL B2 = FN(floor_tiny)(FMAR(bz, bz, FMAR(by, by, bx * bx)));
+    const REAL EB = FMAR(bz, ez, FMAR(by, ey, bx * ex));
+    ex = ex - (EB * bx) / B2;
+    ey = ey - (EB * by) / B2;
+    ez = ez - (EB * bz) / B2;
+    const REAL E2 = FMAR(ez, ez, FMAR(ey, ey, ex * ex));
+    if (E2 > B2) {
+      const REAL s = SQRTR(B2 / E2);
+      ex = ex * s;
+      ey = ey * s;
+      ez = ez * s;
+    }
+    Ex[ijk] = ex; Ey[ijk] = ey; Ez[ijk] = ez;
+  }
+}
+
+/* Kreiss_Oliger of the CPU build (field_solver_EZ.cpp:324-457): E and B only,
+ * f + KO(f) * (-KOeps * KO_const), the product fused; KO sums the axes
+ * x, y, z left to right */
+static void FN(kreiss_oliger_cpu)(const oracle_params* p, const FN(grid_t) * g, REAL* const* U,
+                                  REAL* const* tmp) {
+  const int sh = p->shift_ghost;
+  const size_t s1 = (size_t)g->d0, s2 = (size_t)g->d0 * g->d1;
+  LOOP_BOX(g, sh) {
+    size_t ijk = (size_t)i + ((size_t)j + (size_t)k * g->d1) * g->d0;
+    for (int f = 0; f < 6; ++f)
+      tmp[f][ijk] = (FN(d6x)(U[f], ijk, 1) + FN(d6x)(U[f], ijk, s1)) + FN(d6x)(U[f], ijk, s2);
+  }
+  /* -KOeps * KO_const with KO_const = -1/64: compiled as KOeps * (1/64) */
+  const REAL c = (REAL)p->KOeps * (REAL)0.015625;
+  LOOP_BOX(g, sh) {
+    size_t ijk = (size_t)i + ((size_t)j + (size_t)k * g->d1) * g->d0;
+    for (int f = 0; f < 6; ++f) U[f][ijk] = FMAR(c, tmp[f][ijk], U[f][ijk]);
+  }
+}
+
 /* Clamps.  CPU build: clean_epar_check_eGTb always (field_solver_EZ.cpp:552-634).
  * GPU build: kernel_Epar if clean_ep, kernel_EgtB if check_egb (.cu:213-270). */
 static void FN(clamps)(const oracle_params* p, const FN(grid_t) * g, REAL* const* U) {
@@ -532,8 +695,13 @@ int FN(oracle_evolve)(const oracle_params* p, REAL* const* U, REAL* const* aux, 
   for (int step = 0; step < nsteps; ++step) {
     for (int f = 0; f < 7; ++f) memcpy(Un[f], U[f], g.n * sizeof(REAL));
     for (int st = 0; st < 5; ++st) {
-      FN(rk_step)(p, &g, U, dU, aux, (REAL)As_d[st], (REAL)Bs_d[st]);
-      FN(clamps)(p, &g, U);
+      if (cpu) {
+        FN(rk_step_cpu)(p, &g, U, dU, aux, (REAL)As_d[st], (REAL)Bs_d[st]);
+        FN(clamps_cpu)(p, &g, U);
+      } else {
+        FN(rk_step)(p, &g, U, dU, aux, (REAL)As_d[st], (REAL)Bs_d[st]);
+        FN(clamps)(p, &g, U);
+      }
       REAL ts = time + (REAL)cs_d[st] * dt;
       if (p->problem == 1) FN(boundary_star)(p, &g, U, ts, 0);
       else if (p->problem == 2 && cpu) FN(boundary_star)(p, &g, U, ts, 1);
@@ -541,8 +709,13 @@ int FN(oracle_evolve)(const oracle_params* p, REAL* const* U, REAL* const* aux, 
       FN(guard_fill)(U, &g, p);
     }
     /* the KO scratch reuses the start-of-step copies, as the reference does */
-    FN(kreiss_oliger)(p, &g, U, Un);
-    FN(clamps)(p, &g, U);
+    if (cpu) {
+      FN(kreiss_oliger_cpu)(p, &g, U, Un);
+      FN(clamps_cpu)(p, &g, U);
+    } else {
+      FN(kreiss_oliger)(p, &g, U, Un);
+      FN(clamps)(p, &g, U);
+    }
     if (p->problem == 1) FN(boundary_star)(p, &g, U, time + dt, 0);
     else if (p->problem == 2 && cpu) FN(boundary_star)(p, &g, U, time + dt, 1);
     FN(guard_fill)(U, &g, p);
