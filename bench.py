@@ -344,6 +344,7 @@ def run_ours(args):
     modes = problems.turbulence_modes()
     data.init_fourier((1.0, 0.0, 0.0), *modes)
     solver = FieldSolverEZ(data, env, "cpu", stream=stream.cuda_stream)
+    solver.set_arithmetic(args.arith)
     dt = np.float32(p.dt)
 
     # warm-up (untimed)
@@ -372,6 +373,25 @@ def run_ours(args):
     timing = solver.last_timing()
     solver.set_timing(False)
     solver.check_finite()
+
+    # the other arithmetic of the same solver, timed the same way on rank 0
+    # (its cost or gain beside the mode measured)
+    other = None
+    if ws == 1 and not args.no_arith_compare:
+        alt = "fast" if args.arith == "reference" else "reference"
+        solver.set_arithmetic(alt)
+        solver.step(float(t), 1)
+        torch.cuda.synchronize(dev)
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        solver.step(float(t), args.steps)
+        a1.record(stream)
+        torch.cuda.synchronize(dev)
+        other = {"mode": alt, "ms_per_step": a0.elapsed_time(a1) / args.steps}
+        solver.set_arithmetic(args.arith)
+        # the fields moved on: start the end-to-end leg from the device set-up
+        data.init_fourier((1.0, 0.0, 0.0), *modes)
 
     value = job_throughput(cells, args.steps, ws, ms_max / 1e3)
     step_ms = ms_max / args.steps
@@ -441,6 +461,10 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": nbytes / args.steps,
                     "d2h_bytes_per_step": nbytes / args.steps + d2h_diag},
+            "arithmetic": {"mode": args.arith,
+                           "note": ("reference: the float build's own operations and rounding, "
+                                    "bit for bit; fast: regrouped, equal to rounding"),
+                           "other": other},
             "cpu_baseline": cpu,
             "error_vs_fp64": err64,
             "clocks": clk,
@@ -777,6 +801,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--arith", choices=["reference", "fast"], default="reference",
+                    help="arithmetic of the flat solver (reference: the float build's own)")
+    ap.add_argument("--no-arith-compare", action="store_true",
+                    help="skip timing the other arithmetic beside the measured one")
     ap.add_argument("--no-fp64-check", action="store_true",
                     help="skip the FP32-vs-FP64 error report of the turbulence run")
     ap.add_argument("--n", type=int, default=N_SIDE,

@@ -39,25 +39,39 @@ def _newest_input() -> float:
 def build(force: bool = False, ptxas_verbose: bool = False, log=None, defines=(),
           out: str | None = None) -> str:
     """Compile the library; `defines` (e.g. ["COFFEE_F32_STY=4"]) override
-    tile-shape macros, `out` writes the library elsewhere than LIB."""
+    tile-shape macros, `out` writes the library elsewhere than LIB.  Each
+    source is compiled to an object by its own nvcc process, in parallel,
+    and the objects are linked into the shared library."""
     target = out or LIB
     if not force and not defines and os.path.exists(target) and \
             os.path.getmtime(target) >= _newest_input():
         return target
-    cmd = [nvcc_path(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "--shared",
-           "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
-           "-I", INCLUDE, "-I", CSRC, "-DCOFFEE_BUILDING_LIBRARY",
-           "-o", target + ".tmp"] + [f"-D{d}" for d in defines]
+    nvcc = nvcc_path()
+    objdir = target + ".objs"
+    os.makedirs(objdir, exist_ok=True)
+    common = [nvcc, "-O3", "-std=c++17", *ARCH, "-lineinfo",
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+              "-I", INCLUDE, "-I", CSRC, "-DCOFFEE_BUILDING_LIBRARY"] + [f"-D{d}" for d in defines]
     if ptxas_verbose:
-        cmd += ["-Xptxas", "-v"]
-    cmd += [os.path.join(CSRC, s) for s in SOURCES]
-    cmd += ["-lcudart"]
-    r = subprocess.run(cmd, capture_output=True, text=True)
-    text = r.stdout + r.stderr
+        common += ["-Xptxas", "-v"]
+    objs = [os.path.join(objdir, os.path.splitext(s)[0] + ".o") for s in SOURCES]
+    procs = [subprocess.Popen(common + ["-c", os.path.join(CSRC, s), "-o", o],
+                              stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+             for s, o in zip(SOURCES, objs)]
+    failed, texts = [], []
+    for s, p in zip(SOURCES, procs):
+        text = p.communicate()[0]
+        texts.append(text)
+        if p.returncode != 0:
+            failed.append(f"{s}: nvcc exited {p.returncode}\n{text[-6000:]}")
     if log is not None:
-        log.write(text)
+        log.write("".join(texts))
+    if failed:
+        raise RuntimeError("\n".join(failed))
+    cmd = [nvcc, *ARCH, "--shared", "-o", target + ".tmp"] + objs + ["-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({r.returncode}):\n{text[-6000:]}")
+        raise RuntimeError(f"nvcc link failed ({r.returncode}):\n{(r.stdout + r.stderr)[-6000:]}")
     os.replace(target + ".tmp", target)
     return target
 

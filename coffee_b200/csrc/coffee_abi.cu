@@ -64,6 +64,7 @@ struct coffee_solver {
   bool absorbing;
   int aux;
   int timing;
+  int arith;    // COFFEE_ARITH_* of the flat solver
   uint64_t synced_generation;
   FlatLaunch launch;
   void* vtab;  // tables / scratch of a non-Cartesian variant (device), or null
@@ -556,7 +557,7 @@ extern "C" int coffee_fields_fill_guards(coffee_fields* f) {
 
 template <typename T>
 static int configure_solver(coffee_solver* s) {
-  return flat_plan<T>(s->env, s->semantics, &s->launch);
+  return flat_plan<T>(s->env, s->semantics, &s->launch, s->arith == COFFEE_ARITH_REFERENCE);
 }
 
 extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int variant,
@@ -597,6 +598,7 @@ extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int varia
   s->stream = static_cast<cudaStream_t>(stream);
   s->aux = 0;
   s->timing = 0;
+  s->arith = COFFEE_ARITH_REFERENCE;
   s->events_used = 0;
   s->synced_generation = 0;
   // the GR solver's inner absorbing region always needs the start-of-step
@@ -685,6 +687,27 @@ extern "C" int coffee_solver_set_aux(coffee_solver* s, int enable) {
     }
   s->aux = enable ? 1 : 0;
   return COFFEE_OK;
+}
+
+extern "C" int coffee_solver_set_arithmetic(coffee_solver* s, int mode) {
+  clear_error();
+  if (!s) return fail(COFFEE_E_INVALID, "coffee_solver_set_arithmetic: null argument");
+  if (mode != COFFEE_ARITH_REFERENCE && mode != COFFEE_ARITH_FAST)
+    return fail(COFFEE_E_INVALID, "unknown arithmetic mode %d", mode);
+  if (s->variant != COFFEE_VARIANT_FLAT) {
+    if (mode == COFFEE_ARITH_REFERENCE) return COFFEE_OK;
+    return fail(COFFEE_E_INVALID, "only the flat EZ solver has a second arithmetic");
+  }
+  if (mode == s->arith) return COFFEE_OK;
+  COFFEE_CUDA_TRY(cudaSetDevice(s->env->device));
+  const int old = s->arith;
+  s->arith = mode;
+  const int rc = (s->f->elem == 4) ? configure_solver<float>(s) : configure_solver<double>(s);
+  if (rc) {
+    s->arith = old;  // keep the previous plan
+    (void)((s->f->elem == 4) ? configure_solver<float>(s) : configure_solver<double>(s));
+  }
+  return rc;
 }
 
 extern "C" int coffee_solver_set_timing(coffee_solver* s, int enable) {

@@ -39,7 +39,9 @@ std::mutex g_noalloc_mutex;
 
 // Once per device, with that device current: look up the device address of
 // the static array (a host-side name of a __device__ variable is not a
-// device address).
+// device address).  The address is cached for the life of the process; it
+// belongs to the device's primary context and goes stale if the caller
+// resets the device (cudaDeviceReset), which the header documents.
 int noalloc_setup(int device, float** scratch) {
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
   if (device < 0 || device >= 64) return fail(COFFEE_E_INVALID, "device %d out of range", device);

@@ -99,7 +99,10 @@ struct Derivs {
   T rotE[3], rotB[3], divE, divB, gradP[3];
 };
 
-template <typename T, bool FIRST, bool BC>
+// XA selects the CPU build's own arithmetic (ez_refarith.cuh) for the
+// current, the taper, the accumulators, the update and the clamps; the
+// derivatives then come in already combined in that arithmetic (Derivs).
+template <typename T, bool FIRST, bool BC, bool XA>
 __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7],
                                             const Derivs<T>& dv, const T dold[7],
                                             const T As, const T Bs, const T tst,
@@ -113,55 +116,109 @@ __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7],
   const T rotEx = dv.rotE[0], rotEy = dv.rotE[1], rotEz = dv.rotE[2];
   const T divE = dv.divE;
   const T divB = dv.divB;
-  T B2 = bx * bx + by * by + bz * bz;
-  if (B2 < Tiny<T>::v) B2 = Tiny<T>::v;
-  const T BrotB = bx * rotBx + by * rotBy + bz * rotBz;
-  const T ErotE = ex * rotEx + ey * rotEy + ez * rotEz;
-  const T cx = ey * bz - ez * by, cy = ez * bx - ex * bz, cz = ex * by - ey * bx;
-  T Jx, Jy, Jz;
-  if (c.use_edotb) {
-    // J with E.B damping (field_solver_EZ.cpp:170-186, .cu:72-91)
-    const T E2 = ex * ex + ey * ey + ez * ez;
-    const T chi2 = B2 - E2;
-    const T EdotB = ex * bx + ey * by + ez * bz;
-    const T E02 = (T)0.5 * (sqrt(chi2 * chi2 + (T)4 * EdotB * EdotB) - chi2) + B2;
-    const T Jp = BrotB - ErotE + EdotB * c.gam_dt;
-    const T a = fdiv(divE, E02), b = fdiv(Jp, B2);
-    Jx = a * cx + b * bx;
-    Jy = a * cy + b * by;
-    Jz = a * cz + b * bz;
-  } else {
-    const T Jp = BrotB - ErotE;
-    const T rB2 = fdiv((T)1, B2);
-    Jx = (divE * cx + Jp * bx) * rB2;
-    Jy = (divE * cy + Jp * by) * rB2;
-    Jz = (divE * cz + Jp * bz) * rB2;
-  }
-  T Px = 0, Py = 0, Pz = 0;
-  if (c.divB_clean) {
-    Px = dv.gradP[0];
-    Py = dv.gradP[1];
-    Pz = dv.gradP[2];
-    if (cpu) {
-      const T s = p_taper(c, col, k);
-      Px *= s;
-      Py *= s;
-      Pz *= s;
-    }
-  }
-  // new accumulators
   T d[7];
-  const T dt = c.dt;
-  d[0] = (rotBx - Jx) * dt;
-  d[1] = (rotBy - Jy) * dt;
-  d[2] = (rotBz - Jz) * dt;
-  d[3] = -(rotEx + Px) * dt;
-  d[4] = -(rotEy + Py) * dt;
-  d[5] = -(rotEz + Pz) * dt;
-  d[6] = -P * c.inv_tau - divB * c.ch2 * dt;
-  if constexpr (!FIRST) {
+  T Jx, Jy, Jz;
+  if constexpr (XA) {
+    // rk_step of the CPU build (field_solver_EZ.cpp:143-259) operation for
+    // operation
+    const T B2 = xa::floor_tiny(xa::dot3(bx, bx, by, by, bz, bz));
+    const T BrotB = xa::dot3(bx, rotBx, by, rotBy, bz, rotBz);
+    const T ErotE = xa::dot3(ex, rotEx, ey, rotEy, ez, rotEz);
+    const T cx = xa::fma(-by, ez, xa::mul(bz, ey));
+    const T cy = xa::fma(-bz, ex, xa::mul(bx, ez));
+    const T cz = xa::fma(-bx, ey, xa::mul(by, ex));
+    if (c.use_edotb) {
+      const T E2 = xa::dot3(ex, ex, ey, ey, ez, ez);
+      const T chi2 = xa::sub(B2, E2);
+      const T EdotB = xa::dot3(bx, ex, by, ey, bz, ez);
+      const T E02 = xa::fma(
+          xa::sub(xa::sqrt(xa::fma(xa::mul(EdotB, (T)4), EdotB, xa::mul(chi2, chi2))), chi2),
+          (T)0.5, B2);
+      const T Jp = xa::fma(EdotB, c.gam_dt, xa::sub(BrotB, ErotE));
+      Jx = xa::add(xa::div(xa::mul(divE, cx), E02), xa::div(xa::mul(bx, Jp), B2));
+      Jy = xa::add(xa::div(xa::mul(divE, cy), E02), xa::div(xa::mul(by, Jp), B2));
+      Jz = xa::add(xa::div(xa::mul(divE, cz), E02), xa::div(xa::mul(bz, Jp), B2));
+    } else {
+      const T Jp = xa::sub(BrotB, ErotE);
+      Jx = xa::div(xa::fma(bx, Jp, xa::mul(divE, cx)), B2);
+      Jy = xa::div(xa::fma(by, Jp, xa::mul(divE, cy)), B2);
+      Jz = xa::div(xa::fma(bz, Jp, xa::mul(divE, cz)), B2);
+    }
+    T Px = 0, Py = 0, Pz = 0;
+    if (c.divB_clean) {
+      Px = dv.gradP[0];
+      Py = dv.gradP[1];
+      Pz = dv.gradP[2];
+    }
+    const T s = p_taper_xa(c, col, k);
+    const T dt = c.dt;
+    // dU As (As = 0 on the first stage, where the old dU is not read)
+    T da[7];
 #pragma unroll
-    for (int f = 0; f < 7; ++f) d[f] = fma(dold[f], As, d[f]);
+    for (int f = 0; f < 7; ++f) {
+      if constexpr (FIRST) da[f] = (T)0;
+      else da[f] = xa::mul(dold[f], As);
+    }
+    d[0] = xa::fma(dt, xa::sub(rotBx, Jx), da[0]);
+    d[1] = xa::fma(dt, xa::sub(rotBy, Jy), da[1]);
+    d[2] = xa::fma(dt, xa::sub(rotBz, Jz), da[2]);
+    d[3] = xa::fma(-dt, xa::fma(Px, s, rotEx), da[3]);
+    d[4] = xa::fma(-dt, xa::fma(Py, s, rotEy), da[4]);
+    d[5] = xa::fma(-dt, xa::fma(Pz, s, rotEz), da[5]);
+    // dP As - P / tau with the product fused, minus dt (divB ch2)
+    if constexpr (FIRST)
+      d[6] = xa::fma(-dt, xa::mul(divB, c.ch2), -xa::div(P, c.tau));
+    else
+      d[6] = xa::fma(-dt, xa::mul(divB, c.ch2), xa::fma(dold[6], As, -xa::div(P, c.tau)));
+  } else {
+    T B2 = bx * bx + by * by + bz * bz;
+    if (B2 < Tiny<T>::v) B2 = Tiny<T>::v;
+    const T BrotB = bx * rotBx + by * rotBy + bz * rotBz;
+    const T ErotE = ex * rotEx + ey * rotEy + ez * rotEz;
+    const T cx = ey * bz - ez * by, cy = ez * bx - ex * bz, cz = ex * by - ey * bx;
+    if (c.use_edotb) {
+      // J with E.B damping (field_solver_EZ.cpp:170-186, .cu:72-91)
+      const T E2 = ex * ex + ey * ey + ez * ez;
+      const T chi2 = B2 - E2;
+      const T EdotB = ex * bx + ey * by + ez * bz;
+      const T E02 = (T)0.5 * (sqrt(chi2 * chi2 + (T)4 * EdotB * EdotB) - chi2) + B2;
+      const T Jp = BrotB - ErotE + EdotB * c.gam_dt;
+      const T a = fdiv(divE, E02), b = fdiv(Jp, B2);
+      Jx = a * cx + b * bx;
+      Jy = a * cy + b * by;
+      Jz = a * cz + b * bz;
+    } else {
+      const T Jp = BrotB - ErotE;
+      const T rB2 = fdiv((T)1, B2);
+      Jx = (divE * cx + Jp * bx) * rB2;
+      Jy = (divE * cy + Jp * by) * rB2;
+      Jz = (divE * cz + Jp * bz) * rB2;
+    }
+    T Px = 0, Py = 0, Pz = 0;
+    if (c.divB_clean) {
+      Px = dv.gradP[0];
+      Py = dv.gradP[1];
+      Pz = dv.gradP[2];
+      if (cpu) {
+        const T s = p_taper(c, col, k);
+        Px *= s;
+        Py *= s;
+        Pz *= s;
+      }
+    }
+    // new accumulators
+    const T dt = c.dt;
+    d[0] = (rotBx - Jx) * dt;
+    d[1] = (rotBy - Jy) * dt;
+    d[2] = (rotBz - Jz) * dt;
+    d[3] = -(rotEx + Px) * dt;
+    d[4] = -(rotEy + Py) * dt;
+    d[5] = -(rotEz + Pz) * dt;
+    d[6] = -P * c.inv_tau - divB * c.ch2 * dt;
+    if constexpr (!FIRST) {
+#pragma unroll
+      for (int f = 0; f < 7; ++f) d[f] = fma(dold[f], As, d[f]);
+    }
   }
   // the start-of-step copy is only read inside the absorbing layer
   T sig = (T)0;
@@ -180,9 +237,16 @@ __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7],
     aux.p[4][o] = divB;
   }
   T nu[7];
+  if constexpr (XA) {
+    // mul_add(dU, Bs, U), then clean_epar_check_eGTb
 #pragma unroll
-  for (int f = 0; f < 7; ++f) nu[f] = fma(d[f], Bs, u[f]);
-  apply_clamps(c, nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
+    for (int f = 0; f < 7; ++f) nu[f] = xa::fma(d[f], Bs, u[f]);
+    apply_clamps_xa(nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
+  } else {
+#pragma unroll
+    for (int f = 0; f < 7; ++f) nu[f] = fma(d[f], Bs, u[f]);
+    apply_clamps(c, nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
+  }
   if constexpr (BC) star_boundary(c, col.i, col.j, k, tst, nu);
   if (BC && (flags & ST_LAST) != 0 && sig > (T)0) {
     V7<T> uv, unv;
@@ -324,7 +388,7 @@ constexpr size_t stage_smem_bytes(bool first) {
          (first ? 0 : (size_t)stage_dring<BC, PF>() * 7 * TX * TY * sizeof(T));
 }
 
-template <typename T, int TX, int TY, int PF, bool FIRST, bool BC, int V>
+template <typename T, int TX, int TY, int PF, bool FIRST, bool BC, int V, bool XA>
 __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     ez_stage_kernel(const __grid_constant__ EzConst<T> c, const F7<const T> uin,
                     const F7<T> uout, const F7<T> du, const F7<T> un, const F5<T> aux,
@@ -355,7 +419,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
   const unsigned amask = __ballot_sync(0xffffffffu, active);
   const uint32_t sz = (uint32_t)g.sz;
   const uint32_t own = (uint32_t)j * (uint32_t)g.sy + (uint32_t)i;
-  const ColumnCtx<T> col = make_column(c, i, j);
+  const ColumnCtx<T> col = make_column<XA>(c, i, j);
   const L loader(g, sbase, tid, g.lo[0] + (int)blockIdx.x * TX - 2,
                  g.lo[1] + (int)blockIdx.y * TY - 2);
   const uint32_t dme = dbase + (uint32_t)(tid * ES);
@@ -398,6 +462,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
 
   const T six = c.inv_delta[0] / (T)12, siy = c.inv_delta[1] / (T)12,
           siz = c.inv_delta[2] / (T)12;
+  const T ix = c.inv_delta[0], iy = c.inv_delta[1], iz = c.inv_delta[2];
   const uint32_t corner = sbase + (uint32_t)((ty * SX + tx + loader.xoff) * ES);
   // Register window: in window phase S, w[(S + q) % 5][f] = field f at
   // (i, j, k - 2 + q).  Planes k-2 .. k+1 are carried from the previous
@@ -430,27 +495,53 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
       // next group from being hoisted, which bounds the live registers.
       T u[7], dold[7];
       Derivs<T> dv;
+      // dxyz[a]: the derivative of field f along axis a, inv_delta-scaled;
+      // in the reference arithmetic (XA) the unscaled quotient of diff1_4,
+      // which curl_div scales and combines as the CPU build does
       auto d1 = [&](auto fc, T* dxyz) {
         constexpr int f = decltype(fc)::value;
         constexpr int o = f * FB;
-        dxyz[0] = d1_4(lds<T, o + CEN - 2 * ES>(a0), lds<T, o + CEN - ES>(a0),
-                       lds<T, o + CEN + ES>(a0), lds<T, o + CEN + 2 * ES>(a0), six);
-        dxyz[1] = d1_4(lds<T, o + 2 * ES>(a0), lds<T, o + (SX + 2) * ES>(a0),
-                       lds<T, o + (3 * SX + 2) * ES>(a0), lds<T, o + (4 * SX + 2) * ES>(a0), siy);
+        if constexpr (XA) {
+          dxyz[0] = xa::dq(lds<T, o + CEN - 2 * ES>(a0), lds<T, o + CEN - ES>(a0),
+                           lds<T, o + CEN + ES>(a0), lds<T, o + CEN + 2 * ES>(a0));
+          dxyz[1] = xa::dq(lds<T, o + 2 * ES>(a0), lds<T, o + (SX + 2) * ES>(a0),
+                           lds<T, o + (3 * SX + 2) * ES>(a0), lds<T, o + (4 * SX + 2) * ES>(a0));
+        } else {
+          dxyz[0] = d1_4(lds<T, o + CEN - 2 * ES>(a0), lds<T, o + CEN - ES>(a0),
+                         lds<T, o + CEN + ES>(a0), lds<T, o + CEN + 2 * ES>(a0), six);
+          dxyz[1] = d1_4(lds<T, o + 2 * ES>(a0), lds<T, o + (SX + 2) * ES>(a0),
+                         lds<T, o + (3 * SX + 2) * ES>(a0), lds<T, o + (4 * SX + 2) * ES>(a0), siy);
+        }
         w[(S + 4) % 5][f] = lds<T, o + CEN>(ap2);
         u[f] = w[(S + 2) % 5][f];
-        dxyz[2] = d1_4(w[S % 5][f], w[(S + 1) % 5][f], w[(S + 3) % 5][f], w[(S + 4) % 5][f],
-                       siz);
+        if constexpr (XA)
+          dxyz[2] = xa::dq(w[S % 5][f], w[(S + 1) % 5][f], w[(S + 3) % 5][f], w[(S + 4) % 5][f]);
+        else
+          dxyz[2] = d1_4(w[S % 5][f], w[(S + 1) % 5][f], w[(S + 3) % 5][f], w[(S + 4) % 5][f],
+                         siz);
+      };
+      // curl and divergence of one vector field from its derivatives; in the
+      // reference arithmetic the curl's first product is rounded and its
+      // second fused (rk_step, field_solver_EZ.cpp:143-150)
+      auto curl_div = [&](const T* xd, const T* yd, const T* zd, T* rot, T& dvg) {
+        if constexpr (XA) {
+          rot[0] = xa::fma(-iz, yd[2], xa::mul(iy, zd[1]));
+          rot[1] = xa::fma(-ix, zd[0], xa::mul(iz, xd[2]));
+          rot[2] = xa::fma(-iy, xd[1], xa::mul(ix, yd[0]));
+          dvg = xa::fma(iz, zd[2], xa::fma(iy, yd[1], xa::mul(ix, xd[0])));
+        } else {
+          rot[0] = zd[1] - yd[2];
+          rot[1] = xd[2] - zd[0];
+          rot[2] = yd[0] - xd[1];
+          dvg = xd[0] + yd[1] + zd[2];
+        }
       };
       {
         T bxd[3], byd[3], bzd[3];
         d1(std::integral_constant<int, 3>{}, bxd);
         d1(std::integral_constant<int, 4>{}, byd);
         d1(std::integral_constant<int, 5>{}, bzd);
-        dv.rotB[0] = bzd[1] - byd[2];
-        dv.rotB[1] = bxd[2] - bzd[0];
-        dv.rotB[2] = byd[0] - bxd[1];
-        dv.divB = bxd[0] + byd[1] + bzd[2];
+        curl_div(bxd, byd, bzd, dv.rotB, dv.divB);
       }
       __syncwarp(amask);
       {
@@ -458,13 +549,15 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
         d1(std::integral_constant<int, 0>{}, exd);
         d1(std::integral_constant<int, 1>{}, eyd);
         d1(std::integral_constant<int, 2>{}, ezd);
-        dv.rotE[0] = ezd[1] - eyd[2];
-        dv.rotE[1] = exd[2] - ezd[0];
-        dv.rotE[2] = eyd[0] - exd[1];
-        dv.divE = exd[0] + eyd[1] + ezd[2];
+        curl_div(exd, eyd, ezd, dv.rotE, dv.divE);
       }
       __syncwarp(amask);
       d1(std::integral_constant<int, 6>{}, dv.gradP);
+      if constexpr (XA) {
+        dv.gradP[0] = xa::mul(ix, dv.gradP[0]);
+        dv.gradP[1] = xa::mul(iy, dv.gradP[1]);
+        dv.gradP[2] = xa::mul(iz, dv.gradP[2]);
+      }
       if constexpr (!FIRST) {
         const uint32_t ad = dme + dslot(sc, Z{}, k);
         static_for<7>([&](auto fc) {
@@ -472,7 +565,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
           dold[f] = lds<T, f * DFB>(ad);
         });
       }
-      stage_point<T, FIRST, BC>(c, u, dv, dold, As, Bs, tst, flags, col, k,
+      stage_point<T, FIRST, BC, XA>(c, u, dv, dold, As, Bs, tst, flags, col, k,
                                 (uint32_t)k * sz + own, du, un, aux, uout);
       if constexpr (ZU == 1) {
 #pragma unroll
@@ -546,7 +639,7 @@ constexpr size_t ko_smem_bytes() {
   return (size_t)ko_ring<BC, PF>() * 7 * TileLoader<T, TX, TY, 3, V>::FB;
 }
 
-template <typename T, int TX, int TY, int PF, bool BC, int V>
+template <typename T, int TX, int TY, int PF, bool BC, int V, bool XA>
 __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     ez_ko_kernel(const __grid_constant__ EzConst<T> c, const F7<const T> uin,
                  const F7<T> uout, const T tko, const int kchunk) {
@@ -569,7 +662,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
   const bool active = (i < g.hi[0]) && (j < g.hi[1]);
   const uint32_t sz = (uint32_t)g.sz;
   const uint32_t own = (uint32_t)j * (uint32_t)g.sy + (uint32_t)i;
-  const ColumnCtx<T> col = make_column(c, i, j);
+  const ColumnCtx<T> col = make_column<XA>(c, i, j);
   const L loader(g, sbase, tid, g.lo[0] + (int)blockIdx.x * TX - 3,
                  g.lo[1] + (int)blockIdx.y * TY - 3);
   const int kend = k1 + 3;  // planes [k0, k1+3) pass through shared memory
@@ -616,21 +709,29 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
         w[(S + 6) % 7][f] = lds<T, o + CEN>(a3);
         const T cv = w[(S + 3) % 7][f];
         if (f < 6 || ko_p) {
-          const T kx = d6_2(lds<T, o + CEN - 3 * ES>(a0), lds<T, o + CEN - 2 * ES>(a0),
-                            lds<T, o + CEN - ES>(a0), cv, lds<T, o + CEN + ES>(a0),
-                            lds<T, o + CEN + 2 * ES>(a0), lds<T, o + CEN + 3 * ES>(a0));
-          const T ky = d6_2(lds<T, o + 3 * ES>(a0), lds<T, o + (SX + 3) * ES>(a0),
-                            lds<T, o + (2 * SX + 3) * ES>(a0), cv,
-                            lds<T, o + (4 * SX + 3) * ES>(a0), lds<T, o + (5 * SX + 3) * ES>(a0),
-                            lds<T, o + (6 * SX + 3) * ES>(a0));
-          const T kz = d6_2(w[S % 7][f], w[(S + 1) % 7][f], w[(S + 2) % 7][f], cv,
-                            w[(S + 4) % 7][f], w[(S + 5) % 7][f], w[(S + 6) % 7][f]);
-          nu[f] = fma(kx + ky + kz, c.ko_c, cv);
+          auto d6 = [](T m3, T m2, T m1, T c0, T p1, T p2, T p3) {
+            if constexpr (XA) return xa::d6(m3, m2, m1, c0, p1, p2, p3);
+            else return d6_2(m3, m2, m1, c0, p1, p2, p3);
+          };
+          const T kx = d6(lds<T, o + CEN - 3 * ES>(a0), lds<T, o + CEN - 2 * ES>(a0),
+                          lds<T, o + CEN - ES>(a0), cv, lds<T, o + CEN + ES>(a0),
+                          lds<T, o + CEN + 2 * ES>(a0), lds<T, o + CEN + 3 * ES>(a0));
+          const T ky = d6(lds<T, o + 3 * ES>(a0), lds<T, o + (SX + 3) * ES>(a0),
+                          lds<T, o + (2 * SX + 3) * ES>(a0), cv,
+                          lds<T, o + (4 * SX + 3) * ES>(a0), lds<T, o + (5 * SX + 3) * ES>(a0),
+                          lds<T, o + (6 * SX + 3) * ES>(a0));
+          const T kz = d6(w[S % 7][f], w[(S + 1) % 7][f], w[(S + 2) % 7][f], cv,
+                          w[(S + 4) % 7][f], w[(S + 5) % 7][f], w[(S + 6) % 7][f]);
+          // the reference arithmetic sums the axes x, y, z left to right and
+          // fuses f + KO (-KOeps KO_const) (field_solver_EZ.cpp:350-420)
+          if constexpr (XA) nu[f] = xa::fma(c.ko_c, xa::add(xa::add(kx, ky), kz), cv);
+          else nu[f] = fma(kx + ky + kz, c.ko_c, cv);
         } else {
           nu[f] = cv;
         }
       });
-      apply_clamps(c, nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
+      if constexpr (XA) apply_clamps_xa(nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
+      else apply_clamps(c, nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
       if constexpr (BC) star_boundary(c, i, j, k, tko, nu);
       store_with_images(g, col, uout, k, (uint32_t)k * sz + own, nu);
       if constexpr (ZU == 1) {

@@ -185,16 +185,17 @@ inline bool flat_needs_bc(const coffee_params& p, int semantics) {
 struct FlatLaunch {
   bool bc;   // star / absorbing-layer code compiled in
   bool vec;  // planes copied as aligned element pairs (even row length d0)
+  bool xa;   // the CPU build's own arithmetic (CPU semantics, ez_refarith.cuh)
   int kchunk_stage, kchunk_ko;
   dim3 grid_stage, grid_ko;
 };
 
-template <typename T, bool BC, int V>
+template <typename T, bool BC, int V, bool XA>
 struct FlatKernels {
   using S = Shape<T>;
-  static constexpr auto first = ez_stage_kernel<T, S::STX, S::STY, S::SPF, true, BC, V>;
-  static constexpr auto rest = ez_stage_kernel<T, S::STX, S::STY, S::SPF, false, BC, V>;
-  static constexpr auto ko = ez_ko_kernel<T, S::KTX, S::KTY, S::KPF, BC, V>;
+  static constexpr auto first = ez_stage_kernel<T, S::STX, S::STY, S::SPF, true, BC, V, XA>;
+  static constexpr auto rest = ez_stage_kernel<T, S::STX, S::STY, S::SPF, false, BC, V, XA>;
+  static constexpr auto ko = ez_ko_kernel<T, S::KTX, S::KTY, S::KPF, BC, V, XA>;
 
   static cudaError_t set_attributes() {
     cudaError_t e = cudaFuncSetAttribute(first, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -232,27 +233,47 @@ struct FlatKernels {
   }
 };
 
-// Calls fn(FlatKernels<T, BC, V>{}) for the kernel set L selects.
+// Calls fn(FlatKernels<T, BC, V, XA>{}) for the kernel set L selects.
+template <typename T, bool XA, class Fn>
+inline void with_flat_kernels_xa(const FlatLaunch& L, Fn&& fn) {
+  if (L.bc) {
+    if (L.vec) fn(FlatKernels<T, true, 2, XA>{});
+    else fn(FlatKernels<T, true, 1, XA>{});
+  } else {
+    if (L.vec) fn(FlatKernels<T, false, 2, XA>{});
+    else fn(FlatKernels<T, false, 1, XA>{});
+  }
+}
 template <typename T, class Fn>
 inline void with_flat_kernels(const FlatLaunch& L, Fn&& fn) {
-  if (L.bc) {
-    if (L.vec) fn(FlatKernels<T, true, 2>{});
-    else fn(FlatKernels<T, true, 1>{});
-  } else {
-    if (L.vec) fn(FlatKernels<T, false, 2>{});
-    else fn(FlatKernels<T, false, 1>{});
-  }
+  if (L.xa) with_flat_kernels_xa<T, true>(L, fn);
+  else with_flat_kernels_xa<T, false>(L, fn);
 }
 
 // Set the shared-memory limits of every flat kernel of precision T on the
 // current device and plan the launch geometry of `env`'s grid.
+// reference_arith: the CPU semantics run in the CPU build's own arithmetic
+// (the default); false selects the regrouped, faster arithmetic.
 template <typename T>
-inline int flat_plan(const coffee_env* env, int semantics, FlatLaunch* L) {
+inline int flat_plan(const coffee_env* env, int semantics, FlatLaunch* L,
+                     bool reference_arith = true) {
   using S = Shape<T>;
-  COFFEE_CUDA_TRY((FlatKernels<T, true, 1>::set_attributes()));
-  COFFEE_CUDA_TRY((FlatKernels<T, false, 1>::set_attributes()));
-  COFFEE_CUDA_TRY((FlatKernels<T, true, 2>::set_attributes()));
-  COFFEE_CUDA_TRY((FlatKernels<T, false, 2>::set_attributes()));
+  L->bc = flat_needs_bc(env->p, semantics);
+  L->vec = env->grid.dims[0] % 2 == 0;
+  L->xa = reference_arith && semantics == SEM_CPU_REF;
+  // the shared-memory limits of the four kernel sets of this arithmetic (a
+  // caller may still switch the pair copies off, as coffee_noalloc.cu does)
+  if (L->xa) {
+    COFFEE_CUDA_TRY((FlatKernels<T, true, 1, true>::set_attributes()));
+    COFFEE_CUDA_TRY((FlatKernels<T, false, 1, true>::set_attributes()));
+    COFFEE_CUDA_TRY((FlatKernels<T, true, 2, true>::set_attributes()));
+    COFFEE_CUDA_TRY((FlatKernels<T, false, 2, true>::set_attributes()));
+  } else {
+    COFFEE_CUDA_TRY((FlatKernels<T, true, 1, false>::set_attributes()));
+    COFFEE_CUDA_TRY((FlatKernels<T, false, 1, false>::set_attributes()));
+    COFFEE_CUDA_TRY((FlatKernels<T, true, 2, false>::set_attributes()));
+    COFFEE_CUDA_TRY((FlatKernels<T, false, 2, false>::set_attributes()));
+  }
   // the flat kernels index an array with 32-bit element offsets (an FP32
   // array of 2^31 points alone would take a twentieth of the GPU's memory,
   // and a run holds at least 21 of them)
@@ -261,8 +282,6 @@ inline int flat_plan(const coffee_env* env, int semantics, FlatLaunch* L) {
   if (npts >= (1LL << 31))
     return fail(COFFEE_E_CONFIG, "%lld points per array: the flat solver takes fewer than 2^31",
                 npts);
-  L->bc = flat_needs_bc(env->p, semantics);
-  L->vec = env->grid.dims[0] % 2 == 0;
   int per_sm_stage = 1, per_sm_ko = 1;
   cudaError_t occ = cudaSuccess;
   with_flat_kernels<T>(*L, [&](auto K) { occ = decltype(K)::occupancy(&per_sm_stage, &per_sm_ko); });

@@ -5,6 +5,7 @@
 #pragma once
 
 #include "ez_common.cuh"
+#include "ez_refarith.cuh"
 
 namespace coffee {
 
@@ -39,6 +40,26 @@ __device__ __forceinline__ void apply_clamps(const EzConst<T>& c, T& ex, T& ey, 
       ey *= s;
       ez *= s;
     }
+  }
+}
+
+// The CPU build's clean_epar_check_eGTb in that build's own arithmetic
+// (field_solver_EZ.cpp:552-634; the rounding and fusing rules are those of
+// ez_refarith.cuh): E -= ((E.B) B_a) / B^2 per component, then, where
+// |E|^2 > B^2, E *= sqrt(B^2 / |E|^2).
+template <typename T>
+__device__ __forceinline__ void apply_clamps_xa(T& ex, T& ey, T& ez, T bx, T by, T bz) {
+  const T B2 = xa::floor_tiny(xa::dot3(bx, bx, by, by, bz, bz));
+  const T EB = xa::dot3(bx, ex, by, ey, bz, ez);
+  ex = xa::sub(ex, xa::div(xa::mul(EB, bx), B2));
+  ey = xa::sub(ey, xa::div(xa::mul(EB, by), B2));
+  ez = xa::sub(ez, xa::div(xa::mul(EB, bz), B2));
+  const T E2 = xa::dot3(ex, ex, ey, ey, ez, ez);
+  if (E2 > B2) {
+    const T s = xa::sqrt(xa::div(B2, E2));
+    ex = xa::mul(ex, s);
+    ey = xa::mul(ey, s);
+    ez = xa::mul(ez, s);
   }
 }
 
@@ -313,7 +334,7 @@ template <typename T>
 struct ColumnCtx {
   int i, j;
   bool xy_simple;  // the point writes only itself along x and y (no guard image)
-  T taper_x, taper_y, taper_dz;
+  T taper_x, taper_y, taper_dz;  // (reference arithmetic: taper_dz holds the lane)
 };
 
 // The P-gradient taper of the CPU build's rk_step
@@ -363,7 +384,17 @@ __device__ __forceinline__ bool only_self(const GridGeom& g, int axis, int i) {
   return i >= 2 * gd && i < g.dims[axis] - 2 * gd;
 }
 
+// The same taper in the CPU build's own arithmetic (ez_refarith.cuh):
+// coordinates by two FMAs each, r = sqrt(x x + y y + z z) with the last two
+// products fused, and the vectorclass tanh.
 template <typename T>
+__device__ __forceinline__ T p_taper_xa(const EzConst<T>& c, const ColumnCtx<T>& col, int k) {
+  const T z = xa::lane_pos(c.delta[2], c.lower[2], k - c.g.guard[2], col.taper_dz);
+  const T r = xa::sqrt(xa::dot3(col.taper_x, col.taper_x, col.taper_y, col.taper_y, z, z));
+  return xa::taper_of_r(r);
+}
+
+template <bool XA, typename T>
 __device__ __forceinline__ ColumnCtx<T> make_column(const EzConst<T>& c, int i, int j) {
   ColumnCtx<T> col;
   col.i = i;
@@ -371,9 +402,15 @@ __device__ __forceinline__ ColumnCtx<T> make_column(const EzConst<T>& c, int i, 
   col.xy_simple = only_self(c.g, 0, i) && only_self(c.g, 1, j);
   const int lane = (i - c.g.lo[0]) % c.taper_lanes;
   const T fl = (T)lane;
-  col.taper_x = fl * c.delta[0] + grid_pos(c, 0, i - lane);
-  col.taper_y = fl * c.delta[1] + grid_pos(c, 1, j);
-  col.taper_dz = fl * c.delta[2];
+  if constexpr (XA) {
+    col.taper_x = xa::lane_pos(c.delta[0], c.lower[0], i - lane - c.g.guard[0], fl);
+    col.taper_y = xa::lane_pos(c.delta[1], c.lower[1], j - c.g.guard[1], fl);
+    col.taper_dz = fl;
+  } else {
+    col.taper_x = fl * c.delta[0] + grid_pos(c, 0, i - lane);
+    col.taper_y = fl * c.delta[1] + grid_pos(c, 1, j);
+    col.taper_dz = fl * c.delta[2];
+  }
   return col;
 }
 

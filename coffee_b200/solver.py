@@ -205,6 +205,15 @@ class FieldSolverEZ:
     def set_aux(self, enable: bool):
         check(self.lib.coffee_solver_set_aux(self.handle, int(bool(enable))))
 
+    def set_arithmetic(self, mode: str):
+        """'reference' (the default): the CPU semantics compute every
+        operation of the reference CPU build in its order and rounding, so an
+        FP32 run gives the float build's fields bit for bit (star and
+        absorbing boundaries agree to rounding).  'fast': the same algorithm
+        regrouped for fewer instructions, equal to rounding."""
+        m = {"reference": 0, "fast": 1}[mode]
+        check(self.lib.coffee_solver_set_arithmetic(self.handle, m))
+
     def set_timing(self, enable: bool):
         check(self.lib.coffee_solver_set_timing(self.handle, int(bool(enable))))
 
@@ -263,13 +272,15 @@ class FieldSolverEZ:
 
 
 def run_flat(params: SimParams, fields, nsteps: int, time0: float = 0.0, semantics: str = "cpu",
-             aux: bool = False, device: int = 0):
+             aux: bool = False, device: int = 0, arithmetic: str = "reference"):
     """Upload ``fields``, advance ``nsteps`` on the GPU, return the 7 fields
     (and J, divE, divB when ``aux``)."""
     env = SimEnvironment(params, device)
     data = SimData(env, fields[0].dtype)
     data.upload(fields)
     solver = FieldSolverEZ(data, env, semantics)
+    if arithmetic != "reference":
+        solver.set_arithmetic(arithmetic)
     if aux:
         solver.set_aux(True)
     solver.step(time0, nsteps)

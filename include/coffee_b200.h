@@ -211,6 +211,25 @@ COFFEE_API int coffee_solver_step(coffee_solver* s, double time, int nsteps);
  * default: they cost 20 bytes per cell per stage).  The staggered solver
  * has no such outputs (COFFEE_E_INVALID). */
 COFFEE_API int coffee_solver_set_aux(coffee_solver* s, int enable);
+enum { /* arithmetic of the flat EZ solver (coffee_solver_set_arithmetic) */
+  COFFEE_ARITH_REFERENCE = 0, /* the default.  CPU semantics: every operation of the
+                               * reference CPU build's rk_step, Kreiss_Oliger and
+                               * clean_epar_check_eGTb (field_solver_EZ.cpp:105-634) in
+                               * its order and rounding, including the fused
+                               * multiply-adds its compiler forms and its vector
+                               * library's tanh, so that FP32 runs give the float
+                               * build's fields bit for bit (the star and absorbing
+                               * boundaries agree to rounding).  GPU semantics: as
+                               * COFFEE_ARITH_FAST. */
+  COFFEE_ARITH_FAST = 1       /* the same algorithm with the derivatives and the current
+                               * regrouped for fewer instructions (reciprocal-based
+                               * division, one exponential in the taper); agrees with
+                               * COFFEE_ARITH_REFERENCE to rounding */
+};
+/* Select the arithmetic of a flat solver's following steps (no counterpart
+ * in the reference, which has one arithmetic per build).  The other
+ * variants have only COFFEE_ARITH_REFERENCE. */
+COFFEE_API int coffee_solver_set_arithmetic(coffee_solver* s, int mode);
 /* Bracket every kernel launch of the following coffee_solver_step calls with
  * CUDA events on the solver's stream (1) or not (0, the default). */
 COFFEE_API int coffee_solver_set_timing(coffee_solver* s, int enable);
@@ -299,8 +318,13 @@ COFFEE_API int coffee_batch_destroy(coffee_batch* b);
  * 64^3 interior with 3 guards, 70^3 = 343,000 points); larger grids are
  * rejected with COFFEE_E_INVALID.  It calls no cudaMalloc or cudaFree.  The
  * first call on a device looks up the array's device address for that
- * device; make that first call before any stream capture.  All calls share
- * the one array: calls that overlap on the GPU (other streams, other host
+ * device and keeps it for the life of the process: it belongs to the
+ * device's primary context, so it is stale after cudaDeviceReset (do not
+ * call this after resetting the device).  The first call also loads the
+ * kernels' code, which may allocate and synchronise inside the driver:
+ * make it once outside the caller's critical pipeline, and before any
+ * stream capture.  All calls share the one array, which keeps the last
+ * call's contents: calls that overlap on the GPU (other streams, other host
  * threads) race.  J, divE and divB are not produced. */
 COFFEE_API int coffee_evolve_noalloc(const coffee_params* p, int semantics,
                                      float* const fields[7], double time, int nsteps,

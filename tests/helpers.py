@@ -64,3 +64,22 @@ def fp32_parity(out, ref32, ref64_same_algo, names=NAMES):
         rep.append(f"{names[f]}: vs ref32 {vs32:.2e} (bar {bar32:.1e}) vs fp64 {vs64:.2e} "
                    f"(ref32 noise {noise:.2e}, bar {bar64:.1e}){'' if good else '  <-- FAIL'}")
     return ok, "\n".join(rep)
+
+
+def wide_box_case():
+    """A periodic turbulence box of side 7.3 around the origin, 16^3: the
+    CPU build's P-gradient taper (argument 2 (r - 3)) then spans both
+    branches of its tanh, the polynomial one (|arg| <= 5/8) and the
+    exponential one, and the grid is incommensurate with the modes."""
+    from coffee_b200 import problems
+
+    p = problems.turbulence_params(16)
+    p.lower = [-3.65, -3.4, -3.9]
+    p.size = [7.3, 7.3, 7.3]
+    p.dt = 0.5 * 7.3 / 16
+    return p, problems.turbulence_fields(p, np.float32)
+
+
+def count_differing(a, b):
+    """Number of points whose values differ (0 and -0 count as equal)."""
+    return int(np.count_nonzero(np.asarray(a) != np.asarray(b)))

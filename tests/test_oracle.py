@@ -4,7 +4,8 @@ reference's own CPU build, through the committed golden fixtures
 import numpy as np
 import pytest
 
-from helpers import fp32_parity, golden_cases, load_golden, rel_l2
+from helpers import (count_differing, fp32_parity, golden_cases, load_golden, rel_l2,
+                     wide_box_case)
 from oracle import oracle
 
 
@@ -77,3 +78,14 @@ def test_port_matches_reference_shifted_box():
     out, _ = oracle.run_port(p, f64, 3, taper_lanes=8)
     for f in range(7):
         assert rel_l2(out[f], ref[f]) < 1e-11
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="oracle/_ref not built")
+def test_port_is_the_reference_across_the_taper():
+    """A fresh case from the reference float build itself: a box around the
+    origin where the taper's tanh takes both of its branches."""
+    p, f32 = wide_box_case()
+    ref, _, _ = oracle.run_reference(p, f32, 3)
+    out, _ = oracle.run_port(p, f32, 3, taper_lanes=16)
+    for f in range(7):
+        assert count_differing(out[f], ref[f]) == 0, (f, rel_l2(out[f], ref[f]))

@@ -4,9 +4,11 @@ that cannot take the device synchronisation an allocation may cause.
 
 It is called through the C ABI on device arrays the test owns, twice in a
 row (the static scratch keeps the first call's contents), and each result is
-compared with coffee_solver_step on the same fields.  The file is named to be
-collected last; it passes alone in a fresh process and after the other
-tests."""
+compared with coffee_solver_step on the same fields: the two run the same
+kernels on the same inputs, so the fields must be equal bit for bit.  The
+second call must leave the device's free memory unchanged.  The file is
+named to be collected last; it passes alone in a fresh process and after
+the other tests."""
 import ctypes
 
 import numpy as np
@@ -14,9 +16,35 @@ import pytest
 
 from coffee_b200 import _lib, problems
 from coffee_b200.solver import FieldSolverEZ, SimData, SimEnvironment, to_coffee_params
-from helpers import REL_FLOOR, rel_l2
+from helpers import rel_l2
 
 pytestmark = pytest.mark.gpu
+
+
+def _cudart():
+    for name in ("libcudart.so", "libcudart.so.12"):
+        try:
+            return ctypes.CDLL(name)
+        except OSError:
+            continue
+    import glob
+    import os
+
+    import torch  # the wheel ships the runtime next to torch's own libraries
+    for path in glob.glob(os.path.join(os.path.dirname(torch.__file__), "..", "nvidia",
+                                       "cuda_runtime", "lib", "libcudart.so*")):
+        return ctypes.CDLL(path)
+    raise OSError("libcudart not found")
+
+
+def _free_device_bytes():
+    free, total = ctypes.c_size_t(), ctypes.c_size_t()
+    assert _cudart().cudaMemGetInfo(ctypes.byref(free), ctypes.byref(total)) == 0
+    return free.value
+
+
+def _sync():
+    assert _cudart().cudaDeviceSynchronize() == 0
 
 
 def _noalloc(lib, params, ptrs, time, nsteps):
@@ -53,13 +81,18 @@ def test_noalloc_matches_solver_twice():
     lib = env.lib
     _noalloc(lib, cp, ptrs, 0.0, 2)
     got1 = own.download()
+    free0 = _free_device_bytes()
     _noalloc(lib, cp, ptrs, float(t1b), 1)
+    _sync()
+    free1 = _free_device_bytes()
     got2 = own.download()
     assert t2 > 0
+    assert free1 == free0, f"the second call changed free device memory by {free0 - free1} bytes"
     for name, got, ref in (("first call", got1, ref1), ("second call", got2, ref2)):
         for k in range(7):
             err = rel_l2(got[k], ref[k])
-            assert err <= REL_FLOOR, f"{name}: field {k} differs from coffee_solver_step ({err:.2e})"
+            assert np.array_equal(got[k], ref[k]), \
+                f"{name}: field {k} differs from coffee_solver_step (rel L2 {err:.2e})"
     solver.close()
     own.close()
     ref_data.close()
