@@ -98,6 +98,7 @@ SIGNATURES = {
     "coffee_solver_step": (_i, [_vp, _d, _i]),
     "coffee_solver_set_aux": (_i, [_vp, _i]),
     "coffee_solver_set_arithmetic": (_i, [_vp, _i]),
+    "coffee_solver_set_taper_lanes": (_i, [_vp, _i]),
     "coffee_solver_set_timing": (_i, [_vp, _i]),
     "coffee_solver_last_timing": (_i, [_vp, _P(_d), _P(_i), _P(_d)]),
     "coffee_fields_init_fourier": (_i, [_vp, _P(_d), _i, _P(_d), _P(_d), _P(_d), _i, _P(_d),

@@ -65,6 +65,7 @@ struct coffee_solver {
   int aux;
   int timing;
   int arith;    // COFFEE_ARITH_* of the flat solver
+  int taper_lanes;  // SIMD lanes of the CPU build's taper (0: by precision)
   uint64_t synced_generation;
   FlatLaunch launch;
   void* vtab;  // tables / scratch of a non-Cartesian variant (device), or null
@@ -599,6 +600,7 @@ extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int varia
   s->aux = 0;
   s->timing = 0;
   s->arith = COFFEE_ARITH_REFERENCE;
+  s->taper_lanes = 0;
   s->events_used = 0;
   s->synced_generation = 0;
   // the GR solver's inner absorbing region always needs the start-of-step
@@ -710,6 +712,16 @@ extern "C" int coffee_solver_set_arithmetic(coffee_solver* s, int mode) {
   return rc;
 }
 
+extern "C" int coffee_solver_set_taper_lanes(coffee_solver* s, int lanes) {
+  clear_error();
+  if (!s) return fail(COFFEE_E_INVALID, "coffee_solver_set_taper_lanes: null argument");
+  if (lanes < 0 || lanes > 64) return fail(COFFEE_E_INVALID, "taper lanes %d not in 0..64", lanes);
+  if (s->variant != COFFEE_VARIANT_FLAT)
+    return fail(COFFEE_E_INVALID, "only the flat EZ solver has the CPU build's taper");
+  s->taper_lanes = lanes;
+  return COFFEE_OK;
+}
+
 extern "C" int coffee_solver_set_timing(coffee_solver* s, int enable) {
   if (!s) return fail(COFFEE_E_INVALID, "coffee_solver_set_timing: null argument");
   s->timing = enable ? 1 : 0;
@@ -767,6 +779,7 @@ template <typename T>
 static int run_steps(coffee_solver* s, double time, int nsteps) {
   EzConst<T> c;
   build_const<T>(s->env, s->semantics, &c);
+  if (s->taper_lanes > 0) c.taper_lanes = s->taper_lanes;
   coffee_fields* f = s->f;
   cudaStream_t st = s->stream;
   const size_t bytes = f->n * f->elem;

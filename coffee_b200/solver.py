@@ -214,6 +214,12 @@ class FieldSolverEZ:
         m = {"reference": 0, "fast": 1}[mode]
         check(self.lib.coffee_solver_set_arithmetic(self.handle, m))
 
+    def set_taper_lanes(self, lanes: int):
+        """SIMD width of the CPU build's P-gradient taper offsets (0: by
+        precision, 16 for float and 8 for double as in the reference's two
+        builds)."""
+        check(self.lib.coffee_solver_set_taper_lanes(self.handle, int(lanes)))
+
     def set_timing(self, enable: bool):
         check(self.lib.coffee_solver_set_timing(self.handle, int(bool(enable))))
 

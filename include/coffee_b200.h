@@ -230,6 +230,13 @@ enum { /* arithmetic of the flat EZ solver (coffee_solver_set_arithmetic) */
  * in the reference, which has one arithmetic per build).  The other
  * variants have only COFFEE_ARITH_REFERENCE. */
 COFFEE_API int coffee_solver_set_arithmetic(coffee_solver* s, int mode);
+/* The SIMD width by which the CPU build's P-gradient taper offsets a point's
+ * x, y and z (field_solver_EZ.cpp:222-224): 16 in its float build, 8 in its
+ * double build (AVX-512), so the two builds differ in more than rounding.
+ * 0 (the default) takes the width of the field precision; another value
+ * (1..64) runs a precision with the other build's width, e.g. FP64 with 16
+ * lanes as the exact counterpart of an FP32 run.  Flat solver only. */
+COFFEE_API int coffee_solver_set_taper_lanes(coffee_solver* s, int lanes);
 /* Bracket every kernel launch of the following coffee_solver_step calls with
  * CUDA events on the solver's stream (1) or not (0, the default). */
 COFFEE_API int coffee_solver_set_timing(coffee_solver* s, int enable);
