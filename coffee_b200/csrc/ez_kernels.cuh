@@ -497,15 +497,20 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
       Derivs<T> dv;
       // dxyz[a]: the derivative of field f along axis a, inv_delta-scaled;
       // in the reference arithmetic (XA) the unscaled quotient of diff1_4,
-      // which curl_div scales and combines as the CPU build does
-      auto d1 = [&](auto fc, T* dxyz) {
+      // which curl_div scales and combines as the CPU build does.  EX
+      // selects the exact division for the rare quotients the fast one
+      // flags in `tiny` (xa::div12_fast).
+      bool tiny = false;
+      auto d1 = [&](auto fc, auto ex, T* dxyz) {
         constexpr int f = decltype(fc)::value;
+        constexpr bool EX = decltype(ex)::value;
         constexpr int o = f * FB;
         if constexpr (XA) {
-          dxyz[0] = xa::dq(lds<T, o + CEN - 2 * ES>(a0), lds<T, o + CEN - ES>(a0),
-                           lds<T, o + CEN + ES>(a0), lds<T, o + CEN + 2 * ES>(a0));
-          dxyz[1] = xa::dq(lds<T, o + 2 * ES>(a0), lds<T, o + (SX + 2) * ES>(a0),
-                           lds<T, o + (3 * SX + 2) * ES>(a0), lds<T, o + (4 * SX + 2) * ES>(a0));
+          dxyz[0] = xa::dq<EX>(lds<T, o + CEN - 2 * ES>(a0), lds<T, o + CEN - ES>(a0),
+                               lds<T, o + CEN + ES>(a0), lds<T, o + CEN + 2 * ES>(a0), tiny);
+          dxyz[1] = xa::dq<EX>(lds<T, o + 2 * ES>(a0), lds<T, o + (SX + 2) * ES>(a0),
+                               lds<T, o + (3 * SX + 2) * ES>(a0),
+                               lds<T, o + (4 * SX + 2) * ES>(a0), tiny);
         } else {
           dxyz[0] = d1_4(lds<T, o + CEN - 2 * ES>(a0), lds<T, o + CEN - ES>(a0),
                          lds<T, o + CEN + ES>(a0), lds<T, o + CEN + 2 * ES>(a0), six);
@@ -515,7 +520,8 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
         w[(S + 4) % 5][f] = lds<T, o + CEN>(ap2);
         u[f] = w[(S + 2) % 5][f];
         if constexpr (XA)
-          dxyz[2] = xa::dq(w[S % 5][f], w[(S + 1) % 5][f], w[(S + 3) % 5][f], w[(S + 4) % 5][f]);
+          dxyz[2] = xa::dq<EX>(w[S % 5][f], w[(S + 1) % 5][f], w[(S + 3) % 5][f],
+                               w[(S + 4) % 5][f], tiny);
         else
           dxyz[2] = d1_4(w[S % 5][f], w[(S + 1) % 5][f], w[(S + 3) % 5][f], w[(S + 4) % 5][f],
                          siz);
@@ -536,23 +542,31 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
           dvg = xd[0] + yd[1] + zd[2];
         }
       };
-      {
-        T bxd[3], byd[3], bzd[3];
-        d1(std::integral_constant<int, 3>{}, bxd);
-        d1(std::integral_constant<int, 4>{}, byd);
-        d1(std::integral_constant<int, 5>{}, bzd);
-        curl_div(bxd, byd, bzd, dv.rotB, dv.divB);
-      }
-      __syncwarp(amask);
-      {
-        T exd[3], eyd[3], ezd[3];
-        d1(std::integral_constant<int, 0>{}, exd);
-        d1(std::integral_constant<int, 1>{}, eyd);
-        d1(std::integral_constant<int, 2>{}, ezd);
-        curl_div(exd, eyd, ezd, dv.rotE, dv.divE);
-      }
-      __syncwarp(amask);
-      d1(std::integral_constant<int, 6>{}, dv.gradP);
+      auto derivatives = [&](auto ex) {
+        {
+          T bxd[3], byd[3], bzd[3];
+          d1(std::integral_constant<int, 3>{}, ex, bxd);
+          d1(std::integral_constant<int, 4>{}, ex, byd);
+          d1(std::integral_constant<int, 5>{}, ex, bzd);
+          curl_div(bxd, byd, bzd, dv.rotB, dv.divB);
+        }
+        __syncwarp(amask);
+        {
+          T exd[3], eyd[3], ezd[3];
+          d1(std::integral_constant<int, 0>{}, ex, exd);
+          d1(std::integral_constant<int, 1>{}, ex, eyd);
+          d1(std::integral_constant<int, 2>{}, ex, ezd);
+          curl_div(exd, eyd, ezd, dv.rotE, dv.divE);
+        }
+        __syncwarp(amask);
+        d1(std::integral_constant<int, 6>{}, ex, dv.gradP);
+      };
+      derivatives(std::false_type{});
+      // a quotient in the subnormal range (|t| < 2^-124, t != 0): the whole
+      // warp recomputes its derivatives with the exact division (the same
+      // operands are still in shared memory and the window)
+      if constexpr (XA)
+        if (__any_sync(amask, tiny)) derivatives(std::true_type{});
       if constexpr (XA) {
         dv.gradP[0] = xa::mul(ix, dv.gradP[0]);
         dv.gradP[1] = xa::mul(iy, dv.gradP[1]);

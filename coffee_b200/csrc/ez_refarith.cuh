@@ -39,29 +39,39 @@ __device__ __forceinline__ float sqrt(float a) { return __fsqrt_rn(a); }
 __device__ __forceinline__ double sqrt(double a) { return __dsqrt_rn(a); }
 
 // t / 12, correctly rounded.  FP32: q = t (1/12), then one Newton
-// correction with the exact residual t - 12 q (an FMA).  An exhaustive
-// check over every finite float shows this is the IEEE quotient for
-// |t| >= 2^-124; the rest (zeros, whose sign the correction can lose, and
-// tiny inputs whose quotient is subnormal) take the IEEE division.
-__device__ __forceinline__ float div12(float t) {
+// correction with the exact residual t - 12 q (an FMA), and the sign of t
+// (which the correction loses for t = -0).  An exhaustive check over every
+// finite float (on the CPU, with the same IEEE operations) shows that this
+// is the IEEE quotient for every t except 0 < |t| < 2^-124, whose quotient
+// is subnormal; `tiny` is set for those, and the caller recomputes them
+// with div12_exact.
+__device__ __forceinline__ float div12_fast(float t, bool& tiny) {
   constexpr float r12 = 1.0f / 12.0f;
   float q = __fmul_rn(t, r12);
   const float e = __fmaf_rn(-q, 12.0f, t);
-  q = __fmaf_rn(e, r12, q);
-  if (fabsf(t) < 0x1p-124f) q = __fdiv_rn(t, 12.0f);
+  q = copysignf(__fmaf_rn(e, r12, q), t);
+  tiny |= (fabsf(t) < 0x1p-124f) & (t != 0.0f);
   return q;
 }
-__device__ __forceinline__ double div12(double t) { return __ddiv_rn(t, 12.0); }
+__device__ __forceinline__ double div12_fast(double t, bool&) { return __ddiv_rn(t, 12.0); }
+__device__ __forceinline__ float div12_exact(float t) {
+  bool tiny = false;
+  const float q = div12_fast(t, tiny);
+  return tiny ? __fdiv_rn(t, 12.0f) : q;
+}
+__device__ __forceinline__ double div12_exact(double t) { return __ddiv_rn(t, 12.0); }
 
 // diff1_4 of the reference (finite_diff_simd.h:15-25) before its inv_delta
 // factor: (((f-2 - 8 f-1) + 8 f+1) - f+2) / 12, the two products by 8 fused
-// (they are exact, so fused or not gives the same value).
-template <typename T>
-__device__ __forceinline__ T dq(T m2, T m1, T p1, T p2) {
+// (they are exact, so fused or not gives the same value).  EXACT = false
+// flags in `tiny` the inputs whose fast quotient may be off (div12_fast).
+template <bool EXACT, typename T>
+__device__ __forceinline__ T dq(T m2, T m1, T p1, T p2, bool& tiny) {
   T t = fma(m1, (T)-8, m2);
   t = fma(p1, (T)8, t);
   t = sub(t, p2);
-  return div12(t);
+  if constexpr (EXACT) return div12_exact(t);
+  else return div12_fast(t, tiny);
 }
 
 // diff6_2 of the reference (finite_diff_simd.h:41-58): each weighted term
