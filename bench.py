@@ -152,6 +152,16 @@ def _slab_input(tmpdir, steps_dtype="f32"):
     return p, path, cfg
 
 
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_reference_run(steps: int, warmup: int, nproc: int | None = None):
     """Run the reference CPU build (or the restatement) on host cores.
 
@@ -241,6 +251,7 @@ def run_reference_arm(args):
     if rank != 0:
         return 0
     r = cpu_reference_run(args.steps, args.warmup)
+    one = cpu_reference_run(args.steps, args.warmup, nproc=1)
     line = {
         "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -248,12 +259,55 @@ def run_reference_arm(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded random force-free turbulence)",
         "config": {"workload": "turbulence512 (CPU sample: 512x512x8 slabs)", "grid": [512, 512, 512],
-                   "guard": 3, "periodic": True, "cfl": 0.5, "semantics": "reference CPU build"},
+                   "guard": 3, "periodic": True, "cfl": 0.5, "semantics": "reference CPU build",
+                   "aggregate": ("P-core aggregate proxy: one single-threaded reference process "
+                                 "per host core on its own periodic slab, no halo exchange")},
         "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
-                         "sample": r["sample"]},
+                         "sample": r["sample"], "cpu_model": cpu_model(),
+                         "one_core": {"value": one["value"], "unit": UNIT, "cores": 1,
+                                      "sample": one["sample"]}},
         "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_reference_gpu_arm(args):
+    """The reference's own GPU build of field_solver_EZ (compiled from its
+    sources into oracle/_ref/coffee_refgpu_float, single-rank device guard
+    fill) on the same turbulence problem: a second, GPU-side baseline."""
+    import numpy as np
+
+    from coffee_b200 import problems
+    from coffee_b200.solver import SimData, SimEnvironment
+    from oracle import oracle
+
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    p = problems.turbulence_params(args.n)
+    env = SimEnvironment(p)
+    data = SimData(env, np.float32)
+    data.init_fourier((1.0, 0.0, 0.0), *problems.turbulence_modes())
+    f = data.download()
+    data.close()
+    env.close()
+    # the reference's GPU build runs the GPU semantics (field_solver_EZ.cu)
+    _, _, info = oracle.run_reference_gpu("ez", p, f, args.steps, warmup=args.warmup,
+                                          timeout=3600)
+    cells = args.n ** 3
+    value = cells * args.steps / info["seconds"]
+    line = {"impl": "reference-gpu", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * info["seconds"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded random force-free turbulence, seed 20261203)",
+            "config": {"workload": f"turbulence{args.n}", "grid": [args.n] * 3, "guard": 3,
+                       "periodic": True, "cfl": 0.5,
+                       "semantics": "reference GPU build (field_solver_EZ.cu)",
+                       "build": ("oracle/_ref/coffee_refgpu_float: the reference's CUDA sources "
+                                 "compiled for sm_100a, guard fill on the device")}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -452,9 +506,13 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_reference_run(steps=2, warmup=1)
-        cpu = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": cpu["kind"],
-               "sample": cpu["sample"]}
+        agg = cpu_reference_run(steps=2, warmup=1)
+        one = cpu_reference_run(steps=2, warmup=1, nproc=1)
+        cpu = {"value": agg["value"], "unit": UNIT, "cores": agg["cores"], "kind": agg["kind"],
+               "sample": agg["sample"] + " (P-core aggregate proxy: no halo exchange)",
+               "cpu_model": cpu_model(),
+               "one_core": {"value": one["value"], "unit": UNIT, "cores": 1, "kind": one["kind"],
+                            "sample": one["sample"]}}
 
     if rank == 0:
         line = {
@@ -818,7 +876,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--impl", choices=["ours", "reference", "reference-gpu"], default="ours",
+                    help="reference-gpu: the reference's own GPU build on the turbulence problem")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fp64-steps", type=int, default=FP64_CHECK_STEPS,
                     help="length of the FP32-vs-FP64 comparison (rank 0, one GPU)")
@@ -845,6 +904,8 @@ def main():
         return run_variant(args)
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.impl == "reference-gpu":
+        return run_reference_gpu_arm(args)
     return run_ours(args)
 
 

@@ -181,7 +181,7 @@ def refgpu_binary(dtype=np.float32) -> str:
 
 
 def run_reference_gpu(solver: str, p: SimParams, fields, nsteps: int, time0: float = 0.0,
-                      aux: bool = False, timeout: float | None = 600):
+                      aux: bool = False, timeout: float | None = 600, warmup: int = 0):
     """Run the reference's own GPU build (oracle/ref_harness_gpu) of one of
     its solvers: "ez", "sph", "cyl" or "gr".  Needs a GPU.  Returns
     (fields, aux_or_None, info) like run_reference."""
@@ -196,6 +196,8 @@ def run_reference_gpu(solver: str, p: SimParams, fields, nsteps: int, time0: flo
         fout = os.path.join(wd, "out.fld")
         write_fld(fin, fields, guard=tuple(p.guard), time=time0)
         cmd = [exe, solver, fin, fout, str(int(nsteps))] + (["--aux"] if aux else [])
+        if warmup:
+            cmd += ["--warmup", str(int(warmup))]
         env = dict(os.environ, COFFEE_ORACLE_CONFIG=cfg)
         r = subprocess.run(cmd, cwd=wd, env=env, capture_output=True, text=True,
                            timeout=timeout)
