@@ -13,6 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcoffee_b200.so")
 
 COFFEE_OK = 0
+COFFEE_E_TIMEOUT = -6
 ERRORS = {
     -1: "COFFEE_E_INVALID", -2: "COFFEE_E_CONFIG", -3: "COFFEE_E_CUDA", -4: "COFFEE_E_NOMEM",
     -5: "COFFEE_E_NONFINITE", -6: "COFFEE_E_TIMEOUT", -7: "COFFEE_E_IO",
@@ -120,6 +121,7 @@ SIGNATURES = {
     "coffee_conv3d_forward_tc": (_i, [_vp, _i, _i, _i, _i, _i, _vp, _i, _vp, _vp, _vp, _i,
                                       ctypes.c_float, _vp]),
     "coffee_conv3d_tc_fault": (_i, [_P(_i), _i]),
+    "coffee_conv3d_tc_set_test_wait": (_i, [ctypes.c_longlong, _i]),
     "coffee_conv3d_flip_weights": (_i, [_vp, _i, _i, _vp, _vp]),
     "coffee_conv3d_backward_data": (_i, [_vp, _i, _i, _i, _i, _i, _vp, _i, _vp, _vp]),
     "coffee_conv3d_backward_weight_workspace": (ctypes.c_size_t, [_i, _i]),

@@ -465,10 +465,13 @@ int check_grid(int n, int d, int h, int w) {
 //     32 w .. 32 w + 31) and store.  Two accumulators in tensor memory let
 //     the epilogue of one tile overlap the MMAs of the next.
 //
-// Every wait is bounded (kTcWaitCycles) and also ends when another role of
-// the CTA has given up: a wait that runs out sets g_tc_fault, the roles stop
-// issuing work, the MMA thread waits (bounded) for what it committed, and
-// the CTA frees its tensor memory and returns.
+// Every wait is bounded (a cycle limit, kTcWaitCycles unless a test sets a
+// shorter one) and also ends when another role of the CTA has given up: a
+// wait that runs out sets g_tc_fault and the host-visible fault word, the
+// roles stop issuing work, the producer waits (with the full bound) for
+// every load it has in flight and the MMA thread for what it committed, and
+// the CTA frees its tensor memory and returns.  The launching call of the
+// next convolution reports COFFEE_E_TIMEOUT until the fault is cleared.
 constexpr int kTcM = 128;                         // points per tile = MMA M
 constexpr int kTcStages = 8;                      // A ring slots at most (32 KB of ring)
 constexpr int kTcRing = 32768;                    // bytes of the A ring
@@ -476,6 +479,15 @@ constexpr int kTcThreads = 192;                   // 4 epilogue warps, producer,
 constexpr long long kTcWaitCycles = 4000000000LL; // about 2 s at 1.9 GHz
 
 __device__ int g_tc_fault;
+
+// Launch parameters of the waits: the cycle limit, and (for the test of the
+// timeout path only) a producer that issues nothing, so that the MMA
+// thread's first wait runs out while no copy or MMA is in flight.
+struct TcWaitParams {
+  long long cycles;
+  int stall_producer;
+  int* fault;  // host-mapped word, set on a timeout, read by the launching calls
+};
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -504,7 +516,8 @@ __device__ __forceinline__ void tc_st16(uint32_t addr, uint4 v) {
 
 // Wait for the phase of parity `parity` of the mbarrier at `mbar`; false if
 // it did not complete within kTcWaitCycles or another role gave up (*abort).
-__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity, volatile int* abort) {
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity, volatile int* abort,
+                                        const TcWaitParams& wp) {
   const long long t0 = clock64();
   while (true) {
     uint32_t done;
@@ -516,11 +529,28 @@ __device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity, volatile
         : "memory");
     if (done) return true;
     if (*abort) return false;
-    if (clock64() - t0 > kTcWaitCycles) {
+    if (clock64() - t0 > wp.cycles) {
       *abort = 1;
       atomicExch(&g_tc_fault, 1);
+      if (wp.fault) atomicExch_system(wp.fault, 1);
       return false;
     }
+  }
+}
+
+// Wait (bounded by kTcWaitCycles) for the phase of parity `parity` of the
+// mbarrier at `mbar`, whatever the other roles do: the drain of work in flight.
+__device__ __forceinline__ void tc_drain_wait(uint32_t mbar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (clock64() - t0 < kTcWaitCycles) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return;
   }
 }
 
@@ -533,7 +563,7 @@ template <int N, int CB>
 __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
     const __grid_constant__ CUtensorMap xmap, Grid4 g, int C, const bf16* __restrict__ w,
     const float* __restrict__ bias, float* __restrict__ z, bf16* __restrict__ a, int act,
-    float slope, TcBox box) {
+    float slope, TcBox box, const TcWaitParams wp) {
   static_assert(N % 16 == 0 && N >= 16 && N <= 64, "N = 16, 32, 48 or 64");
   static_assert(CB == 16 || CB == 32 || CB == 64, "boxes of 16, 32 or 64 channels");
   constexpr int NCOLS = N <= 32 ? 32 : 64;  // columns of one accumulator (power of two >= 32)
@@ -611,14 +641,14 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
     if (lane == 0) {
       uint32_t step = 0;
       const uint64_t map = reinterpret_cast<uint64_t>(&xmap);
-      for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      for (long long t = blockIdx.x; t < ntiles && !wp.stall_producer; t += gridDim.x) {
         int n, x0, y0, z0;
         tile_origin(t, n, x0, y0, z0);
         bool ok = true;
         int tap = 0, q = 0;
         for (int s = 0; s < nstage && ok; ++s, ++step) {
           const uint32_t b = step % stages;
-          if (step >= stages && !tc_wait(empty0 + 8 * b, ((step / stages) - 1) & 1, abort)) {
+          if (step >= stages && !tc_wait(empty0 + 8 * b, ((step / stages) - 1) & 1, abort, wp)) {
             ok = false;
             break;
           }
@@ -640,20 +670,14 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
         }
         if (!ok) break;
       }
-      if (*abort && step > 0) {
-        // the loads already issued must land before the CTA's memory goes away
-        const uint32_t last = step - 1;
-        const long long t0 = clock64();
-        while (clock64() - t0 < kTcWaitCycles) {
-          uint32_t done;
-          asm volatile(
-              "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-              " selp.u32 %0, 1, 0, p;\n}\n"
-              : "=r"(done)
-              : "r"(full0 + 8 * (last % stages)), "r"((last / stages) & 1)
-              : "memory");
-          if (done) break;
-        }
+      if (*abort) {
+        // every load already issued must land before the CTA's memory goes
+        // away: the last `stages` steps are the only ones that can be in
+        // flight (a slot is reloaded only after its previous load was
+        // consumed), and each is the latest phase of its slot's barrier
+        const uint32_t first = step > stages ? step - stages : 0;
+        for (uint32_t s2 = first; s2 < step; ++s2)
+          tc_drain_wait(full0 + 8 * (s2 % stages), (s2 / stages) & 1);
       }
     }
   } else if (warp == 5) {
@@ -663,7 +687,7 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
       bool ok = true;
       for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++tiles) {
         const uint32_t acc = tiles & 1, use = tiles >> 1;
-        if (tiles >= 2 && !tc_wait(free0 + 8 * acc, (use - 1) & 1, abort)) {
+        if (tiles >= 2 && !tc_wait(free0 + 8 * acc, (use - 1) & 1, abort, wp)) {
           ok = false;
           break;
         }
@@ -673,7 +697,7 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
         int cq = 0;   // first channel of the stage's box
         for (int s = 0; s < nstage; ++s, ++step) {
           const uint32_t b = step % stages;
-          if (!tc_wait(full0 + 8 * b, (step / stages) & 1, abort)) {
+          if (!tc_wait(full0 + 8 * b, (step / stages) & 1, abort, wp)) {
             ok = false;
             break;
           }
@@ -704,19 +728,10 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
             : "memory");
       }
       if (!ok && step > 0) {
-        // what was committed must finish before the tensor memory is freed
+        // what was committed must finish before the tensor memory is freed:
+        // the commit of the last step tracks every MMA issued before it
         const uint32_t last = step - 1;
-        const long long t0 = clock64();
-        while (clock64() - t0 < kTcWaitCycles) {
-          uint32_t done;
-          asm volatile(
-              "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-              " selp.u32 %0, 1, 0, p;\n}\n"
-              : "=r"(done)
-              : "r"(empty0 + 8 * (last % stages)), "r"((last / stages) & 1)
-              : "memory");
-          if (done) break;
-        }
+        tc_drain_wait(empty0 + 8 * (last % stages), (last / stages) & 1);
       }
     }
   } else {
@@ -725,7 +740,7 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
     uint32_t tiles = 0;
     for (long long t = blockIdx.x; t < ntiles; t += gridDim.x, ++tiles) {
       const uint32_t acc = tiles & 1;
-      if (!tc_wait(ready0 + 8 * acc, (tiles >> 1) & 1, abort)) break;
+      if (!tc_wait(ready0 + 8 * acc, (tiles >> 1) & 1, abort, wp)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       uint32_t r[N];
 #pragma unroll
@@ -808,9 +823,37 @@ int pow2_at_least(int v) {
   return p;
 }
 
+// Wait parameters of the following launches (coffee_conv3d_tc_set_test_wait)
+// and the host-mapped fault word the kernels set on a timeout.
+long long g_tc_cycles = kTcWaitCycles;
+int g_tc_stall = 0;
+volatile int* g_tc_fault_host = nullptr;
+int* g_tc_fault_dev = nullptr;
+
+int tc_fault_word() {
+  if (g_tc_fault_host) return COFFEE_OK;
+  void* h = nullptr;
+  COFFEE_CUDA_TRY(cudaHostAlloc(&h, sizeof(int), cudaHostAllocMapped));
+  *static_cast<volatile int*>(h) = 0;
+  void* d = nullptr;
+  const cudaError_t err = cudaHostGetDevicePointer(&d, h, 0);
+  if (err != cudaSuccess) {
+    cudaFreeHost(h);
+    return fail(COFFEE_E_CUDA, "cudaHostGetDevicePointer: %s", cudaGetErrorString(err));
+  }
+  g_tc_fault_host = static_cast<volatile int*>(h);
+  g_tc_fault_dev = static_cast<int*>(d);
+  return COFFEE_OK;
+}
+
 template <int N>
 int launch_fwd_tc(const bf16* x, Grid4 g, int C, const bf16* w, const float* bias, float* z,
                   bf16* a, int act, float slope, cudaStream_t st) {
+  if (int rc = tc_fault_word()) return rc;
+  if (*g_tc_fault_host)
+    return fail(COFFEE_E_TIMEOUT,
+                "an earlier tcgen05 convolution ran out of time waiting on its pipeline "
+                "(its results are invalid); clear the fault with coffee_conv3d_tc_fault");
   const size_t smem = 1024 + (size_t)kTcRing + (size_t)27 * C * N * 2;
   // channels per TMA box: the widest that divides C; 48 channels in one
   // 64-channel box (the last 16 zero-filled, not multiplied)
@@ -862,7 +905,8 @@ int launch_fwd_tc(const bf16* x, Grid4 g, int C, const bf16* w, const float* bia
   per_sm = std::max(1, std::min(per_sm, 512 / (2 * (N <= 32 ? 32 : 64))));
   const long long ntiles = (long long)g.n * box.tx * box.ty * box.tz;
   const unsigned blocks = (unsigned)std::min<long long>(ntiles, (long long)sms * per_sm);
-  kern<<<blocks, kTcThreads, smem, st>>>(map, g, C, w, bias, z, a, act, slope, box);
+  const TcWaitParams wp{g_tc_cycles, g_tc_stall, g_tc_fault_dev};
+  kern<<<blocks, kTcThreads, smem, st>>>(map, g, C, w, bias, z, a, act, slope, box, wp);
   COFFEE_CUDA_TRY(cudaGetLastError());
   return COFFEE_OK;
 }
@@ -913,10 +957,20 @@ extern "C" int coffee_conv3d_tc_fault(int* fault, int clear) {
   clear_error();
   if (!fault) return fail(COFFEE_E_INVALID, "coffee_conv3d_tc_fault: null argument");
   COFFEE_CUDA_TRY(cudaMemcpyFromSymbol(fault, g_tc_fault, sizeof(int)));
+  if (g_tc_fault_host && *g_tc_fault_host) *fault = 1;
   if (clear) {
     const int zero = 0;
     COFFEE_CUDA_TRY(cudaMemcpyToSymbol(g_tc_fault, &zero, sizeof(int)));
+    if (g_tc_fault_host) *g_tc_fault_host = 0;
   }
+  return COFFEE_OK;
+}
+
+extern "C" int coffee_conv3d_tc_set_test_wait(long long cycles, int stall_producer) {
+  clear_error();
+  if (cycles < 0) return fail(COFFEE_E_INVALID, "wait limit must be >= 0 cycles");
+  g_tc_cycles = cycles > 0 ? cycles : kTcWaitCycles;
+  g_tc_stall = stall_producer ? 1 : 0;
   return COFFEE_OK;
 }
 

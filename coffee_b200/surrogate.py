@@ -28,7 +28,7 @@ import math
 import numpy as np
 
 from . import _lib, problems
-from ._lib import check
+from ._lib import CoffeeError, check
 
 SLOPE = 0.1
 CIN, C1, C2, COUT = 16, 16, 32, 16
@@ -82,6 +82,16 @@ def tc_fault(clear=True):
     flag = ctypes.c_int(0)
     check(_lib.load().coffee_conv3d_tc_fault(ctypes.byref(flag), int(clear)))
     return bool(flag.value)
+
+
+def check_tc():
+    """Raise if a tcgen05 convolution ran out of time since the last check
+    (synchronises).  A timeout also makes every later tcgen05 launch fail
+    with COFFEE_E_TIMEOUT, so a training loop stops at its next launch; this
+    covers the last launches of a run."""
+    if tc_fault(clear=False):
+        raise CoffeeError(_lib.COFFEE_E_TIMEOUT,
+                          "a tcgen05 convolution ran out of time: its results are invalid")
 
 
 def conv_backward_data(dy, wt_bf16, c, dx):
@@ -423,6 +433,7 @@ def train(net, samples, iters, lr=2e-3, log_every=50):
         net.step(rate)
         if it % log_every == 0 or it == iters - 1:
             losses.append((it, float(loss)))
+    check_tc()
     return losses
 
 
@@ -430,6 +441,7 @@ def predict(net, p, start, incl):
     torch = _torch()
     x = torch.from_numpy(features(p, start, incl)[None]).cuda().to(torch.bfloat16)
     out = net.forward(x)
+    check_tc()
     return apply_prediction(p, start, out[0].cpu().numpy())
 
 

@@ -41,9 +41,20 @@ COFFEE_API int coffee_conv3d_forward(const void* x, int n, int d, int h, int w, 
 COFFEE_API int coffee_conv3d_forward_tc(const void* x, int n, int d, int h, int w, int c,
                                         const void* weight, int k, const float* bias, float* z,
                                         void* a, int act, float slope, void* stream);
-/* *fault = 1 if a wait of the tcgen05 kernel ran out of time since the last
- * clear (its results are then invalid); clear != 0 resets it.  Synchronous. */
+/* Every pipeline wait of the tcgen05 kernel is bounded (about 2 s).  A wait
+ * that runs out makes the kernel drain what it has in flight, free its
+ * tensor memory and return with its results invalid; it sets a fault that
+ * every later coffee_conv3d_forward_tc call reports as COFFEE_E_TIMEOUT
+ * (without synchronising) until it is cleared.  coffee_conv3d_tc_fault:
+ * *fault = 1 if such a wait ran out since the last clear; clear != 0 resets
+ * it.  Synchronous. */
 COFFEE_API int coffee_conv3d_tc_fault(int* fault, int clear);
+/* Test hook of the timeout path (no counterpart in the reference): the
+ * following coffee_conv3d_forward_tc launches bound their waits by `cycles`
+ * GPU clock cycles (0 restores the default) and, with stall_producer != 0,
+ * issue no TMA loads at all, so that the MMA thread's first
+ * wait runs out while nothing is in flight. */
+COFFEE_API int coffee_conv3d_tc_set_test_wait(long long cycles, int stall_producer);
 /* wt (C, 27, K) = w (K, 27, C) with the taps reversed: the weights of the
  * transposed convolution. */
 COFFEE_API int coffee_conv3d_flip_weights(const void* weight, int k, int c, void* wt,

@@ -157,6 +157,47 @@ def test_tcgen05_forward_matches_oracle_and_mma_sync(c, k, shape):
 
 
 @pytest.mark.gpu
+def test_tcgen05_wait_that_runs_out_is_reported_and_recovers():
+    """A pipeline wait of the tcgen05 convolution that runs out.  The test
+    hook makes the producer issue no loads and bounds the waits at 20,000
+    cycles (about 10 us), so the MMA thread's first wait runs out while no
+    copy or MMA is in flight.  The kernel returns; the fault is reported by
+    coffee_conv3d_tc_fault and, without any synchronisation, as
+    COFFEE_E_TIMEOUT by the next launch; once it is cleared and the default
+    limit restored, a normal call gives the mma.sync kernel's result."""
+    from coffee_b200 import _lib
+    from coffee_b200 import surrogate as sg
+    torch = _torch()
+    lib = _lib.load()
+    rng = np.random.default_rng(11)
+    shape, c, k = (1, 8, 8, 8), 16, 16
+    x = co.bf16(rng.standard_normal(shape + (c,)))
+    w = co.bf16(rng.standard_normal((k, 27, c)) * 0.2)
+    xt, wt = _bf16_tensor(x), _bf16_tensor(w)
+    sg.tc_fault(clear=True)
+    z = torch.full(shape + (k,), float("nan"), dtype=torch.float32, device="cuda")
+    try:
+        _lib.check(lib.coffee_conv3d_tc_set_test_wait(20000, 1))
+        sg.conv_forward_tc(xt, wt, None, k, False, z, None)
+        torch.cuda.synchronize()
+        assert sg.tc_fault(clear=False)
+        with pytest.raises(_lib.CoffeeError) as err:
+            sg.conv_forward_tc(xt, wt, None, k, False, z, None)
+        assert "COFFEE_E_TIMEOUT" in str(err.value)
+        with pytest.raises(_lib.CoffeeError):
+            sg.check_tc()
+    finally:
+        lib.coffee_conv3d_tc_set_test_wait(0, 0)
+        sg.tc_fault(clear=True)
+    sg.conv_forward_tc(xt, wt, None, k, False, z, None)
+    z_ref = torch.empty_like(z)
+    sg.conv_forward(xt, wt, None, k, False, z_ref, None)
+    torch.cuda.synchronize()
+    assert not sg.tc_fault()
+    assert _rel(_np(z), _np(z_ref)) < 1e-5
+
+
+@pytest.mark.gpu
 def test_network_gradients_match_oracle():
     """Loss and every layer's gradients of the U-Net on the library's kernels
     against the FP64 restatement with the same BF16 rounding points."""
