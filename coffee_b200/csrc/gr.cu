@@ -2,6 +2,7 @@
 // for the constitutive fields E and H, and the step loop.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 
 #include "coffee_b200.h"
@@ -51,6 +52,25 @@ void fill_gr_const(const coffee_env* env, GrConst<T>* c) {
   c->r2 = (T)(0.01 * rH);
   c->dd = (T)(0.2 * rH);
   c->absorbing = 1;  // the inner layer always acts in the last stage
+  // the near-horizon box of the FP64 metric table: grid points within
+  // kNearRH r_H of the hole along every axis (possibly empty)
+  for (int a = 0; a < 3; ++a) {
+    const double lo = -kNearRH * rH, hi = kNearRH * rH;
+    int i0 = (int)std::ceil((lo - (double)g.lower[a]) / (double)g.delta[a]) + g.guard[a];
+    int i1 = (int)std::floor((hi - (double)g.lower[a]) / (double)g.delta[a]) + g.guard[a] + 1;
+    i0 = std::max(0, std::min(i0, g.dims[a]));
+    i1 = std::max(i0, std::min(i1, g.dims[a]));
+    c->nb_lo[a] = i0;
+    c->nb_n[a] = i1 - i0;
+  }
+}
+
+// points of the near-horizon metric table of env's grid
+template <typename T>
+size_t near_points(const coffee_env* env) {
+  GrConst<T> c;
+  fill_gr_const<T>(env, &c);
+  return (size_t)c.nb_n[0] * c.nb_n[1] * c.nb_n[2];
 }
 
 template <typename T>
@@ -79,6 +99,7 @@ int gr_steps_t(const coffee_env* env, void* ehbuf, void* const A_[7], void* cons
   for (int k = 0; k < 6; ++k) eh.p[k] = static_cast<T*>(ehbuf) + k * n;
   eh.p[6] = nullptr;
   const T* sgt = static_cast<const T*>(ehbuf) + 6 * n;  // sqrt(gamma), set up by gr_setup
+  const T* mt = sgt + n;                                 // the near-horizon metric table
   const dim3 gfull = grid_over(c.d[0], c.d[1], c.d[2]);
   const dim3 gbox = grid_over(c.hi[0] - c.lo[0], c.hi[1] - c.lo[1], c.hi[2] - c.lo[2]);
   for (int step = 0; step < nsteps; ++step) {
@@ -88,23 +109,23 @@ int gr_steps_t(const coffee_env* env, void* ehbuf, void* const A_[7], void* cons
       int flags = 0;
       if (s == 4) flags |= AX_LAST | (aux_ ? AX_AUX : 0);
       if (s == 0) flags |= AX_WRITE_UN;
-      gr_eh_kernel<T><<<gfull, kBlock, 0, st>>>(c, src, eh);
+      gr_eh_kernel<T><<<gfull, kBlock, 0, st>>>(c, src, eh, mt);
       COFFEE_CUDA_TRY(cudaGetLastError());
       const int kind = s == 0 ? COFFEE_KERNEL_STAGE_FIRST : COFFEE_KERNEL_STAGE;
       int rc = hook ? hook->before(kind) : COFFEE_OK;
       if (rc) return rc;
       if (s == 0)
-        gr_stage_kernel<T, true><<<gbox, kBlock, 0, st>>>(c, src, eh, dst, dU, Un, aux, sgt,
+        gr_stage_kernel<T, true><<<gbox, kBlock, 0, st>>>(c, src, eh, dst, dU, Un, aux, mt, sgt,
                                                           (T)kAs[s], (T)kBs[s], flags);
       else
-        gr_stage_kernel<T, false><<<gbox, kBlock, 0, st>>>(c, src, eh, dst, dU, Un, aux, sgt,
+        gr_stage_kernel<T, false><<<gbox, kBlock, 0, st>>>(c, src, eh, dst, dU, Un, aux, mt, sgt,
                                                            (T)kAs[s], (T)kBs[s], flags);
       COFFEE_CUDA_TRY(cudaGetLastError());
       if (hook && (rc = hook->after(kind))) return rc;
     }
     int rc = hook ? hook->before(COFFEE_KERNEL_KO) : COFFEE_OK;
     if (rc) return rc;
-    gr_ko_kernel<T><<<gbox, kBlock, 0, st>>>(c, Bb, A);
+    gr_ko_kernel<T><<<gbox, kBlock, 0, st>>>(c, Bb, A, mt);
     COFFEE_CUDA_TRY(cudaGetLastError());
     if (hook && (rc = hook->after(COFFEE_KERNEL_KO))) return rc;
   }
@@ -127,31 +148,34 @@ int gr_check(const coffee_env* env) {
 
 namespace {
 template <typename T>
-int gr_fill_sqrt_gamma(const coffee_env* env, void* ehbuf) {
+int gr_fill_metric(const coffee_env* env, void* ehbuf) {
   GrConst<T> c;
   fill_gr_const<T>(env, &c);
   const size_t n = (size_t)c.d[0] * c.d[1] * c.d[2];
-  gr_sqrt_gamma_kernel<T><<<grid_over(c.d[0], c.d[1], c.d[2]), kBlock>>>(
-      c, static_cast<T*>(ehbuf) + 6 * n);
+  T* sg = static_cast<T*>(ehbuf) + 6 * n;
+  gr_metric_kernel<T><<<grid_over(c.d[0], c.d[1], c.d[2]), kBlock>>>(c, sg + n, sg);
   COFFEE_CUDA_TRY(cudaGetLastError());
   COFFEE_CUDA_TRY(cudaDeviceSynchronize());
   return COFFEE_OK;
 }
 }  // namespace
 
-// Scratch of the GR solver: E and H (6 arrays) and the sqrt(gamma) table.
+// Scratch of the GR solver: E and H (6 arrays), sqrt(gamma) of every point
+// and the near-horizon metric table (kMetricComps arrays over the box), all
+// evaluated in FP64.
 int gr_setup(const coffee_env* env, int elem, void** ehbuf) {
   const coffee_grid& g = env->grid;
   const size_t n = (size_t)g.dims[0] * g.dims[1] * g.dims[2];
+  const size_t nt = elem == 4 ? near_points<float>(env) : near_points<double>(env);
   *ehbuf = nullptr;
-  cudaError_t err = cudaMalloc(ehbuf, 7 * n * (size_t)elem);
+  cudaError_t err = cudaMalloc(ehbuf, (7 * n + kMetricComps * nt + 1) * (size_t)elem);
   if (err != cudaSuccess) {
     *ehbuf = nullptr;
-    return fail(COFFEE_E_NOMEM, "GR scratch (E, H, sqrt(gamma)) allocation failed: %s",
+    return fail(COFFEE_E_NOMEM, "GR scratch (E, H, metric table) allocation failed: %s",
                 cudaGetErrorString(err));
   }
-  const int rc = elem == 4 ? gr_fill_sqrt_gamma<float>(env, *ehbuf)
-                           : gr_fill_sqrt_gamma<double>(env, *ehbuf);
+  const int rc = elem == 4 ? gr_fill_metric<float>(env, *ehbuf)
+                           : gr_fill_metric<double>(env, *ehbuf);
   if (rc) {
     cudaFree(*ehbuf);
     *ehbuf = nullptr;

@@ -8,10 +8,11 @@
 // writes E and H over the whole grid (the reference's get_Ed / get_Hd), the
 // other does the LSRK update, the clamps and, in the last stage, both
 // absorbing layers in one pass over the update box, reading the current
-// buffer and writing the other one.  The metric is evaluated analytically
-// per point in field precision, as the reference does; unlike the
-// reference, each point evaluates it once per launch (the reference calls
-// get_r inside every metric component, about forty times per point).
+// buffer and writing the other one.  Near the horizon the metric comes from
+// a table evaluated once per solver in FP64 (gr_metric_kernel); elsewhere it
+// is evaluated per point in field precision, as the reference does, but
+// once per point and launch (the reference calls get_r inside every metric
+// component, about forty times per point).
 #pragma once
 
 #include "axisym_kernels.cuh"
@@ -31,6 +32,7 @@ struct GrConst {
   T xl[3], xh[3];           // outer layer edges (boundary.cu:43-54)
   T pmlscale, sigpml;
   T r1, r2, dd;             // inner layer: 0.7 r_H, 0.01 r_H, 0.2 r_H (:617-621)
+  int nb_lo[3], nb_n[3];    // the near-horizon box of the metric table (grid indices)
 };
 
 // r of the Kerr-Schild coordinates (metric_cks_impl.hpp:17-24)
@@ -52,26 +54,35 @@ __device__ __forceinline__ T cks_sqrt_gamma(T a, T x, T y, T z) {
   return sqrt(T(1) + T(2) * r * r * r / den);
 }
 
-// All metric functions at one point (metric_cks_impl.hpp:13-181).
-template <typename T>
+// All metric functions at one point (metric_cks_impl.hpp:13-181), in
+// precision T with the TINY floors of the field precision TF.
+template <typename T, typename TF = T>
 struct Cks {
   T r, alpha, sg;
   T bu[3];
   T gd11, gd12, gd13, gd22, gd23, gd33;
   T gu11, gu12, gu13, gu22, gu23, gu33;
 
+  Cks() = default;
   __device__ __forceinline__ Cks(T a, T x, T y, T z) {
-    r = cks_r(a, x, y, z);
+    constexpr T tiny = (T)Tiny<TF>::v;
+    {
+      const T R2 = x * x + y * y + z * z;
+      const T q = R2 - a * a;
+      T s = q * q + T(4) * (a * z) * (a * z);
+      if (s < tiny) s = tiny;
+      r = sqrt((q + sqrt(s)) * T(0.5));
+    }
     const T r2 = r * r, r3 = r2 * r, r4 = r2 * r2;
     const T aa = a * a, azz = aa * z * z;
     T den = r4 + azz;
-    if (den < Tiny<T>::v) den = Tiny<T>::v;
+    if (den < tiny) den = tiny;
     T denu = T(2) * r3 + r4 + azz;
-    if (denu < Tiny<T>::v) denu = Tiny<T>::v;
+    if (denu < tiny) denu = tiny;
     T ar = aa + r2;
     T ar2 = ar * ar;
-    if (ar < Tiny<T>::v) ar = Tiny<T>::v;
-    if (ar2 < Tiny<T>::v) ar2 = Tiny<T>::v;
+    if (ar < tiny) ar = tiny;
+    if (ar2 < tiny) ar2 = tiny;
     const T lx = r * x + a * y, ly = -a * x + r * y;
     const T iden = T(1) / den, idenu = T(1) / denu, iar = T(1) / ar, iar2 = T(1) / ar2;
     const T gam = T(1) + T(2) * r3 * iden;
@@ -112,32 +123,94 @@ __device__ __forceinline__ T gr_pos(const GrConst<T>& c, int a, int n) {
   return c.lower[a] + c.delta[a] * (T)(n - c.g[a]);
 }
 
-// sqrt(gamma) at every grid point, evaluated once per solver in FP64 and
-// rounded: the divergence stencil (div4, field_solver_gr_EZ.cu:44-86)
-// weights each neighbour by it.
+// The near-horizon metric table.  Within a box of half-width kNearRH r_H
+// around the hole the metric is evaluated once per solver in FP64 (at the
+// grid's coordinates in the field precision, where the reference evaluates
+// it) and rounded to the field precision: there the field-precision formula
+// loses digits (r from sqrt((q + sqrt(q^2 + 4 a^2 z^2)) / 2) with
+// q = R^2 - a^2 cancels inside the horizon, giving FP32 errors of 1e-5 in r
+// and the shift against 1e-7 outside 1.5 r_H).  Elsewhere it is evaluated in
+// the field precision per point, as the reference does.  kMetricComps
+// components, component q of table point t at m[q * nt + t]: r, alpha,
+// sqrt(gamma), beta^1..3, gamma_11, _12, _13, _22, _23, _33, gamma^11, ^12,
+// ^13, ^22, ^23, ^33.
+constexpr int kMetricComps = 18;
+constexpr double kNearRH = 3.0;
+
 template <typename T>
-__global__ void gr_sqrt_gamma_kernel(const __grid_constant__ GrConst<T> c, T* sg) {
+__device__ __forceinline__ long long near_index(const GrConst<T>& c, int i, int j, int k) {
+  const int a = i - c.nb_lo[0], b = j - c.nb_lo[1], e = k - c.nb_lo[2];
+  if ((unsigned)a >= (unsigned)c.nb_n[0] || (unsigned)b >= (unsigned)c.nb_n[1] ||
+      (unsigned)e >= (unsigned)c.nb_n[2])
+    return -1;
+  return a + (long long)c.nb_n[0] * (b + (long long)c.nb_n[1] * e);
+}
+
+template <typename T>
+__global__ void gr_metric_kernel(const __grid_constant__ GrConst<T> c, T* __restrict__ m,
+                                 T* __restrict__ sg) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
   if (i >= c.d[0] || j >= c.d[1] || k >= c.d[2]) return;
   const long long o = i + (long long)c.d[0] * (j + (long long)c.d[1] * k);
-  const double x = (double)gr_pos(c, 0, i), y = (double)gr_pos(c, 1, j),
-               z = (double)gr_pos(c, 2, k);
-  sg[o] = (T)cks_sqrt_gamma<double>((double)c.a, x, y, z);
+  const Cks<double, T> q((double)c.a, (double)gr_pos(c, 0, i), (double)gr_pos(c, 1, j),
+                         (double)gr_pos(c, 2, k));
+  // sqrt(gamma) of every point: the divergence stencil (div4,
+  // field_solver_gr_EZ.cu:44-86) weights each neighbour by it
+  sg[o] = (T)q.sg;
+  const long long t = near_index(c, i, j, k);
+  if (t < 0) return;
+  const long long nt = (long long)c.nb_n[0] * c.nb_n[1] * c.nb_n[2];
+  const double v[kMetricComps] = {q.r,    q.alpha, q.sg,   q.bu[0], q.bu[1], q.bu[2],
+                                  q.gd11, q.gd12,  q.gd13, q.gd22,  q.gd23,  q.gd33,
+                                  q.gu11, q.gu12,  q.gu13, q.gu22,  q.gu23,  q.gu33};
+#pragma unroll
+  for (int a = 0; a < kMetricComps; ++a) m[a * nt + t] = (T)v[a];
+}
+
+// The metric at grid point (i, j, k) with coordinates (x, y, z): from the
+// table inside the near-horizon box, else evaluated here.
+template <typename T>
+__device__ __forceinline__ Cks<T> metric_at(const GrConst<T>& c, const T* __restrict__ m,
+                                            int i, int j, int k, T x, T y, T z) {
+  const long long t = near_index(c, i, j, k);
+  if (t < 0) return Cks<T>(c.a, x, y, z);
+  const long long nt = (long long)c.nb_n[0] * c.nb_n[1] * c.nb_n[2];
+  Cks<T> q;
+  q.r = __ldg(m + t);
+  q.alpha = __ldg(m + nt + t);
+  q.sg = __ldg(m + 2 * nt + t);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) q.bu[a] = __ldg(m + (3 + a) * nt + t);
+  q.gd11 = __ldg(m + 6 * nt + t);
+  q.gd12 = __ldg(m + 7 * nt + t);
+  q.gd13 = __ldg(m + 8 * nt + t);
+  q.gd22 = __ldg(m + 9 * nt + t);
+  q.gd23 = __ldg(m + 10 * nt + t);
+  q.gd33 = __ldg(m + 11 * nt + t);
+  q.gu11 = __ldg(m + 12 * nt + t);
+  q.gu12 = __ldg(m + 13 * nt + t);
+  q.gu13 = __ldg(m + 14 * nt + t);
+  q.gu22 = __ldg(m + 15 * nt + t);
+  q.gu23 = __ldg(m + 16 * nt + t);
+  q.gu33 = __ldg(m + 17 * nt + t);
+  return q;
 }
 
 // E and H over the whole grid (kernel_compute_E_gr / kernel_compute_H_gr,
 // field_solver_gr_EZ.cu:88-186).  eh[0..2] = E, eh[3..5] = H.
 template <typename T>
 __global__ void __launch_bounds__(256) gr_eh_kernel(const __grid_constant__ GrConst<T> c,
-                                                    const F7<T> u, const F7<T> eh) {
+                                                    const F7<T> u, const F7<T> eh,
+                                                    const T* __restrict__ mt) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int k = blockIdx.z * blockDim.z + threadIdx.z;
   if (i >= c.d[0] || j >= c.d[1] || k >= c.d[2]) return;
   const long long o = i + (long long)c.d[0] * (j + (long long)c.d[1] * k);
-  const Cks<T> m(c.a, gr_pos(c, 0, i), gr_pos(c, 1, j), gr_pos(c, 2, k));
+  const Cks<T> m =
+      metric_at(c, mt, i, j, k, gr_pos(c, 0, i), gr_pos(c, 1, j), gr_pos(c, 2, k));
   const T D[3] = {__ldg(u.p[0] + o), __ldg(u.p[1] + o), __ldg(u.p[2] + o)};
   const T B[3] = {__ldg(u.p[3] + o), __ldg(u.p[4] + o), __ldg(u.p[5] + o)};
   T Dd[3], Bd[3];
@@ -231,6 +304,7 @@ __global__ void __launch_bounds__(256, COFFEE_GR_STAGE_MIN_BLOCKS) gr_stage_kern
                                                        const F7<T> u, const F7<T> eh,
                                                        const F7<T> out, const F7<T> du,
                                                        const F7<T> un, const F5<T> aux,
+                                                       const T* __restrict__ mt,
                                                        const T* __restrict__ sgt, const T As,
                                                        const T Bs, const int flags) {
   const int i = c.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
@@ -241,7 +315,7 @@ __global__ void __launch_bounds__(256, COFFEE_GR_STAGE_MIN_BLOCKS) gr_stage_kern
   const long long o = i + sy * j + sz * k;
   const long long st[3] = {sx, sy, sz};
   const T x = gr_pos(c, 0, i), y = gr_pos(c, 1, j), z = gr_pos(c, 2, k);
-  const Cks<T> m(c.a, x, y, z);
+  const Cks<T> m = metric_at(c, mt, i, j, k, x, y, z);
   const T igms = T(1) / m.sg;
 
   auto d1 = [&](const T* f, int ax) {
@@ -344,7 +418,8 @@ __global__ void __launch_bounds__(256, COFFEE_GR_STAGE_MIN_BLOCKS) gr_stage_kern
 // 3D 6th difference of finite_diff.h:84-92), then the clamps (:895-900).
 template <typename T>
 __global__ void __launch_bounds__(256) gr_ko_kernel(const __grid_constant__ GrConst<T> c,
-                                                    const F7<T> u, const F7<T> out) {
+                                                    const F7<T> u, const F7<T> out,
+                                                    const T* __restrict__ mt) {
   const int i = c.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = c.lo[1] + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = c.lo[2] + blockIdx.z * blockDim.z + threadIdx.z;
@@ -365,7 +440,8 @@ __global__ void __launch_bounds__(256) gr_ko_kernel(const __grid_constant__ GrCo
     }
     v[a] = __ldg(f + o) + c.ko_c * (tx + ty + tz);
   }
-  const Cks<T> m(c.a, gr_pos(c, 0, i), gr_pos(c, 1, j), gr_pos(c, 2, k));
+  const Cks<T> m =
+      metric_at(c, mt, i, j, k, gr_pos(c, 0, i), gr_pos(c, 1, j), gr_pos(c, 2, k));
   gr_clamps(c, m, v);
 #pragma unroll
   for (int a = 0; a < 7; ++a) out.p[a][o] = v[a];
