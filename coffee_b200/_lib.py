@@ -21,7 +21,10 @@ ERRORS = {
 
 FIELD_IDS = {"Ex": 0, "Ey": 1, "Ez": 2, "Bx": 3, "By": 4, "Bz": 5, "P": 6,
              "Jx": 7, "Jy": 8, "Jz": 9, "divE": 10, "divB": 11,
-             "B0x": 12, "B0y": 13, "B0z": 14}
+             "B0x": 12, "B0y": 13, "B0z": 14,
+             "dU_EgtB": 15, "dU_Epar": 16, "dU_KO": 17,
+             "dU_EgtB_cum": 18, "dU_Epar_cum": 19, "dU_KO_cum": 20}
+ENERGY_DIAG_NAMES = ("dU_EgtB", "dU_Epar", "dU_KO", "dU_EgtB_cum", "dU_Epar_cum", "dU_KO_cum")
 VARIANT_FLAT = 0
 VARIANT_LOGSPH = 1
 VARIANT_CYL = 2
@@ -100,6 +103,7 @@ SIGNATURES = {
     "coffee_solver_set_aux": (_i, [_vp, _i]),
     "coffee_solver_set_arithmetic": (_i, [_vp, _i]),
     "coffee_solver_set_taper_lanes": (_i, [_vp, _i]),
+    "coffee_solver_set_energy_diag": (_i, [_vp, _i]),
     "coffee_solver_set_timing": (_i, [_vp, _i]),
     "coffee_solver_last_timing": (_i, [_vp, _P(_d), _P(_i), _P(_d)]),
     "coffee_fields_init_fourier": (_i, [_vp, _P(_d), _i, _P(_d), _P(_d), _P(_d), _i, _P(_d),

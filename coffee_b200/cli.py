@@ -34,6 +34,11 @@ one line ``step time Wb We`` per output (the energy file of
 ``main-wave.cpp``), Cartesian solvers only (the staggered solver's energies
 interpolate every component to the vertices, as its total_energy does).  Steps between two events run as one
 ``coffee_solver_step`` call, which advances time exactly as the loop does.
+With ``--energy-diag`` (flat drivers) the field files also hold the CPU
+build's energy-change diagnostics dU_EgtB, dU_Epar, dU_KO, dU_EgtB_cum,
+dU_Epar_cum, dU_KO_cum after J, div E, div B, and the _cum arrays are reset
+to zero after each output, as the reference's exporter does
+(``src/utils/data_exporter.cpp:624-638``).
 """
 from __future__ import annotations
 
@@ -87,6 +92,8 @@ def parse_args(argv=None):
     ap.add_argument("--steps", type=int, default=None, help="override max_steps")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--precision", choices=("f32", "f64"), default="f32")
+    ap.add_argument("--energy-diag", action="store_true",
+                    help="flat drivers: write the CPU build's dU_* energy diagnostics")
     return ap.parse_args(argv)
 
 
@@ -129,12 +136,18 @@ def _solver(kind, data, env, sem_gpu):
             GRYEE: sv.FieldSolverGr}[kind](data, env)
 
 
-def _write_output(path, data, s, step, time, ds, guard, flat):
+def _write_output(path, data, s, step, time, ds, guard, flat, energy_diag=False):
     names = ["Ex", "Ey", "Ez", "Bx", "By", "Bz", "P"]
     arrays = data.download(names)
     if flat:
         arrays += data.download(["Jx", "Jy", "Jz", "divE", "divB"])
         names += ["Jx", "Jy", "Jz", "divE", "divB"]
+    if energy_diag:
+        from ._lib import ENERGY_DIAG_NAMES, FIELD_IDS
+        arrays += data.download(ENERGY_DIAG_NAMES)
+        zero = np.zeros_like(arrays[0])
+        for name in ENERGY_DIAG_NAMES[3:]:
+            data.upload_field(FIELD_IDS[name], zero)
     sl = tuple(slice(g, a - g, ds) for g, a in zip(guard[::-1], arrays[0].shape))
     write_fld(path, [np.ascontiguousarray(a[sl]) for a in arrays], guard=(0, 0, 0), time=time,
               step=step)
@@ -155,6 +168,11 @@ def run(args) -> int:
     s = _solver(d.kind, data, env, sem_gpu=False)
     if flat:
         s.set_aux(True)  # J, div E, div B for the outputs
+    energy_diag = bool(getattr(args, "energy_diag", False))
+    if energy_diag:
+        if not flat:
+            raise ValueError("--energy-diag needs a flat (field_solver_EZ) driver")
+        s.set_energy_diag(True)
     ftype = np.dtype(dtype).type
     dt = ftype(p.dt)
     step, time = 0, ftype(0.0)
@@ -176,7 +194,7 @@ def run(args) -> int:
                             step)
         if out:
             _write_output(os.path.join(args.output, f"fld.{step:05d}.fld"), data, s, step,
-                          float(time), ds, guard, flat)
+                          float(time), ds, guard, flat, energy_diag)
             if energies:
                 wb, we = s.total_energy("B"), s.total_energy("E")
                 with open(os.path.join(args.output, "energy.txt"), "a") as fh:

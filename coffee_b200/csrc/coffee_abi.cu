@@ -66,6 +66,7 @@ struct coffee_solver {
   int timing;
   int arith;    // COFFEE_ARITH_* of the flat solver
   int taper_lanes;  // SIMD lanes of the CPU build's taper (0: by precision)
+  int energy_diag;  // the CPU build's energy-change diagnostics kept
   uint64_t synced_generation;
   FlatLaunch launch;
   void* vtab;  // tables / scratch of a non-Cartesian variant (device), or null
@@ -423,7 +424,7 @@ extern "C" int coffee_fields_upload(coffee_fields* f, int id, const void* host) 
     if (rc) return rc;
     COFFEE_CUDA_TRY(cudaMemcpy(f->d[id], host, bytes, cudaMemcpyHostToDevice));
   }
-  ++f->generation;
+  if (id < 7) ++f->generation;  // E, B, P: the solvers re-copy their second buffer
   return COFFEE_OK;
 }
 
@@ -558,7 +559,8 @@ extern "C" int coffee_fields_fill_guards(coffee_fields* f) {
 
 template <typename T>
 static int configure_solver(coffee_solver* s) {
-  return flat_plan<T>(s->env, s->semantics, &s->launch, s->arith == COFFEE_ARITH_REFERENCE);
+  return flat_plan<T>(s->env, s->semantics, &s->launch, s->arith == COFFEE_ARITH_REFERENCE,
+                      s->energy_diag != 0);
 }
 
 extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int variant,
@@ -601,6 +603,7 @@ extern "C" int coffee_solver_create(coffee_env* env, coffee_fields* f, int varia
   s->timing = 0;
   s->arith = COFFEE_ARITH_REFERENCE;
   s->taper_lanes = 0;
+  s->energy_diag = 0;
   s->events_used = 0;
   s->synced_generation = 0;
   // the GR solver's inner absorbing region always needs the start-of-step
@@ -701,12 +704,39 @@ extern "C" int coffee_solver_set_arithmetic(coffee_solver* s, int mode) {
     return fail(COFFEE_E_INVALID, "only the flat EZ solver has a second arithmetic");
   }
   if (mode == s->arith) return COFFEE_OK;
+  if (s->energy_diag && mode != COFFEE_ARITH_REFERENCE)
+    return fail(COFFEE_E_INVALID, "the energy diagnostics need the reference arithmetic");
   COFFEE_CUDA_TRY(cudaSetDevice(s->env->device));
   const int old = s->arith;
   s->arith = mode;
   const int rc = (s->f->elem == 4) ? configure_solver<float>(s) : configure_solver<double>(s);
   if (rc) {
     s->arith = old;  // keep the previous plan
+    (void)((s->f->elem == 4) ? configure_solver<float>(s) : configure_solver<double>(s));
+  }
+  return rc;
+}
+
+extern "C" int coffee_solver_set_energy_diag(coffee_solver* s, int enable) {
+  clear_error();
+  if (!s) return fail(COFFEE_E_INVALID, "coffee_solver_set_energy_diag: null argument");
+  enable = enable ? 1 : 0;
+  if (enable == s->energy_diag) return COFFEE_OK;
+  if (enable && (s->variant != COFFEE_VARIANT_FLAT || s->semantics != COFFEE_SEM_CPU_REF ||
+                 s->arith != COFFEE_ARITH_REFERENCE))
+    return fail(COFFEE_E_INVALID,
+                "the energy diagnostics are the CPU build's: flat solver, CPU semantics and "
+                "the reference arithmetic only");
+  if (enable)
+    for (int id = COFFEE_DU_EGTB; id <= COFFEE_DU_KO_CUM; ++id) {
+      int rc = ensure_field(s->f, id);
+      if (rc) return rc;
+    }
+  COFFEE_CUDA_TRY(cudaSetDevice(s->env->device));
+  s->energy_diag = enable;
+  const int rc = (s->f->elem == 4) ? configure_solver<float>(s) : configure_solver<double>(s);
+  if (rc) {
+    s->energy_diag = 1 - enable;
     (void)((s->f->elem == 4) ? configure_solver<float>(s) : configure_solver<double>(s));
   }
   return rc;
@@ -824,8 +854,11 @@ static int run_steps(coffee_solver* s, double time, int nsteps) {
     if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(s->ev_end, st));
     return COFFEE_OK;
   }
+  F6<T> dg;
+  for (int a = 0; a < 6; ++a) dg.p[a] = static_cast<T*>(f->d[COFFEE_DU_EGTB + a]);
   int rc = flat_steps<T>(c, s->launch, f7<T>(f->d), f7<T>(s->B), f7<T>(s->dU), f7<T>(s->Un), aux,
-                         s->aux != 0, time, nsteps, st, s->timing ? &hook : nullptr);
+                         s->aux != 0, time, nsteps, st, s->timing ? &hook : nullptr,
+                         s->energy_diag ? &dg : nullptr);
   if (rc) return rc;
   if (s->timing) COFFEE_CUDA_TRY(cudaEventRecord(s->ev_end, st));
   return COFFEE_OK;

@@ -53,6 +53,9 @@ template <typename T> struct F7 { T* p[7]; };
 // functions so that the caller's registers never need an address.
 template <typename T> struct V7 { T v[7]; };
 template <typename T> struct F5 { T* p[5]; };
+// The CPU build's energy-change arrays (sim_data.h:15-16), in this order:
+// dU_EgtB, dU_Epar, dU_KO, dU_EgtB_cum, dU_Epar_cum, dU_KO_cum.
+template <typename T> struct F6 { T* p[6]; };
 
 // ---- cp.async helpers (sm_80+ asynchronous global->shared copies) --------
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {

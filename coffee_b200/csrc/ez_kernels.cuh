@@ -102,14 +102,14 @@ struct Derivs {
 // XA selects the CPU build's own arithmetic (ez_refarith.cuh) for the
 // current, the taper, the accumulators, the update and the clamps; the
 // derivatives then come in already combined in that arithmetic (Derivs).
-template <typename T, bool FIRST, bool BC, bool XA>
+template <typename T, bool FIRST, bool BC, bool XA, bool DG>
 __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7],
                                             const Derivs<T>& dv, const T dold[7],
                                             const T As, const T Bs, const T tst,
                                             const int flags, const ColumnCtx<T>& col,
                                             const int k, const uint32_t o, const F7<T>& du,
                                             const F7<T>& un, const F5<T>& aux,
-                                            const F7<T>& uout) {
+                                            const F7<T>& uout, const F6<T>& dg) {
   const bool cpu = c.semantics == SEM_CPU_REF;
   const T ex = u[0], ey = u[1], ez = u[2], bx = u[3], by = u[4], bz = u[5], P = u[6];
   const T rotBx = dv.rotB[0], rotBy = dv.rotB[1], rotBz = dv.rotB[2];
@@ -241,7 +241,10 @@ __device__ __forceinline__ void stage_point(const EzConst<T>& c, const T u[7],
     // mul_add(dU, Bs, U), then clean_epar_check_eGTb
 #pragma unroll
     for (int f = 0; f < 7; ++f) nu[f] = xa::fma(d[f], Bs, u[f]);
-    apply_clamps_xa(nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
+    if constexpr (DG)
+      apply_clamps_xa_dg<FIRST>(nu[0], nu[1], nu[2], nu[3], nu[4], nu[5], dg, o);
+    else
+      apply_clamps_xa(nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
   } else {
 #pragma unroll
     for (int f = 0; f < 7; ++f) nu[f] = fma(d[f], Bs, u[f]);
@@ -388,11 +391,15 @@ constexpr size_t stage_smem_bytes(bool first) {
          (first ? 0 : (size_t)stage_dring<BC, PF>() * 7 * TX * TY * sizeof(T));
 }
 
-template <typename T, int TX, int TY, int PF, bool FIRST, bool BC, int V, bool XA>
+// DG (with XA only): also accumulate the CPU build's energy-change
+// diagnostics of the clamps into dg.
+template <typename T, int TX, int TY, int PF, bool FIRST, bool BC, int V, bool XA, bool DG>
 __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     ez_stage_kernel(const __grid_constant__ EzConst<T> c, const F7<const T> uin,
                     const F7<T> uout, const F7<T> du, const F7<T> un, const F5<T> aux,
-                    const T As, const T Bs, const T tst, const int kchunk, const int flags) {
+                    const F6<T> dg, const T As, const T Bs, const T tst, const int kchunk,
+                    const int flags) {
+  static_assert(XA || !DG, "the energy diagnostics need the reference arithmetic");
   using L = TileLoader<T, TX, TY, 2, V>;
   constexpr int R = stage_ring<BC, PF>();    // field ring slots
   constexpr int DR = stage_dring<BC, PF>();  // dU ring slots
@@ -579,8 +586,8 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
           dold[f] = lds<T, f * DFB>(ad);
         });
       }
-      stage_point<T, FIRST, BC, XA>(c, u, dv, dold, As, Bs, tst, flags, col, k,
-                                (uint32_t)k * sz + own, du, un, aux, uout);
+      stage_point<T, FIRST, BC, XA, DG>(c, u, dv, dold, As, Bs, tst, flags, col, k,
+                                        (uint32_t)k * sz + own, du, un, aux, uout, dg);
       if constexpr (ZU == 1) {
 #pragma unroll
         for (int q = 0; q < 4; ++q)
@@ -653,10 +660,11 @@ constexpr size_t ko_smem_bytes() {
   return (size_t)ko_ring<BC, PF>() * 7 * TileLoader<T, TX, TY, 3, V>::FB;
 }
 
-template <typename T, int TX, int TY, int PF, bool BC, int V, bool XA>
+template <typename T, int TX, int TY, int PF, bool BC, int V, bool XA, bool DG>
 __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
     ez_ko_kernel(const __grid_constant__ EzConst<T> c, const F7<const T> uin,
-                 const F7<T> uout, const T tko, const int kchunk) {
+                 const F7<T> uout, const F6<T> dg, const T tko, const int kchunk) {
+  static_assert(XA || !DG, "the energy diagnostics need the reference arithmetic");
   using L = TileLoader<T, TX, TY, 3, V>;
   constexpr int R = ko_ring<BC, PF>();
   constexpr int ZU = ko_zunroll<BC>();
@@ -744,10 +752,26 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
           nu[f] = cv;
         }
       });
-      if constexpr (XA) apply_clamps_xa(nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
-      else apply_clamps(c, nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
+      const uint32_t o = (uint32_t)k * sz + own;
+      if constexpr (DG) {
+        // dU_KO = (|B|^2 + |E|^2) after the pass minus before it, and
+        // dU_KO_cum += it (field_solver_EZ.cpp:398-455)
+        constexpr int C3 = (S + 3) % 7;  // the window slot of plane k
+        const T u0 = xa::add(xa::dot3(w[C3][3], w[C3][3], w[C3][4], w[C3][4], w[C3][5], w[C3][5]),
+                             xa::dot3(w[C3][0], w[C3][0], w[C3][1], w[C3][1], w[C3][2], w[C3][2]));
+        const T u1 = xa::add(xa::dot3(nu[3], nu[3], nu[4], nu[4], nu[5], nu[5]),
+                             xa::dot3(nu[0], nu[0], nu[1], nu[1], nu[2], nu[2]));
+        const T dko = xa::sub(u1, u0);
+        dg.p[5][o] = xa::add(dko, dg.p[5][o]);
+        dg.p[2][o] = dko;
+        apply_clamps_xa_dg<false>(nu[0], nu[1], nu[2], nu[3], nu[4], nu[5], dg, o);
+      } else if constexpr (XA) {
+        apply_clamps_xa(nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
+      } else {
+        apply_clamps(c, nu[0], nu[1], nu[2], nu[3], nu[4], nu[5]);
+      }
       if constexpr (BC) star_boundary(c, i, j, k, tko, nu);
-      store_with_images(g, col, uout, k, (uint32_t)k * sz + own, nu);
+      store_with_images(g, col, uout, k, o, nu);
       if constexpr (ZU == 1) {
 #pragma unroll
         for (int q = 0; q < 6; ++q)

@@ -186,16 +186,17 @@ struct FlatLaunch {
   bool bc;   // star / absorbing-layer code compiled in
   bool vec;  // planes copied as aligned element pairs (even row length d0)
   bool xa;   // the CPU build's own arithmetic (CPU semantics, ez_refarith.cuh)
+  bool dg;   // and its energy-change diagnostics (xa only)
   int kchunk_stage, kchunk_ko;
   dim3 grid_stage, grid_ko;
 };
 
-template <typename T, bool BC, int V, bool XA>
+template <typename T, bool BC, int V, bool XA, bool DG = false>
 struct FlatKernels {
   using S = Shape<T>;
-  static constexpr auto first = ez_stage_kernel<T, S::STX, S::STY, S::SPF, true, BC, V, XA>;
-  static constexpr auto rest = ez_stage_kernel<T, S::STX, S::STY, S::SPF, false, BC, V, XA>;
-  static constexpr auto ko = ez_ko_kernel<T, S::KTX, S::KTY, S::KPF, BC, V, XA>;
+  static constexpr auto first = ez_stage_kernel<T, S::STX, S::STY, S::SPF, true, BC, V, XA, DG>;
+  static constexpr auto rest = ez_stage_kernel<T, S::STX, S::STY, S::SPF, false, BC, V, XA, DG>;
+  static constexpr auto ko = ez_ko_kernel<T, S::KTX, S::KTY, S::KPF, BC, V, XA, DG>;
 
   static cudaError_t set_attributes() {
     cudaError_t e = cudaFuncSetAttribute(first, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -218,52 +219,62 @@ struct FlatKernels {
   }
   static void stage(bool is_first, const FlatLaunch& L, cudaStream_t st, const EzConst<T>& c,
                     const F7<const T>& src, const F7<T>& dst, const F7<T>& du, const F7<T>& un,
-                    const F5<T>& aux, T As, T Bs, T tst, int flags) {
+                    const F5<T>& aux, const F6<T>& dg, T As, T Bs, T tst, int flags) {
     const dim3 bs(S::STX, S::STY);
     if (is_first)
-      first<<<L.grid_stage, bs, stage_smem<T, V, BC>(true), st>>>(c, src, dst, du, un, aux, As, Bs,
-                                                              tst, L.kchunk_stage, flags);
+      first<<<L.grid_stage, bs, stage_smem<T, V, BC>(true), st>>>(
+          c, src, dst, du, un, aux, dg, As, Bs, tst, L.kchunk_stage, flags);
     else
-      rest<<<L.grid_stage, bs, stage_smem<T, V, BC>(false), st>>>(c, src, dst, du, un, aux, As, Bs,
-                                                              tst, L.kchunk_stage, flags);
+      rest<<<L.grid_stage, bs, stage_smem<T, V, BC>(false), st>>>(
+          c, src, dst, du, un, aux, dg, As, Bs, tst, L.kchunk_stage, flags);
   }
   static void ko_pass(const FlatLaunch& L, cudaStream_t st, const EzConst<T>& c,
-                      const F7<const T>& src, const F7<T>& dst, T tko) {
-    ko<<<L.grid_ko, dim3(S::KTX, S::KTY), ko_smem<T, V, BC>(), st>>>(c, src, dst, tko, L.kchunk_ko);
+                      const F7<const T>& src, const F7<T>& dst, const F6<T>& dg, T tko) {
+    ko<<<L.grid_ko, dim3(S::KTX, S::KTY), ko_smem<T, V, BC>(), st>>>(c, src, dst, dg, tko,
+                                                                     L.kchunk_ko);
   }
 };
 
-// Calls fn(FlatKernels<T, BC, V, XA>{}) for the kernel set L selects.
-template <typename T, bool XA, class Fn>
+// Calls fn(FlatKernels<T, BC, V, XA, DG>{}) for the kernel set L selects.
+template <typename T, bool XA, bool DG, class Fn>
 inline void with_flat_kernels_xa(const FlatLaunch& L, Fn&& fn) {
   if (L.bc) {
-    if (L.vec) fn(FlatKernels<T, true, 2, XA>{});
-    else fn(FlatKernels<T, true, 1, XA>{});
+    if (L.vec) fn(FlatKernels<T, true, 2, XA, DG>{});
+    else fn(FlatKernels<T, true, 1, XA, DG>{});
   } else {
-    if (L.vec) fn(FlatKernels<T, false, 2, XA>{});
-    else fn(FlatKernels<T, false, 1, XA>{});
+    if (L.vec) fn(FlatKernels<T, false, 2, XA, DG>{});
+    else fn(FlatKernels<T, false, 1, XA, DG>{});
   }
 }
 template <typename T, class Fn>
 inline void with_flat_kernels(const FlatLaunch& L, Fn&& fn) {
-  if (L.xa) with_flat_kernels_xa<T, true>(L, fn);
-  else with_flat_kernels_xa<T, false>(L, fn);
+  if (L.xa && L.dg) with_flat_kernels_xa<T, true, true>(L, fn);
+  else if (L.xa) with_flat_kernels_xa<T, true, false>(L, fn);
+  else with_flat_kernels_xa<T, false, false>(L, fn);
 }
 
 // Set the shared-memory limits of every flat kernel of precision T on the
 // current device and plan the launch geometry of `env`'s grid.
 // reference_arith: the CPU semantics run in the CPU build's own arithmetic
 // (the default); false selects the regrouped, faster arithmetic.
+// energy_diag: with the reference arithmetic, also accumulate the CPU
+// build's energy-change diagnostics.
 template <typename T>
 inline int flat_plan(const coffee_env* env, int semantics, FlatLaunch* L,
-                     bool reference_arith = true) {
+                     bool reference_arith = true, bool energy_diag = false) {
   using S = Shape<T>;
   L->bc = flat_needs_bc(env->p, semantics);
   L->vec = env->grid.dims[0] % 2 == 0;
   L->xa = reference_arith && semantics == SEM_CPU_REF;
+  L->dg = L->xa && energy_diag;
   // the shared-memory limits of the four kernel sets of this arithmetic (a
   // caller may still switch the pair copies off, as coffee_noalloc.cu does)
-  if (L->xa) {
+  if (L->dg) {
+    COFFEE_CUDA_TRY((FlatKernels<T, true, 1, true, true>::set_attributes()));
+    COFFEE_CUDA_TRY((FlatKernels<T, false, 1, true, true>::set_attributes()));
+    COFFEE_CUDA_TRY((FlatKernels<T, true, 2, true, true>::set_attributes()));
+    COFFEE_CUDA_TRY((FlatKernels<T, false, 2, true, true>::set_attributes()));
+  } else if (L->xa) {
     COFFEE_CUDA_TRY((FlatKernels<T, true, 1, true>::set_attributes()));
     COFFEE_CUDA_TRY((FlatKernels<T, false, 1, true>::set_attributes()));
     COFFEE_CUDA_TRY((FlatKernels<T, true, 2, true>::set_attributes()));
@@ -322,7 +333,11 @@ struct LaunchHook {
 template <typename T>
 inline int flat_steps(const EzConst<T>& c, const FlatLaunch& L, const F7<T>& A, const F7<T>& Bb,
                       const F7<T>& dU, const F7<T>& Un, const F5<T>& aux, bool want_aux,
-                      double time, int nsteps, cudaStream_t st, LaunchHook* hook) {
+                      double time, int nsteps, cudaStream_t st, LaunchHook* hook,
+                      const F6<T>* dg = nullptr) {
+  F6<T> dgv;
+  for (int a = 0; a < 6; ++a) dgv.p[a] = dg ? dg->p[a] : nullptr;
+  if (L.dg && !dg) return fail(COFFEE_E_INVALID, "energy diagnostics planned without arrays");
   const T dt = c.dt;
   T t = (T)time;
   for (int step = 0; step < nsteps; ++step) {
@@ -342,8 +357,8 @@ inline int flat_steps(const EzConst<T>& c, const FlatLaunch& L, const F7<T>& A, 
         if (rc) return rc;
       }
       with_flat_kernels<T>(L, [&](auto K) {
-        decltype(K)::stage(i == 0, L, st, c, srcc, dst, dU, Un, aux, (T)kAs[i], (T)kBs[i], tst,
-                           flags);
+        decltype(K)::stage(i == 0, L, st, c, srcc, dst, dU, Un, aux, dgv, (T)kAs[i], (T)kBs[i],
+                           tst, flags);
       });
       COFFEE_CUDA_TRY(cudaGetLastError());
       if (hook) {
@@ -357,7 +372,7 @@ inline int flat_steps(const EzConst<T>& c, const FlatLaunch& L, const F7<T>& A, 
       int rc = hook->before(COFFEE_KERNEL_KO);
       if (rc) return rc;
     }
-    with_flat_kernels<T>(L, [&](auto K) { decltype(K)::ko_pass(L, st, c, srcc, A, t + dt); });
+    with_flat_kernels<T>(L, [&](auto K) { decltype(K)::ko_pass(L, st, c, srcc, A, dgv, t + dt); });
     COFFEE_CUDA_TRY(cudaGetLastError());
     if (hook) {
       int rc = hook->after(COFFEE_KERNEL_KO);

@@ -63,6 +63,37 @@ __device__ __forceinline__ void apply_clamps_xa(T& ex, T& ey, T& ez, T bx, T by,
   }
 }
 
+// The same clamps, adding the energy changes they make at point o to the
+// CPU build's diagnostics (clean_epar_check_eGTb, field_solver_EZ.cpp:
+// 578-624): |E|^2 after the cleaning minus before it to dU_Epar and
+// dU_Epar_cum, |E|^2 after both clamps minus before the cleaning to dU_EgtB
+// and dU_EgtB_cum.  FIRST: the step's first accumulation into dU_Epar and
+// dU_EgtB, which evolve_fields zeroes at its start (:1019-1021).
+template <bool FIRST, typename T>
+__device__ __forceinline__ void apply_clamps_xa_dg(T& ex, T& ey, T& ez, T bx, T by, T bz,
+                                                   const F6<T>& dg, uint32_t o) {
+  const T B2 = xa::floor_tiny(xa::dot3(bx, bx, by, by, bz, bz));
+  const T EB = xa::dot3(bx, ex, by, ey, bz, ez);
+  const T u0 = xa::dot3(ex, ex, ey, ey, ez, ez);
+  ex = xa::sub(ex, xa::div(xa::mul(EB, bx), B2));
+  ey = xa::sub(ey, xa::div(xa::mul(EB, by), B2));
+  ez = xa::sub(ez, xa::div(xa::mul(EB, bz), B2));
+  const T E2 = xa::dot3(ex, ex, ey, ey, ez, ez);
+  T u1g = E2;
+  if (E2 > B2) {
+    const T s = xa::sqrt(xa::div(B2, E2));
+    ex = xa::mul(ex, s);
+    ey = xa::mul(ey, s);
+    ez = xa::mul(ez, s);
+    u1g = xa::dot3(ex, ex, ey, ey, ez, ez);
+  }
+  const T dp = xa::sub(E2, u0), dgt = xa::sub(u1g, u0);
+  dg.p[4][o] = xa::add(dp, dg.p[4][o]);
+  dg.p[1][o] = xa::add(FIRST ? (T)0 : dg.p[1][o], dp);
+  dg.p[3][o] = xa::add(dgt, dg.p[3][o]);
+  dg.p[0][o] = xa::add(FIRST ? (T)0 : dg.p[0][o], dgt);
+}
+
 // ------------------------------------------------------- star field models
 // dipole2 / quadrupole / quadru_dipole (src/algorithms/pulsar_impl.hpp:57-129),
 // evaluated in double (the reference promotes through its double literals)

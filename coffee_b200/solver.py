@@ -214,6 +214,11 @@ class FieldSolverEZ:
         m = {"reference": 0, "fast": 1}[mode]
         check(self.lib.coffee_solver_set_arithmetic(self.handle, m))
 
+    def set_energy_diag(self, enable: bool):
+        """Keep the CPU build's energy-change diagnostics dU_EgtB, dU_Epar,
+        dU_KO and their _cum sums (SimData.download(_lib.ENERGY_DIAG_NAMES))."""
+        check(self.lib.coffee_solver_set_energy_diag(self.handle, int(bool(enable))))
+
     def set_taper_lanes(self, lanes: int):
         """SIMD width of the CPU build's P-gradient taper offsets (0: by
         precision, 16 for float and 8 for double as in the reference's two
@@ -278,9 +283,12 @@ class FieldSolverEZ:
 
 
 def run_flat(params: SimParams, fields, nsteps: int, time0: float = 0.0, semantics: str = "cpu",
-             aux: bool = False, device: int = 0, arithmetic: str = "reference"):
+             aux: bool = False, device: int = 0, arithmetic: str = "reference",
+             energy_diag: bool = False):
     """Upload ``fields``, advance ``nsteps`` on the GPU, return the 7 fields
-    (and J, divE, divB when ``aux``)."""
+    (and J, divE, divB when ``aux``; with ``energy_diag`` the aux list is
+    followed by the 6 energy-change arrays dU_EgtB, dU_Epar, dU_KO and their
+    _cum sums)."""
     env = SimEnvironment(params, device)
     data = SimData(env, fields[0].dtype)
     data.upload(fields)
@@ -289,9 +297,13 @@ def run_flat(params: SimParams, fields, nsteps: int, time0: float = 0.0, semanti
         solver.set_arithmetic(arithmetic)
     if aux:
         solver.set_aux(True)
+    if energy_diag:
+        solver.set_energy_diag(True)
     solver.step(time0, nsteps)
     out = data.download()
     auxa = data.download(("Jx", "Jy", "Jz", "divE", "divB")) if aux else None
+    if energy_diag:
+        auxa = (auxa or []) + data.download(_lib.ENERGY_DIAG_NAMES)
     solver.close()
     data.close()
     env.close()

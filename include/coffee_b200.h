@@ -63,6 +63,11 @@ enum { /* field ids for coffee_fields_ptr / upload / download */
   /* background field sim_data::B0, read by the staggered solver (allocated
    * on first use; zero until written) */
   COFFEE_B0X, COFFEE_B0Y, COFFEE_B0Z,
+  /* the CPU build's energy-change diagnostics, sim_data::dU_* (sim_data.h:
+   * 15-16), written by the flat solver with coffee_solver_set_energy_diag
+   * (allocated on first use, zero until written) */
+  COFFEE_DU_EGTB, COFFEE_DU_EPAR, COFFEE_DU_KO,
+  COFFEE_DU_EGTB_CUM, COFFEE_DU_EPAR_CUM, COFFEE_DU_KO_CUM,
   COFFEE_NUM_FIELDS
 };
 enum { /* solver variants */
@@ -230,6 +235,17 @@ enum { /* arithmetic of the flat EZ solver (coffee_solver_set_arithmetic) */
  * in the reference, which has one arithmetic per build).  The other
  * variants have only COFFEE_ARITH_REFERENCE. */
 COFFEE_API int coffee_solver_set_arithmetic(coffee_solver* s, int mode);
+/* Keep the CPU build's per-point energy-change diagnostics (1) or not (0,
+ * the default) in the following steps: the change of |E|^2 made by the E.B
+ * cleaning (COFFEE_DU_EPAR) and by both clamps (COFFEE_DU_EGTB), summed over
+ * the stages and the closing KO pass of a step, and the change of
+ * |E|^2 + |B|^2 made by the KO pass (COFFEE_DU_KO), each zeroed at the start
+ * of every step as evolve_fields does (field_solver_EZ.cpp:1019-1021), and
+ * their sums over steps (COFFEE_DU_*_CUM), which keep accumulating until the
+ * caller resets them (the reference's exporter does after each output,
+ * data_exporter.cpp:633-638).  Computed in the CPU build's own arithmetic:
+ * flat solver, CPU semantics, COFFEE_ARITH_REFERENCE only. */
+COFFEE_API int coffee_solver_set_energy_diag(coffee_solver* s, int enable);
 /* The SIMD width by which the CPU build's P-gradient taper offsets a point's
  * x, y and z (field_solver_EZ.cpp:222-224): 16 in its float build, 8 in its
  * double build (AVX-512), so the two builds differ in more than rounding.

@@ -270,11 +270,15 @@ class vector_field {
 // src/data/sim_data.h:11-24.  E, B, P are the evolved fields; B0 holds the
 // force-free current J, as the reference's EZ solvers write it there
 // (field_solver_EZ.cu:580-581); divE, divB are the last stage's divergences.
-// The per-cell energy-change diagnostics dU_* of the CPU build are not kept.
+// dU_* are the CPU build's per-cell energy-change diagnostics, written when
+// the solver's set_energy_diag(true) is on (their device arrays are made on
+// first use; sync_to_host() leaves them out: call their own sync_to_host).
 class sim_data {
  public:
   vector_field<Scalar> E, B, B0;
   multi_array<Scalar> P, divB, divE;
+  multi_array<Scalar> dU_EgtB, dU_Epar, dU_KO;
+  multi_array<Scalar> dU_EgtB_cum, dU_Epar_cum, dU_KO_cum;
   const sim_environment& env;
 
   explicit sim_data(const sim_environment& e) : E(e.grid()), B(e.grid()), B0(e.grid()), env(e) {
@@ -282,6 +286,9 @@ class sim_data {
     P = multi_array<Scalar>(g.dims[0], g.dims[1], g.dims[2]);
     divB = multi_array<Scalar>(g.dims[0], g.dims[1], g.dims[2]);
     divE = multi_array<Scalar>(g.dims[0], g.dims[1], g.dims[2]);
+    multi_array<Scalar>* du[6] = {&dU_EgtB, &dU_Epar, &dU_KO,
+                                  &dU_EgtB_cum, &dU_Epar_cum, &dU_KO_cum};
+    for (auto* a : du) *a = multi_array<Scalar>(g.dims[0], g.dims[1], g.dims[2]);
     coffee_check(coffee_fields_create(e.handle(), (int)sizeof(Scalar), &m_fields), "sim_data");
     for (int i = 0; i < 3; ++i) {
       E.data(i).bind(m_fields, COFFEE_EX + i);
@@ -291,6 +298,7 @@ class sim_data {
     P.bind(m_fields, COFFEE_P);
     divE.bind(m_fields, COFFEE_DIVE);
     divB.bind(m_fields, COFFEE_DIVB);
+    for (int i = 0; i < 6; ++i) du[i]->bind(m_fields, COFFEE_DU_EGTB + i);
   }
   ~sim_data() { coffee_fields_destroy(m_fields); }
   sim_data(const sim_data&) = delete;
@@ -339,6 +347,11 @@ class field_solver_EZ {
   field_solver_EZ(const field_solver_EZ&) = delete;
   field_solver_EZ& operator=(const field_solver_EZ&) = delete;
 
+  // Keep the CPU build's energy-change diagnostics in sim_data::dU_*
+  // (coffee_solver_set_energy_diag).
+  void set_energy_diag(bool enable) {
+    coffee_check(coffee_solver_set_energy_diag(m_solver, enable ? 1 : 0), "set_energy_diag");
+  }
   // One step: 5 LSRK stages + Kreiss-Oliger, clamps, boundaries, guards.
   void evolve_fields(Scalar time) {
     coffee_check(coffee_solver_step(m_solver, (double)time, 1), "evolve_fields");

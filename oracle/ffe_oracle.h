@@ -66,11 +66,15 @@ typedef struct oracle_params {
 /* Advance E, B, P by `nsteps` full steps starting at `time0`.  `fields` holds
  * 7 arrays (Ex Ey Ez Bx By Bz P) of dims = N + 2*guard each, guards
  * included.  Optional `aux` (may be NULL) receives J (3 arrays), divE, divB
- * of the last stage.  Returns 0, or a negative code on bad input / OOM. */
+ * of the last stage.  Optional `diag` (may be NULL; CPU-build semantics
+ * only) holds the 6 energy-change arrays dU_EgtB, dU_Epar, dU_KO,
+ * dU_EgtB_cum, dU_Epar_cum, dU_KO_cum (sim_data.h:15-16): the first three are
+ * rewritten every step, the _cum ones accumulated from their values on
+ * entry.  Returns 0, or a negative code on bad input / OOM. */
 int oracle_evolve_f32(const oracle_params* p, float* const* fields, float* const* aux,
-                      int nsteps, double time0);
+                      float* const* diag, int nsteps, double time0);
 int oracle_evolve_f64(const oracle_params* p, double* const* fields, double* const* aux,
-                      int nsteps, double time0);
+                      double* const* diag, int nsteps, double time0);
 
 #ifdef __cplusplus
 }

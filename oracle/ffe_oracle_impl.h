@@ -340,8 +340,13 @@ static void FN(rk_step_cpu)(const oracle_params* p, const FN(grid_t) * g, REAL* 
   }
 }
 
-/* clean_epar_check_eGTb of the CPU build (field_solver_EZ.cpp:552-634) */
-static void FN(clamps_cpu)(const oracle_params* p, const FN(grid_t) * g, REAL* const* U) {
+/* clean_epar_check_eGTb of the CPU build (field_solver_EZ.cpp:552-634).  With
+ * dg (the energy-change arrays dU_EgtB, dU_Epar, dU_KO and their _cum), the
+ * change of |E|^2 by the E.B cleaning is added to dU_Epar and dU_Epar_cum and
+ * the change of |E|^2 by both clamps (from before the cleaning) to dU_EgtB
+ * and dU_EgtB_cum, as the reference accumulates them. */
+static void FN(clamps_cpu)(const oracle_params* p, const FN(grid_t) * g, REAL* const* U,
+                           REAL* const* dg) {
   const int sh = p->shift_ghost;
   REAL *Ex = U[0], *Ey = U[1], *Ez = U[2], *Bx = U[3], *By = U[4], *Bz = U[5];
   LOOP_BOX(g, sh) {
@@ -350,6 +355,7 @@ static void FN(clamps_cpu)(const oracle_params* p, const FN(grid_t) * g, REAL* c
     REAL ex = Ex[ijk], ey = Ey[ijk], ez = Ez[ijk];
     const REAL B2 = FN(floor_tiny)(FMAR(bz, bz, FMAR(by, by, bx * bx)));
     const REAL EB = FMAR(bz, ez, FMAR(by, ey, bx * ex));
+    const REAL u0 = FMAR(ez, ez, FMAR(ey, ey, ex * ex));
     ex = ex - (EB * bx) / B2;
     ey = ey - (EB * by) / B2;
     ez = ez - (EB * bz) / B2;
@@ -360,6 +366,14 @@ static void FN(clamps_cpu)(const oracle_params* p, const FN(grid_t) * g, REAL* c
       ey = ey * s;
       ez = ez * s;
     }
+    if (dg) {
+      const REAL dp = E2 - u0;
+      dg[4][ijk] = dp + dg[4][ijk];
+      dg[1][ijk] = dg[1][ijk] + dp;
+      const REAL dgt = FMAR(ez, ez, FMAR(ey, ey, ex * ex)) - u0;
+      dg[3][ijk] = dgt + dg[3][ijk];
+      dg[0][ijk] = dg[0][ijk] + dgt;
+    }
     Ex[ijk] = ex; Ey[ijk] = ey; Ez[ijk] = ez;
   }
 }
@@ -368,7 +382,7 @@ static void FN(clamps_cpu)(const oracle_params* p, const FN(grid_t) * g, REAL* c
  * f + KO(f) * (-KOeps * KO_const), the product fused; KO sums the axes
  * x, y, z left to right */
 static void FN(kreiss_oliger_cpu)(const oracle_params* p, const FN(grid_t) * g, REAL* const* U,
-                                  REAL* const* tmp) {
+                                  REAL* const* tmp, REAL* const* dg) {
   const int sh = p->shift_ghost;
   const size_t s1 = (size_t)g->d0, s2 = (size_t)g->d0 * g->d1;
   LOOP_BOX(g, sh) {
@@ -380,7 +394,18 @@ static void FN(kreiss_oliger_cpu)(const oracle_params* p, const FN(grid_t) * g, 
   const REAL c = (REAL)p->KOeps * (REAL)0.015625;
   LOOP_BOX(g, sh) {
     size_t ijk = (size_t)i + ((size_t)j + (size_t)k * g->d1) * g->d0;
+    /* |E|^2 + |B|^2 before and after: dU_KO = the change, dU_KO_cum += it
+     * (field_solver_EZ.cpp:398-455) */
+    const REAL e0 = FMAR(U[2][ijk], U[2][ijk], FMAR(U[1][ijk], U[1][ijk], U[0][ijk] * U[0][ijk]));
+    const REAL b0 = FMAR(U[5][ijk], U[5][ijk], FMAR(U[4][ijk], U[4][ijk], U[3][ijk] * U[3][ijk]));
     for (int f = 0; f < 6; ++f) U[f][ijk] = FMAR(c, tmp[f][ijk], U[f][ijk]);
+    if (dg) {
+      const REAL e1 = FMAR(U[2][ijk], U[2][ijk], FMAR(U[1][ijk], U[1][ijk], U[0][ijk] * U[0][ijk]));
+      const REAL b1 = FMAR(U[5][ijk], U[5][ijk], FMAR(U[4][ijk], U[4][ijk], U[3][ijk] * U[3][ijk]));
+      const REAL du = (b1 + e1) - (b0 + e0);
+      dg[5][ijk] = du + dg[5][ijk];
+      dg[2][ijk] = du;
+    }
   }
 }
 
@@ -646,8 +671,8 @@ static void FN(kreiss_oliger)(const oracle_params* p, const FN(grid_t) * g, REAL
   }
 }
 
-int FN(oracle_evolve)(const oracle_params* p, REAL* const* U, REAL* const* aux, int nsteps,
-                      double time0) {
+int FN(oracle_evolve)(const oracle_params* p, REAL* const* U, REAL* const* aux,
+                      REAL* const* dg, int nsteps, double time0) {
   FN(grid_t) g;
   g.d0 = p->N[0] + 2 * p->guard[0];
   g.d1 = p->N[1] + 2 * p->guard[1];
@@ -692,12 +717,16 @@ int FN(oracle_evolve)(const oracle_params* p, REAL* const* U, REAL* const* aux, 
   const REAL dt = (REAL)p->dt;
   const int cpu = p->semantics == ORACLE_SEM_CPU_REF;
   const int absorbing = 1; /* both builds call it at the last stage */
+  if (!cpu) dg = NULL; /* the GPU build keeps no energy-change arrays */
   for (int step = 0; step < nsteps; ++step) {
     for (int f = 0; f < 7; ++f) memcpy(Un[f], U[f], g.n * sizeof(REAL));
+    /* evolve_fields zeroes dU_KO, dU_Epar, dU_EgtB (field_solver_EZ.cpp:1019-1021) */
+    if (dg)
+      for (int f = 0; f < 3; ++f) memset(dg[f], 0, g.n * sizeof(REAL));
     for (int st = 0; st < 5; ++st) {
       if (cpu) {
         FN(rk_step_cpu)(p, &g, U, dU, aux, (REAL)As_d[st], (REAL)Bs_d[st]);
-        FN(clamps_cpu)(p, &g, U);
+        FN(clamps_cpu)(p, &g, U, dg);
       } else {
         FN(rk_step)(p, &g, U, dU, aux, (REAL)As_d[st], (REAL)Bs_d[st]);
         FN(clamps)(p, &g, U);
@@ -710,8 +739,8 @@ int FN(oracle_evolve)(const oracle_params* p, REAL* const* U, REAL* const* aux, 
     }
     /* the KO scratch reuses the start-of-step copies, as the reference does */
     if (cpu) {
-      FN(kreiss_oliger_cpu)(p, &g, U, Un);
-      FN(clamps_cpu)(p, &g, U);
+      FN(kreiss_oliger_cpu)(p, &g, U, Un, dg);
+      FN(clamps_cpu)(p, &g, U, dg);
     } else {
       FN(kreiss_oliger)(p, &g, U, Un);
       FN(clamps)(p, &g, U);

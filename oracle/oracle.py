@@ -103,15 +103,19 @@ def _load():
             fn = getattr(lib, name)
             fn.restype = ctypes.c_int
             fn.argtypes = [ctypes.POINTER(OracleParams), ctypes.POINTER(ctypes.POINTER(ct)),
-                           ctypes.POINTER(ctypes.POINTER(ct)), ctypes.c_int, ctypes.c_double]
+                           ctypes.POINTER(ctypes.POINTER(ct)), ctypes.POINTER(ctypes.POINTER(ct)),
+                           ctypes.c_int, ctypes.c_double]
         _lib = lib
     return _lib
 
 
 def run_port(p: SimParams, fields, nsteps: int, time0: float = 0.0,
-             semantics: int = SEM_CPU_REF, taper_lanes: int | None = None, aux: bool = False):
+             semantics: int = SEM_CPU_REF, taper_lanes: int | None = None, aux: bool = False,
+             diag: list | None = None):
     """Advance copies of ``fields`` (7 arrays, float32 or float64) by ``nsteps``
-    with the C restatement.  Returns (fields, aux_arrays_or_None)."""
+    with the C restatement.  Returns (fields, aux_arrays_or_None).  ``diag``:
+    6 arrays dU_EgtB, dU_Epar, dU_KO, dU_EgtB_cum, dU_Epar_cum, dU_KO_cum,
+    updated in place (CPU-build semantics)."""
     lib = _load()
     dt = fields[0].dtype
     if taper_lanes is None:
@@ -125,9 +129,15 @@ def run_port(p: SimParams, fields, nsteps: int, time0: float = 0.0,
     if aux:
         auxa = [np.zeros_like(arrs[0]) for _ in range(5)]
         auxp = (P * 5)(*[a.ctypes.data_as(P) for a in auxa])
+    dgp = None
+    if diag is not None:
+        for a in diag:
+            if a.dtype != dt or not a.flags.c_contiguous:
+                raise ValueError("diag arrays must be contiguous and of the fields' dtype")
+        dgp = (P * 6)(*[a.ctypes.data_as(P) for a in diag])
     op = to_oracle_params(p, semantics, taper_lanes)
     fn = lib.oracle_evolve_f32 if dt == np.float32 else lib.oracle_evolve_f64
-    rc = fn(ctypes.byref(op), ptrs, auxp, int(nsteps), float(time0))
+    rc = fn(ctypes.byref(op), ptrs, auxp, dgp, int(nsteps), float(time0))
     if rc != 0:
         raise RuntimeError(f"oracle_evolve failed with {rc}")
     return arrs, auxa
@@ -143,8 +153,11 @@ def ref_binary(dtype=np.float32) -> str:
 
 
 def run_reference(p: SimParams, fields, nsteps: int, time0: float = 0.0, aux: bool = False,
-                  workdir: str | None = None, timeout: float | None = None):
-    """Run the reference's own CPU build.  Returns (fields, aux_or_None, info)."""
+                  workdir: str | None = None, timeout: float | None = None, diag: bool = False):
+    """Run the reference's own CPU build.  Returns (fields, aux_or_None, info);
+    with ``diag`` info["diag"] holds the energy-change arrays dU_EgtB,
+    dU_Epar, dU_KO, dU_EgtB_cum, dU_Epar_cum, dU_KO_cum (the _cum ones zeroed
+    before the first step)."""
     dt = fields[0].dtype
     exe = ref_binary(dt)
     if not os.path.exists(exe):
@@ -157,7 +170,8 @@ def run_reference(p: SimParams, fields, nsteps: int, time0: float = 0.0, aux: bo
         fin = os.path.join(wd, "in.fld")
         fout = os.path.join(wd, "out.fld")
         write_fld(fin, fields, guard=tuple(p.guard), time=time0)
-        cmd = [exe, fin, fout, str(int(nsteps))] + (["--aux"] if aux else [])
+        cmd = [exe, fin, fout, str(int(nsteps))] + (["--aux"] if aux else []) + \
+            (["--diag"] if diag else [])
         env = dict(os.environ, COFFEE_ORACLE_CONFIG=cfg)
         r = subprocess.run(cmd, cwd=wd, env=env, capture_output=True, text=True,
                            timeout=timeout)
@@ -167,6 +181,9 @@ def run_reference(p: SimParams, fields, nsteps: int, time0: float = 0.0, aux: bo
         ff = read_fld(fout)
         out = [a.copy() for a in ff.arrays[:7]]
         auxa = [a.copy() for a in ff.arrays[7:12]] if aux else None
+        if diag:
+            k = 12 if aux else 7
+            info["diag"] = [a.copy() for a in ff.arrays[k:k + 6]]
         return out, auxa, info
     finally:
         if own:

@@ -1,6 +1,6 @@
 // Driver for the reference's own CPU EZ solver (test infrastructure only).
 //
-// Usage:  coffee_ref_{float,double} IN.fld OUT.fld NSTEPS [--aux] [--warmup W]
+// Usage:  coffee_ref_{float,double} IN.fld OUT.fld NSTEPS [--aux] [--diag] [--warmup W]
 //
 // The TOML config is read by the reference's parse_config through the
 // single-rank sim_environment double (ref_env.cpp): $COFFEE_ORACLE_CONFIG or
@@ -13,7 +13,11 @@
 //   3. constructs the reference field_solver_EZ and calls evolve_fields
 //      NSTEPS times, advancing time by dt as src/main-alfven3d.cpp:117-119;
 //   4. writes E, B, P (and with --aux also J = the B0 arrays, divE, divB,
-//      src/algorithms/field_solver_EZ.cpp:149-200) to OUT.fld;
+//      src/algorithms/field_solver_EZ.cpp:149-200; with --diag also the
+//      energy-change arrays dU_EgtB, dU_Epar, dU_KO, dU_EgtB_cum,
+//      dU_Epar_cum, dU_KO_cum of src/data/sim_data.h:15-16, the _cum ones
+//      set to zero before the first step, as the reference's exporter leaves
+//      them after an output, src/utils/data_exporter.cpp:633-638) to OUT.fld;
 //   5. prints one JSON line with the wall time of step 3; with --warmup W,
 //      W further evolve_fields calls run first, untimed.
 // The reference prints a timer line per phase per stage to stdout; those are
@@ -38,16 +42,18 @@ using namespace Coffee;
 
 int main(int argc, char** argv) {
   if (argc < 4) {
-    std::fprintf(stderr, "usage: %s IN.fld OUT.fld NSTEPS [--aux] [--warmup W]\n", argv[0]);
+    std::fprintf(stderr, "usage: %s IN.fld OUT.fld NSTEPS [--aux] [--diag] [--warmup W]\n",
+                 argv[0]);
     return 2;
   }
   const std::string in_path = argv[1], out_path = argv[2];
   const long nsteps = std::atol(argv[3]);
-  bool aux = false;
+  bool aux = false, diag = false;
   long warmup = 0;
   for (int a = 4; a < argc; ++a) {
     const std::string opt = argv[a];
     if (opt == "--aux") aux = true;
+    else if (opt == "--diag") diag = true;
     else if (opt == "--warmup" && a + 1 < argc) warmup = std::atol(argv[++a]);
     else {
       std::fprintf(stderr, "unknown option %s\n", opt.c_str());
@@ -90,6 +96,9 @@ int main(int argc, char** argv) {
   payload.shrink_to_fit();
 
   field_solver_EZ solver(data, env);
+  data.dU_EgtB_cum.assign(0.0);
+  data.dU_Epar_cum.assign(0.0);
+  data.dU_KO_cum.assign(0.0);
 
   // Silence the reference's per-phase timer prints while it runs.
   std::fflush(stdout);
@@ -124,6 +133,14 @@ int main(int argc, char** argv) {
     out.push_back(data.B0.host_ptr(2));
     out.push_back(data.divE.host_ptr());
     out.push_back(data.divB.host_ptr());
+  }
+  if (diag) {
+    out.push_back(data.dU_EgtB.host_ptr());
+    out.push_back(data.dU_Epar.host_ptr());
+    out.push_back(data.dU_KO.host_ptr());
+    out.push_back(data.dU_EgtB_cum.host_ptr());
+    out.push_back(data.dU_Epar_cum.host_ptr());
+    out.push_back(data.dU_KO_cum.host_ptr());
   }
   fld_header hout = hin;
   hout.nfields = (int)out.size();

@@ -180,3 +180,28 @@ def test_config1_fast_arithmetic():
     ok, rep = fp32_parity(out, ref32, ref64)
     print(rep)
     assert ok, rep
+
+
+@pytest.mark.parametrize("name", ["alfven16", "turb16", "wide"])
+def test_energy_diagnostics_bit_for_bit(name):
+    """The CPU build's energy-change diagnostics (dU_EgtB, dU_Epar, dU_KO and
+    the _cum sums from zero) after 3 steps: against the restatement (itself
+    bit for bit the reference float build, tests/test_oracle.py) and against
+    the reference where it is built, bit for bit on the interior."""
+    if name == "wide":
+        p, f32 = wide_box_case()
+    else:
+        p, d = load_golden(name)
+        f32 = list(d["in_f32"])
+    out, extra = run_flat(p, f32, 3, energy_diag=True)
+    dg = [np.zeros_like(f32[0]) for _ in range(6)]
+    ref, _ = oracle.run_port(p, f32, 3, taper_lanes=16, diag=dg)
+    sl = interior(p)
+    for f in range(7):
+        assert count_differing(out[f], ref[f]) == 0, (name, f)
+    for k in range(6):
+        assert count_differing(extra[k][sl], dg[k][sl]) == 0, (name, "dU", k)
+    if oracle.reference_available(np.float32):
+        _, _, info = oracle.run_reference(p, f32, 3, diag=True)
+        for k in range(6):
+            assert count_differing(extra[k][sl], info["diag"][k][sl]) == 0, (name, "ref dU", k)

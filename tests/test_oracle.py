@@ -89,3 +89,24 @@ def test_port_is_the_reference_across_the_taper():
     out, _ = oracle.run_port(p, f32, 3, taper_lanes=16)
     for f in range(7):
         assert count_differing(out[f], ref[f]) == 0, (f, rel_l2(out[f], ref[f]))
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("name", ["alfven16", "turb16", "wide"])
+def test_port_energy_diagnostics_are_the_reference(name):
+    """The CPU build's energy-change arrays (dU_EgtB, dU_Epar, dU_KO and the
+    _cum sums, the latter from zero) after 3 steps, bit for bit on the
+    interior, from the reference float build itself."""
+    if name == "wide":
+        p, f32 = wide_box_case()
+    else:
+        p, d = load_golden(name)
+        f32 = list(d["in_f32"])
+    _, _, info = oracle.run_reference(p, f32, 3, diag=True)
+    dg = [np.zeros_like(f32[0]) for _ in range(6)]
+    oracle.run_port(p, f32, 3, taper_lanes=16, diag=dg)
+    g = p.guard
+    sl = tuple(slice(g[a], g[a] + p.N[a]) for a in (2, 1, 0))
+    for k in range(6):
+        assert count_differing(dg[k][sl], info["diag"][k][sl]) == 0, (name, k)
+    assert float(np.abs(info["diag"][2][sl]).max()) > 0
