@@ -571,9 +571,11 @@ VARIANT_STAGE_BYTES = {"gr-wald": 136, "logsph-batch": 112, "logsph": 112, "cyl-
                        "yee-wave": 72, "yee-pulsar": 72, "gryee-wald": 112}
 
 
-def _variant_cases(workload, n=512):
+def _variant_cases(workload, n=512, batch_runs=64):
     """(list of (solver class name, params, FP32 fields), description); n is
-    the grid side of the staggered workloads (512 is the benchmark)."""
+    the grid side of the staggered workloads (512 is the benchmark),
+    batch_runs the number of runs of the log-spherical batch (64 is the
+    benchmark; the first runs of the seeded draw)."""
     import numpy as np
 
     from coffee_b200 import problems
@@ -616,12 +618,12 @@ def _variant_cases(workload, n=512):
     rng = np.random.default_rng(20261203)
     sizes = [(512, 256), (768, 384), (1024, 512), (2048, 1024)]
     runs = []
-    for _ in range(64):
+    for _ in range(batch_runs):
         nr, nth = sizes[int(rng.integers(len(sizes)))]
         r_lc = float(rng.uniform(3.0, 10.0))
         p = problems.sph_pulsar_params(nr=nr, nth=nth, guard=4, omega=1.0 / r_lc)
         runs.append(("FieldSolverEZSpherical", "sph", p, problems.sph_pulsar_fields(p, np.float32)))
-    return runs, {"workload": "logsph-batch64", "runs": 64,
+    return runs, {"workload": f"logsph-batch{batch_runs}", "runs": batch_runs,
                   "grids": "r x theta drawn from 512x256, 768x384, 1024x512, 2048x1024 (seeded)",
                   "r": [1, 100], "R_LC": [3, 10], "launch": "one kernel per phase for all runs"}
 
@@ -638,7 +640,7 @@ def run_variant(args):
 
         if rank != 0:
             return 0
-        runs, cfg = _variant_cases(args.workload, args.n)
+        runs, cfg = _variant_cases(args.workload, args.n, args.batch_runs)
         secs, cells = 0.0, 0
         for _cls, name, p, f in runs:
             oracle.run_reference_gpu(name, p, f, args.warmup)
@@ -664,7 +666,7 @@ def run_variant(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
-    runs, cfg = _variant_cases(args.workload, args.n)
+    runs, cfg = _variant_cases(args.workload, args.n, args.batch_runs)
     objs = []
     cells = 0
     for cls_name, _name, p, f in runs:
@@ -766,6 +768,23 @@ def run_variant(args):
                     "h2d_bytes_per_step": nbytes / args.steps,
                     "d2h_bytes_per_step": nbytes / args.steps},
             "clocks": clk}
+    if batch is not None:
+        # the persistent mode: every call one cooperative launch with bounded
+        # grid-wide barriers between the phases (it synchronises per call)
+        batch.set_persistent(True)
+        advance(args.warmup)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        advance(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        pms = e0.elapsed_time(e1)
+        batch.set_persistent(False)
+        line["persistent"] = {
+            "ms_per_step": pms / args.steps,
+            "value": job_throughput(cells, args.steps, 1, pms / 1e3),
+            "frac": BYTES_STEP * cells / (pms / args.steps / 1e3) / 1e9 / peak,
+            "launches": 2, "note": "per call: 1 axis launch, 1 cooperative launch of all steps"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if batch is not None:
@@ -866,7 +885,10 @@ def run_surrogate(args):
             "conv_48_16_mma_sync": {"ms": mma_ms, "tflops": mma_flops / (mma_ms / 1e3) / 1e12},
             "gpu_launches": None, "clocks": clk}
     if args.study:
-        line["warm_start_study"] = sg.warm_start_study()
+        # the configured oblique rotator: 384^3, R* = 12 and R_LC = 60 cells,
+        # the network on the 128^3 grid of the same box (surrogate.rotator_study)
+        line["warm_start_study"] = sg.rotator_study(n_train=args.study_train,
+                                                    iters=args.study_iters)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -893,8 +915,14 @@ def main():
     ap.add_argument("--workload", default="turbulence",
                     choices=["turbulence", "gr-wald", "logsph-batch", "logsph", "cyl-pulsar",
                              "yee-wave", "yee-pulsar", "gryee-wald", "surrogate"])
+    ap.add_argument("--batch-runs", type=int, default=64,
+                    help="runs of the logsph-batch workload (64 is the benchmark)")
     ap.add_argument("--study", action="store_true",
                     help="with --workload surrogate: also run the warm-start study")
+    ap.add_argument("--study-train", type=int, default=40,
+                    help="training runs (384^3 each) of the warm-start study")
+    ap.add_argument("--study-iters", type=int, default=2000,
+                    help="training iterations of the warm-start study")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

@@ -118,6 +118,8 @@ SIGNATURES = {
     "coffee_batch_step": (_i, [_vp, _P(_d), _i]),
     "coffee_batch_info": (_i, [_vp, _P(_i), _P(_i), _P(_i), _P(_d)]),
     "coffee_batch_destroy": (_i, [_vp]),
+    "coffee_batch_set_persistent": (_i, [_vp, _i]),
+    "coffee_batch_set_wait_limit": (_i, [_vp, ctypes.c_longlong, _i]),
     "coffee_evolve_noalloc": (_i, [_P(CoffeeParams), _i, _P(_vp), _d, _i, _vp]),
     # learned warm start (include/coffee_surrogate.h); all pointers are device pointers
     "coffee_conv3d_forward": (_i, [_vp, _i, _i, _i, _i, _i, _vp, _i, _vp, _vp, _vp, _i,

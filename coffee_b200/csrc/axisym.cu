@@ -418,7 +418,7 @@ int sph_batch_plan_t(const SphRun* runs, int n, bool tune, cudaStream_t st, SphB
   if (rc) return rc;
   std::vector<T> hdt(n);
   for (int m = 0; m < n; ++m) hdt[m] = (T)runs[m].env->p.dt;
-  cudaError_t err = cudaMalloc(&pl->tnow, sizeof(T) * n);
+  cudaError_t err = cudaMalloc(&pl->tnow, 2 * sizeof(T) * n);
   if (err == cudaSuccess) err = cudaMalloc(&pl->tdt, sizeof(T) * n);
   if (err == cudaSuccess)
     err = cudaMemcpy(pl->tdt, hdt.data(), sizeof(T) * n, cudaMemcpyHostToDevice);
@@ -477,6 +477,54 @@ int sph_batch_capture(SphBatchPlan* pl) {
   return COFFEE_OK;
 }
 
+// Barriers per step of the persistent kernel: 5 x (stage, axis), KO, axis.
+constexpr int kBarriersPerStep = 12;
+
+// nsteps steps of the batch as cooperative launches of the persistent
+// kernel (as many steps per launch as the 32-bit arrival count allows),
+// then a read of the barrier status: COFFEE_E_TIMEOUT if a wait ran out.
+// Synchronises the stream.
+template <typename T>
+int sph_batch_persistent_t(SphBatchPlan* pl, int nsteps, cudaStream_t st) {
+  const long long per_step = (long long)kBarriersPerStep * pl->coop_grid;
+  const int max_steps = (int)std::min<long long>(nsteps, 0xFFFFFFFFLL / per_step - 1);
+  LsrkCoef<T> k;
+  for (int s = 0; s < 5; ++s) {
+    k.As[s] = (T)kAs[s];
+    k.Bs[s] = (T)kBs[s];
+    k.Cs[s] = (T)kCs[s];
+  }
+  const auto* tab = static_cast<const SphBatchEntry<T>*>(pl->table);
+  T* tbuf = static_cast<T*>(pl->tnow);
+  const T* tdt = static_cast<const T*>(pl->tdt);
+  GridSync* gs = static_cast<GridSync*>(pl->sync);
+  int n = pl->n, nb = pl->nblocks, na = pl->naxis;
+  for (int done = 0; done < nsteps;) {
+    int steps = std::min(max_steps, nsteps - done);
+    // an even count leaves the current times in row 0 for the next launch
+    // (the host sets row 0 again at the start of every call)
+    if (steps < nsteps - done && (steps & 1)) --steps;
+    COFFEE_CUDA_TRY(cudaMemsetAsync(gs, 0, sizeof(GridSync), st));
+    long long lim = pl->wait_ns;
+    int stall = pl->stall_block;
+    void* args[] = {(void*)&tab, (void*)&n,     (void*)&nb,  (void*)&na,  (void*)&tbuf,
+                    (void*)&tdt, (void*)&k,     (void*)&steps, (void*)&gs, (void*)&lim,
+                    (void*)&stall};
+    COFFEE_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)sph_batch_persistent_kernel<T>,
+                                                dim3(pl->coop_grid), dim3(pl->tx, pl->ty, 1),
+                                                args, 0, st));
+    GridSync h{};
+    COFFEE_CUDA_TRY(cudaMemcpyAsync(&h, gs, sizeof(GridSync), cudaMemcpyDeviceToHost, st));
+    COFFEE_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h.status != 0)
+      return fail(COFFEE_E_TIMEOUT,
+                  "persistent batch step: grid barrier %d gave up after %lld ns (block %d)",
+                  h.where, pl->wait_ns, h.block);
+    done += steps;
+  }
+  return COFFEE_OK;
+}
+
 // nsteps evolve_fields calls of every run of the batch, each from its own
 // time (advanced in field precision by its own dt): the stage / axis / KO
 // sequence of sph_steps with one launch per phase for the whole batch.
@@ -495,11 +543,14 @@ int sph_batch_run_t(SphBatchPlan* pl, const SphRun* runs, double* times, int nst
   sph_axis_batch_kernel<T><<<pl->naxis, 128, 0, st>>>(
       static_cast<const SphBatchEntry<T>*>(pl->table), n, 0);
   COFFEE_CUDA_TRY(cudaGetLastError());
-  if (use_graph && !pl->step) {
+  if (pl->persistent) {
+    int rc = sph_batch_persistent_t<T>(pl, nsteps, st);
+    if (rc) return rc;
+  } else if (use_graph && !pl->step) {
     int rc = sph_batch_capture<T>(pl);
     if (rc) return rc;
   }
-  for (int step = 0; step < nsteps; ++step) {
+  for (int step = 0; step < nsteps && !pl->persistent; ++step) {
     if (use_graph) {
       COFFEE_CUDA_TRY(cudaGraphLaunch(pl->step, st));
     } else {
@@ -528,7 +579,31 @@ int sph_batch_run(SphBatchPlan* plan, const SphRun* runs, double* times, int nst
                          : sph_batch_run_t<double>(plan, runs, times, nsteps, use_graph, st);
 }
 
+int sph_batch_set_persistent(SphBatchPlan* pl, bool on) {
+  if (on && !pl->sync) {
+    int per_sm = 0, dev = 0, sms = 0, coop = 0;
+    const void* fn = pl->elem == 4 ? (const void*)sph_batch_persistent_kernel<float>
+                                   : (const void*)sph_batch_persistent_kernel<double>;
+    COFFEE_CUDA_TRY(cudaGetDevice(&dev));
+    COFFEE_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    if (!coop) return fail(COFFEE_E_CUDA, "the device has no cooperative launch");
+    COFFEE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    COFFEE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, pl->tx * pl->ty, 0));
+    if (per_sm < 1) return fail(COFFEE_E_CUDA, "the persistent batch kernel does not fit an SM");
+    // no more CTAs than the largest phase has tiles
+    pl->coop_grid = std::max(1, std::min(per_sm * sms, std::max(pl->nblocks, pl->naxis)));
+    cudaError_t err = cudaMalloc(&pl->sync, sizeof(GridSync));
+    if (err != cudaSuccess) {
+      pl->sync = nullptr;
+      return fail(COFFEE_E_NOMEM, "persistent batch: %s", cudaGetErrorString(err));
+    }
+  }
+  pl->persistent = on;
+  return COFFEE_OK;
+}
+
 void sph_batch_free(SphBatchPlan* plan) {
+  if (plan->sync) cudaFree(plan->sync);
   if (plan->step) cudaGraphExecDestroy(plan->step);
   if (plan->cap) cudaStreamDestroy(plan->cap);
   if (plan->table) cudaFree(plan->table);

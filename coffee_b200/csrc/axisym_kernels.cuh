@@ -13,6 +13,7 @@
 // global memory directly.
 #pragma once
 
+#include "coffee_b200.h"
 #include "ez_common.cuh"
 
 namespace coffee {
@@ -41,6 +42,17 @@ constexpr int kSphMinBlocks = COFFEE_SPH_MIN_BLOCKS;
 constexpr int kSphBatchMinBlocks = COFFEE_SPH_BATCH_MIN_BLOCKS;
 constexpr int kCylStageMinBlocks = COFFEE_CYL_STAGE_MIN_BLOCKS;
 constexpr int kCylKoMinBlocks = COFFEE_CYL_KO_MIN_BLOCKS;
+
+// Load of a field value.  NC: through the read-only data path (__ldg), for
+// kernels in which nothing writes the array; otherwise a plain load, as the
+// persistent batch kernel needs: it reads in one phase what other CTAs wrote
+// in an earlier phase of the same launch, which the read-only path does not
+// promise to see.
+template <bool NC, typename T>
+__device__ __forceinline__ T ldf(const T* p) {
+  if constexpr (NC) return __ldg(p);
+  else return *p;
+}
 
 // ---- parameter block of the log-spherical solver ------------------------
 template <typename T>
@@ -186,8 +198,9 @@ __device__ __noinline__ V7<T> sph_absorb(const SphConst<T>& c, V7<T> v, V7<T> n,
 // kernel_compute_ElBl + kernel_rk_step1_sph + kernel_rk_step2_sph, then
 // kernel_Epar_sph, kernel_EgtB_sph, kernel_boundary_pulsar_sph and, in the
 // last stage, kernel_boundary_absorbing_sph (field_solver_EZ_spherical.cu:
-// 175-802, order of :967-990).  FIRST: As = 0, dU is not read.
-template <typename T, bool FIRST>
+// 175-802, order of :967-990).  FIRST: As = 0, dU is not read.  NC: field
+// loads through the read-only path (ldf).
+template <typename T, bool FIRST, bool NC = true>
 __device__ __forceinline__ void sph_stage_point(const SphConst<T>& c, const int i, const int j,
                                                 const F7<T>& u, const F7<T>& out,
                                                 const F7<T>& du, const F7<T>& un,
@@ -215,8 +228,8 @@ __device__ __forceinline__ void sph_stage_point(const SphConst<T>& c, const int 
   const T* By = u.p[4];
   const T* Bz = u.p[5];
   const T* P = u.p[6];
-  auto X = [&](const T* f, int k) { return __ldg(f + o + (k - 2)); };
-  auto Y = [&](const T* f, int k) { return __ldg(f + o + (k - 2) * d0); };
+  auto X = [&](const T* f, int k) { return ldf<NC>(f + o + (k - 2)); };
+  auto Y = [&](const T* f, int k) { return ldf<NC>(f + o + (k - 2) * d0); };
 
   // lowered fields at the stencil points: El_x = r^2 E_x, El_y = r^2 E_y,
   // El_z = (r sin th)^2 E_z (metric_sph.h:90-122)
@@ -245,7 +258,7 @@ __device__ __forceinline__ void sph_stage_point(const SphConst<T>& c, const int 
 
   T v[7];
 #pragma unroll
-  for (int a = 0; a < 7; ++a) v[a] = __ldg(u.p[a] + o);
+  for (int a = 0; a < 7; ++a) v[a] = ldf<NC>(u.p[a] + o);
   const T el[3] = {g11 * v[0], g11 * v[1], g33 * v[2]};
   const T bl[3] = {g11 * v[3], g11 * v[4], g33 * v[5]};
   T B2 = v[3] * bl[0] + v[4] * bl[1] + v[5] * bl[2];
@@ -349,8 +362,8 @@ __global__ void __launch_bounds__(256, kSphMinBlocks) sph_stage_kernel(const __g
 // kernel_EgtB_sph and kernel_boundary_pulsar_sph at t + dt
 // (field_solver_EZ_spherical.cu:444-555, order of :996-1004).  KO_geometry
 // weights the 6th differences by sqrt(gamma) (KO_2d6, :150-173), otherwise
-// they are plain (KO_2d0, :142-148).
-template <typename T>
+// they are plain (KO_2d0, :142-148).  NC as for sph_stage_point.
+template <typename T, bool NC = true>
 __device__ __forceinline__ void sph_ko_point(const SphConst<T>& c, const int i, const int j,
                                              const F7<T>& u, const F7<T>& out, const T tend) {
   const long long d0 = c.d0;
@@ -378,12 +391,12 @@ __device__ __forceinline__ void sph_ko_point(const SphConst<T>& c, const int i, 
     T tx = T(0), ty = T(0);
 #pragma unroll
     for (int k = 0; k < 7; ++k) {
-      tx += wx[k] * __ldg(f + o + (k - 3));
-      ty += wy[k] * __ldg(f + o + (k - 3) * d0);
+      tx += wx[k] * ldf<NC>(f + o + (k - 3));
+      ty += wy[k] * ldf<NC>(f + o + (k - 3) * d0);
     }
     T t = tx + ty;
     if (c.ko_geometry) t = t / gms;
-    v[a] = __ldg(f + o) + c.ko_c * t;
+    v[a] = ldf<NC>(f + o) + c.ko_c * t;
   }
   sph_clamps(c, v, rc * rc, (rc * sc) * (rc * sc));
   V7<T> w;
@@ -546,6 +559,174 @@ __global__ void sph_axis_batch_kernel(const SphBatchEntry<T>* __restrict__ tab, 
   const int i = e.c.lo0 + ((int)blockIdx.x - e.axis0) * blockDim.x + threadIdx.x;
   if (i >= e.c.hi0) return;
   sph_axis_column(e.c, i, on_b ? e.B : e.A);
+}
+
+// ---- the whole batch step in one persistent launch ----------------------
+// One cooperative launch (every CTA resident) runs nsteps steps of every run
+// of a batch: the phases of the per-phase launches (5 x (stage, axis), KO,
+// axis), each over all runs, separated by grid-wide barriers.  In a stage or
+// KO phase the CTAs take kTicketTiles tiles at a time from a ticket counter
+// (the tiles differ in cost: star and absorbing-layer points), asking for
+// the next ticket before working on the current one; the axis phases are
+// split evenly.  On each tile a CTA runs the single-run per-point code, so
+// the results are bitwise those of the per-phase launches.  The run times alternate between two
+// rows of `tbuf`: during step s the stages read row s & 1 and CTA 0 writes
+// t + dt into the other row, which the next step reads after the
+// barriers between.
+//
+// Every barrier wait is bounded, by `limit_ns` of %globaltimer and by an
+// iteration cap: a CTA that gives up records COFFEE_E_TIMEOUT, the barrier
+// and its block in GridSync and returns, and the CTAs still waiting see the
+// status and return as well, so the launch always ends.
+struct GridSync {
+  unsigned int count;  // arrivals so far (barrier q completes at (q + 1) * gridDim.x)
+  int status;          // 0, or COFFEE_E_TIMEOUT once a wait has run out
+  int where;           // index of the barrier that ran out
+  int block;           // the CTA whose wait ran out first
+  unsigned int tickets[2];  // tile tickets of the stage / KO phases (alternating)
+};
+// Tiles a CTA takes per ticket in the stage and KO phases.
+constexpr int kTicketTiles = 4;
+// Phase coefficients of the LSRK stages.
+template <typename T>
+struct LsrkCoef {
+  T As[5], Bs[5], Cs[5];
+};
+
+__device__ __forceinline__ long long globaltimer_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Grid-wide barrier number q (0, 1, ...).  `arrive` = false leaves this
+// CTA's arrival out (the stalled-CTA test of the wait limit).  Returns
+// false when the barrier gave up.
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned q, long long limit_ns,
+                                             bool arrive) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    int ok = 1;
+    if (arrive) {
+      __threadfence();  // this CTA's writes, seen by thread 0 through the barrier above
+      atomicAdd(&gs->count, 1u);
+    }
+    const unsigned target = (q + 1u) * gridDim.x;
+    const long long t0 = globaltimer_ns();
+    const long long cap = limit_ns / 32 + 4096;  // iterations, should the timer stall
+    for (long long it = 0;; ++it) {
+      unsigned c;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(c) : "l"(&gs->count) : "memory");
+      if (c >= target) break;
+      if (*(volatile int*)&gs->status != 0) {
+        ok = 0;
+        break;
+      }
+      if (it >= cap || globaltimer_ns() - t0 > limit_ns) {
+        if (atomicCAS(&gs->status, 0, (int)COFFEE_E_TIMEOUT) == 0) {
+          gs->where = (int)q;
+          gs->block = (int)blockIdx.x;
+        }
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    __threadfence();
+    ok_s = ok;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, kSphBatchMinBlocks) sph_batch_persistent_kernel(
+    const SphBatchEntry<T>* __restrict__ tab, const int n, const int nblocks, const int naxis,
+    T* __restrict__ tbuf, const T* __restrict__ tdt, const LsrkCoef<T> k, const int nsteps,
+    GridSync* __restrict__ gs, const long long limit_ns, const int stall_block) {
+  __shared__ __align__(16) unsigned char buf[sizeof(SphBatchEntry<T>)];
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  const int nt = blockDim.x * blockDim.y;
+  unsigned q = 0;  // barriers passed
+  auto barrier = [&]() {
+    const bool arrive = !(q == 0 && (int)blockIdx.x == stall_block);
+    return grid_barrier(gs, q++, limit_ns, arrive);
+  };
+  // one stage (s = 0..4) or, for s = 5, the KO pass, over every tile
+  __shared__ unsigned base_s;
+  unsigned tp = 0;  // tile phases begun
+  auto tiles = [&](const int s, const T* tcur) {
+    // tile phase tp takes its tickets from counter tp & 1; the other
+    // counter, last used by the tile phase before (finished at a barrier
+    // before this one began), is cleared for the next
+    unsigned* ctr = &gs->tickets[tp & 1];
+    if (blockIdx.x == 0 && tid == 0) gs->tickets[(tp + 1) & 1] = 0u;
+    ++tp;
+    if (tid == 0) base_s = atomicAdd(ctr, (unsigned)kTicketTiles);
+    __syncthreads();
+    unsigned base = base_s;
+    while (base < (unsigned)nblocks) {
+      unsigned pending = 0;
+      if (tid == 0) pending = atomicAdd(ctr, (unsigned)kTicketTiles);  // used after the tiles
+      const int bend = min((int)base + kTicketTiles, nblocks);
+      for (int b = (int)base; b < bend; ++b) {
+        const SphBatchEntry<T>& e = sph_batch_entry(tab, n, b, false, buf);
+        const int lt = b - e.tile0;
+        const int i = e.c.lo0 + (lt % e.tiles_x) * blockDim.x + threadIdx.x;
+        const int j = e.c.lo1 + (lt / e.tiles_x) * blockDim.y + threadIdx.y;
+        if (i < e.c.hi0 && j < e.c.hi1) {
+          if (s == 5) {
+            sph_ko_point<T, false>(e.c, i, j, e.B, e.A,
+                                   batch_time(tcur[e.index], T(1), tdt[e.index]));
+          } else {
+            const int to_b = (s % 2 == 0) ? 1 : 0;
+            int flags = 0;
+            if (s == 4) flags |= AX_LAST | (e.want_aux ? AX_AUX : 0);
+            if (s == 0 && e.c.absorbing) flags |= AX_WRITE_UN;
+            const T tst = batch_time(tcur[e.index], k.Cs[s], tdt[e.index]);
+            if (s == 0)
+              sph_stage_point<T, true, false>(e.c, i, j, e.A, e.B, e.dU, e.Un, e.aux, k.As[0],
+                                              k.Bs[0], tst, flags);
+            else
+              sph_stage_point<T, false, false>(e.c, i, j, to_b ? e.A : e.B, to_b ? e.B : e.A,
+                                               e.dU, e.Un, e.aux, k.As[s], k.Bs[s], tst, flags);
+          }
+        }
+        __syncthreads();  // buf is refilled for the next tile
+      }
+      if (tid == 0) base_s = pending;
+      __syncthreads();
+      base = base_s;
+    }
+  };
+  // the axis boundary of every run on buffer B (on_b) or A, 128 columns a tile
+  auto axis = [&](const int on_b) {
+    for (int b = blockIdx.x; b < naxis; b += gridDim.x) {
+      const SphBatchEntry<T>& e = sph_batch_entry(tab, n, b, true, buf);
+      if ((e.c.axis_lo >= 0 || e.c.axis_hi >= 0) && tid < 128) {
+        const int i = e.c.lo0 + (b - e.axis0) * 128 + tid;
+        if (i < e.c.hi0) sph_axis_column(e.c, i, on_b ? e.B : e.A);
+      }
+      __syncthreads();
+    }
+  };
+  for (int step = 0; step < nsteps; ++step) {
+    const T* tcur = tbuf + (step & 1) * n;
+    if (blockIdx.x == 0)
+      for (int m = tid; m < n; m += nt)
+        tbuf[((step + 1) & 1) * n + m] = batch_time(tcur[m], T(1), tdt[m]);
+    for (int s = 0; s < 5; ++s) {
+      tiles(s, tcur);
+      if (!barrier()) return;
+      axis((s % 2 == 0) ? 1 : 0);
+      if (!barrier()) return;
+    }
+    tiles(5, tcur);
+    if (!barrier()) return;
+    axis(0);
+    if (!barrier()) return;
+  }
 }
 
 // ---- cylindrical helpers ------------------------------------------------

@@ -968,6 +968,23 @@ extern "C" int coffee_batch_step(coffee_batch* b, double* times, int nsteps) {
                        b->stream);
 }
 
+extern "C" int coffee_batch_set_persistent(coffee_batch* b, int on) {
+  clear_error();
+  if (!b) return fail(COFFEE_E_INVALID, "coffee_batch_set_persistent: null argument");
+  COFFEE_CUDA_TRY(cudaSetDevice(b->device));
+  return sph_batch_set_persistent(&b->plan, on != 0);
+}
+
+extern "C" int coffee_batch_set_wait_limit(coffee_batch* b, long long limit_ns, int stall_block) {
+  clear_error();
+  if (!b) return fail(COFFEE_E_INVALID, "coffee_batch_set_wait_limit: null argument");
+  if (limit_ns <= 0) return fail(COFFEE_E_INVALID, "the wait limit must be > 0 ns");
+  if (stall_block < -1) return fail(COFFEE_E_INVALID, "stall_block must be >= -1");
+  b->plan.wait_ns = limit_ns;
+  b->plan.stall_block = stall_block;
+  return COFFEE_OK;
+}
+
 extern "C" int coffee_batch_destroy(coffee_batch* b) {
   if (!b) return COFFEE_OK;
   cudaSetDevice(b->device);

@@ -506,18 +506,18 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
       // in the reference arithmetic (XA) the unscaled quotient of diff1_4,
       // which curl_div scales and combines as the CPU build does.  EX
       // selects the exact division for the rare quotients the fast one
-      // flags in `tiny` (xa::div12_fast).
-      bool tiny = false;
+      // flags through the key minimum `kmin` (xa::div12_fast).
+      uint32_t kmin = 0xFFFFFFFFu;
       auto d1 = [&](auto fc, auto ex, T* dxyz) {
         constexpr int f = decltype(fc)::value;
         constexpr bool EX = decltype(ex)::value;
         constexpr int o = f * FB;
         if constexpr (XA) {
           dxyz[0] = xa::dq<EX>(lds<T, o + CEN - 2 * ES>(a0), lds<T, o + CEN - ES>(a0),
-                               lds<T, o + CEN + ES>(a0), lds<T, o + CEN + 2 * ES>(a0), tiny);
+                               lds<T, o + CEN + ES>(a0), lds<T, o + CEN + 2 * ES>(a0), kmin);
           dxyz[1] = xa::dq<EX>(lds<T, o + 2 * ES>(a0), lds<T, o + (SX + 2) * ES>(a0),
                                lds<T, o + (3 * SX + 2) * ES>(a0),
-                               lds<T, o + (4 * SX + 2) * ES>(a0), tiny);
+                               lds<T, o + (4 * SX + 2) * ES>(a0), kmin);
         } else {
           dxyz[0] = d1_4(lds<T, o + CEN - 2 * ES>(a0), lds<T, o + CEN - ES>(a0),
                          lds<T, o + CEN + ES>(a0), lds<T, o + CEN + 2 * ES>(a0), six);
@@ -528,7 +528,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
         u[f] = w[(S + 2) % 5][f];
         if constexpr (XA)
           dxyz[2] = xa::dq<EX>(w[S % 5][f], w[(S + 1) % 5][f], w[(S + 3) % 5][f],
-                               w[(S + 4) % 5][f], tiny);
+                               w[(S + 4) % 5][f], kmin);
         else
           dxyz[2] = d1_4(w[S % 5][f], w[(S + 1) % 5][f], w[(S + 3) % 5][f], w[(S + 4) % 5][f],
                          siz);
@@ -573,7 +573,7 @@ __global__ void __launch_bounds__(TX * TY, min_blocks<T, TX * TY>())
       // warp recomputes its derivatives with the exact division (the same
       // operands are still in shared memory and the window)
       if constexpr (XA)
-        if (__any_sync(amask, tiny)) derivatives(std::true_type{});
+        if (__any_sync(amask, kmin < xa::kTinyKey)) derivatives(std::true_type{});
       if constexpr (XA) {
         dv.gradP[0] = xa::mul(ix, dv.gradP[0]);
         dv.gradP[1] = xa::mul(iy, dv.gradP[1]);

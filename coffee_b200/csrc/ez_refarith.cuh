@@ -39,39 +39,44 @@ __device__ __forceinline__ float sqrt(float a) { return __fsqrt_rn(a); }
 __device__ __forceinline__ double sqrt(double a) { return __dsqrt_rn(a); }
 
 // t / 12, correctly rounded.  FP32: q = t (1/12), then one Newton
-// correction with the exact residual t - 12 q (an FMA), and the sign of t
-// (which the correction loses for t = -0).  An exhaustive check over every
-// finite float (on the CPU, with the same IEEE operations) shows that this
-// is the IEEE quotient for every t except 0 < |t| < 2^-124, whose quotient
-// is subnormal; `tiny` is set for those, and the caller recomputes them
-// with div12_exact.
-__device__ __forceinline__ float div12_fast(float t, bool& tiny) {
+// correction with the exact residual e = 12 q - t (an FMA): q - e/12 as
+// fma(e, -1/12, q), which also keeps the sign of a zero t.  An exhaustive
+// check over every finite float (on the CPU, with the same IEEE operations)
+// shows that this is the IEEE quotient for every t except
+// 0 < |t| < 2^-124, whose quotient is subnormal.  Those are found by an
+// integer key, 2 bits(t) - 1 (mod 2^32): it drops the sign, sends zero to
+// the largest value, and is below kTinyKey exactly for that range (the same
+// check covers all 2^32 patterns).  The caller keeps the running minimum of
+// the keys in `kmin` and recomputes with div12_exact when it is below
+// kTinyKey.
+constexpr uint32_t kTinyKey = 0x02FFFFFEu;
+__device__ __forceinline__ float div12_fast(float t, uint32_t& kmin) {
   constexpr float r12 = 1.0f / 12.0f;
-  float q = __fmul_rn(t, r12);
-  const float e = __fmaf_rn(-q, 12.0f, t);
-  q = copysignf(__fmaf_rn(e, r12, q), t);
-  tiny |= (fabsf(t) < 0x1p-124f) & (t != 0.0f);
-  return q;
+  const float q = __fmul_rn(t, r12);
+  const float e = __fmaf_rn(q, 12.0f, -t);
+  const uint32_t b = __float_as_uint(t);
+  kmin = min(kmin, b + b - 1u);
+  return __fmaf_rn(e, -r12, q);
 }
-__device__ __forceinline__ double div12_fast(double t, bool&) { return __ddiv_rn(t, 12.0); }
+__device__ __forceinline__ double div12_fast(double t, uint32_t&) { return __ddiv_rn(t, 12.0); }
 __device__ __forceinline__ float div12_exact(float t) {
-  bool tiny = false;
-  const float q = div12_fast(t, tiny);
-  return tiny ? __fdiv_rn(t, 12.0f) : q;
+  uint32_t k = 0xFFFFFFFFu;
+  const float q = div12_fast(t, k);
+  return k < kTinyKey ? __fdiv_rn(t, 12.0f) : q;
 }
 __device__ __forceinline__ double div12_exact(double t) { return __ddiv_rn(t, 12.0); }
 
 // diff1_4 of the reference (finite_diff_simd.h:15-25) before its inv_delta
 // factor: (((f-2 - 8 f-1) + 8 f+1) - f+2) / 12, the two products by 8 fused
 // (they are exact, so fused or not gives the same value).  EXACT = false
-// flags in `tiny` the inputs whose fast quotient may be off (div12_fast).
+// folds into `kmin` the key of the quotient's input (div12_fast).
 template <bool EXACT, typename T>
-__device__ __forceinline__ T dq(T m2, T m1, T p1, T p2, bool& tiny) {
+__device__ __forceinline__ T dq(T m2, T m1, T p1, T p2, uint32_t& kmin) {
   T t = fma(m1, (T)-8, m2);
   t = fma(p1, (T)8, t);
   t = sub(t, p2);
   if constexpr (EXACT) return div12_exact(t);
-  else return div12_fast(t, tiny);
+  else return div12_fast(t, kmin);
 }
 
 // diff6_2 of the reference (finite_diff_simd.h:41-58): each weighted term

@@ -41,9 +41,16 @@ struct SphBatchPlan {
   int order = 0;          // 0: runs in the given order, 1: largest first
   double tuned_ms = 0;    // first-stage time of the chosen layout
   void* tnow = nullptr;   // field-precision start time of the current step, per run
+                          // (2 rows of n: the persistent kernel alternates them)
   void* tdt = nullptr;    // field-precision dt, per run
   cudaStream_t cap = nullptr;          // stream the step is captured on
   cudaGraphExec_t step = nullptr;      // one captured step (made on first use)
+  // the persistent mode: one cooperative launch for all steps of a call
+  bool persistent = false;
+  int coop_grid = 0;                   // its CTAs (all resident)
+  void* sync = nullptr;                // GridSync of its barriers
+  long long wait_ns = 2000000000LL;    // limit of one barrier wait
+  int stall_block = -1;                // test: this CTA skips its first arrival
 };
 // Build the plan; with `tune`, time the first stage for every candidate tile
 // shape and run order (the first stage writes only scratch: the second field
@@ -55,6 +62,8 @@ int sph_batch_plan(const SphRun* runs, int n, int elem, bool tune, cudaStream_t 
 int sph_batch_run(SphBatchPlan* plan, const SphRun* runs, double* times, int nsteps,
                   bool use_graph, cudaStream_t st);
 void sph_batch_free(SphBatchPlan* plan);
+// Switch the persistent mode on or off (sizes its cooperative grid).
+int sph_batch_set_persistent(SphBatchPlan* plan, bool on);
 
 // GR force-free solver in Kerr-Schild coordinates (COFFEE_VARIANT_GR).
 int gr_check(const coffee_env* env);

@@ -398,6 +398,19 @@ class SphBatch:
                                          int(nsteps)))
         self.times = t
 
+    def set_persistent(self, on: bool = True):
+        """All steps of a ``step`` call in one cooperative launch with
+        bounded grid-wide barriers between the phases (bitwise the same
+        results); ``step`` then synchronises and raises ``CoffeeError``
+        (COFFEE_E_TIMEOUT) if a barrier wait ran out."""
+        check(self.lib.coffee_batch_set_persistent(self.handle, int(bool(on))))
+
+    def set_wait_limit(self, limit_ns: int, stall_block: int = -1):
+        """Limit of one barrier wait of the persistent mode (ns); stall_block
+        >= 0 makes that CTA leave out its first arrival (a test of the
+        limit)."""
+        check(self.lib.coffee_batch_set_wait_limit(self.handle, int(limit_ns), int(stall_block)))
+
     def info(self) -> dict:
         """The autotuner's choice: tile shape, run order, first-stage ms."""
         tx, ty, order, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()

@@ -8,8 +8,11 @@ Every arithmetic step of training and inference runs on the library's
 kernels (include/coffee_surrogate.h): BF16 tensor-core convolutions with
 FP32 accumulation for the forward pass and both gradients, and the
 pooling, activation, loss and Adam kernels.  torch provides the device
-memory only.  The training set is made by the flat solver itself: one
-rotating-star run per inclination.
+memory only.  The training set is made by the flat solver itself: oblique
+rotators run from their vacuum dipoles at full resolution and averaged onto
+the network's coarser grid (rotator_training_set); rotator_study measures
+the wall time to a settled spindown luminosity from the cold and the warm
+start.
 
 Network (channels-last, 3x3x3 convolutions, leaky ReLU with slope 0.1):
 
@@ -283,25 +286,15 @@ class UNet:
 
 # ------------------------------------------------------ the star problem
 
-def star_params(N=64, inclination_deg=30.0, omega=0.15):
-    """The rotating-star configuration of the warm-start study: an inclined
-    dipole star of radius 1.5 turning at omega (0.15: light cylinder 6.7) in a
-    box of half size 12 with an absorbing layer."""
-    p = problems.pulsar_params(N=N, guard=3, half_size=12.0, radius=1.5, omega=omega, pml=8)
-    a = math.radians(inclination_deg)
-    p.p1, p.p2, p.p3 = math.sin(a), 0.0, math.cos(a)
-    return p
-
-
 def _coords(p):
     Z, Y, X = problems._xyz(p, np.float32)
     return X, Y, Z
 
 
-def features(p, fields, inclination_deg):
+def features(p, fields, inclination_deg, omega_ref=0.15):
     """Input channels (D, H, W, 16) of the interior: B r^3 / R^3 of the
     dipole state, x, y, z / half size, the star mask, sin and cos of the
-    inclination, the spin omega / 0.15, zeros."""
+    inclination, the spin omega / omega_ref, zeros."""
     g = p.guard[0]
     X, Y, Z = (c[g:-g, g:-g, g:-g] for c in _coords(p))
     R = np.sqrt(X * X + Y * Y + Z * Z)
@@ -314,7 +307,7 @@ def features(p, fields, inclination_deg):
     out[..., 6] = (R < p.radius).astype(np.float32)
     a = math.radians(inclination_deg)
     out[..., 7], out[..., 8] = math.sin(a), math.cos(a)
-    out[..., 9] = p.omega / 0.15
+    out[..., 9] = p.omega / omega_ref
     return out
 
 
@@ -333,22 +326,6 @@ def target_and_mask(p, start, steady):
     mask = ((R > STAR_EDGE * p.radius) & (np.abs(X) < edge) & (np.abs(Y) < edge) &
             (np.abs(Z) < edge)).astype(np.float32)
     return out, mask
-
-
-def apply_prediction(p, start, pred):
-    """The warm-start fields: start + pred / scale outside 1.5 radii (the
-    star's own boundary condition sets the fields inside)."""
-    g = p.guard[0]
-    X, Y, Z = _coords(p)
-    R = np.sqrt(X * X + Y * Y + Z * Z)
-    scale = np.minimum((np.maximum(R, p.radius) / p.radius) ** 3, 1e4).astype(np.float32)
-    keep = R > STAR_EDGE * p.radius
-    out = [a.copy() for a in start]
-    for c in range(7):
-        full = np.zeros_like(start[c])
-        full[g:-g, g:-g, g:-g] = pred[..., c]
-        out[c] = np.where(keep, start[c] + full / scale, start[c]).astype(start[c].dtype)
-    return out
 
 
 # --------------------------------------------------------- warm-start study
@@ -380,22 +357,6 @@ def star_run(p, fields, steps, lum_radius, every=10):
     return out, hist
 
 
-def rotation_mean(hist, period):
-    """The luminosity averaged over the last rotation period at every
-    recorded step that has a full period behind it.  The flux of an oblique
-    rotator through a sphere is steady only on average: on a Cartesian grid
-    it is modulated at the rotation period."""
-    steps = np.array([s for s, _ in hist], float)
-    lums = np.array([l for _, l in hist], float)
-    out = []
-    for s in steps:
-        if s < period:
-            continue
-        sel = (steps > s - period) & (steps <= s)
-        out.append((int(s), float(lums[sel].mean())))
-    return out
-
-
 def settle_step(series, l_ref, tol=0.02):
     """The first step of `series` [(step, value)] from which the value stays
     within tol of l_ref to the end."""
@@ -407,110 +368,260 @@ def settle_step(series, l_ref, tol=0.02):
     return settled
 
 
-def _batch(samples):
+# ------------------------------------------ the configured oblique rotator
+# The warm-start configuration: a star of radius 12 cells with light
+# cylinder R_LC = 60 cells in a 384^3 box with an absorbing outer layer,
+# inclination in [0, 90] degrees, and a network on a 128^3 grid whose
+# prediction is trilinearly upsampled to 384^3.  The reference's star
+# boundary blends the star over 4 cells (d1 = 4 delta,
+# field_solver_EZ.cu:394-528), so the solver needs the star resolved by
+# about 12 cells: the same box run at 128^3 (a 4-cell star) gives a spindown
+# luminosity 12 times too large, at 192^3 4 times (measured).  The training
+# steady states are therefore full-resolution 384^3 runs, averaged over 3^3
+# cells onto the network's 128^3 grid of the same box; the network sees the
+# vacuum dipole there and predicts the change to the steady state.
+
+ROT_N = 384
+ROT_COARSE = 3
+ROT_RADIUS = 12.0
+ROT_RLC_TRAIN = (40.0, 80.0)
+ROT_RLC_TEST = 60.0
+ROT_OMEGA_REF = 1.0 / 60.0
+
+
+def rotator_params(N, inclination_deg, r_lc, pml=None):
+    """The oblique rotator on an N^3 box of unit cells centred on the star:
+    radius 12 cells, surface field of order 1 (b0 = R^3), light cylinder r_lc
+    cells, dipole inclined by inclination_deg to the spin axis, absorbing
+    layer pml cells (N/16 by default), dt = 0.4 cells."""
+    p = problems.pulsar_params(N=N, guard=3, half_size=N / 2.0, radius=ROT_RADIUS,
+                               omega=1.0 / r_lc, b0=ROT_RADIUS ** 3,
+                               pml=pml if pml is not None else max(8, N // 16))
+    a = math.radians(inclination_deg)
+    p.p1, p.p2, p.p3 = math.sin(a), 0.0, math.cos(a)
+    return p
+
+
+def coarse_params(p, coarse=ROT_COARSE):
+    """The network's grid of the box of p: N / coarse points whose point m is
+    the centre of the fine cells coarse m .. coarse m + coarse - 1."""
+    import copy
+    pc = copy.deepcopy(p)
+    pc.N = [n // coarse for n in p.N]
+    pc.lower = [l + 0.5 * (coarse - 1) for l in p.lower]
+    pc.pml = [max(1, m // coarse) for m in p.pml]
+    return pc
+
+
+def period_steps(p):
+    """Steps per rotation period."""
+    return 2 * math.pi / (p.omega * float(np.float32(p.dt)))
+
+
+def _pool(fine, p, coarse=ROT_COARSE):
+    """Mean over coarse^3 cells of the interior of a fine array (with guards),
+    returned with the coarse grid's guard cells (zeros)."""
+    g = p.guard[0]
+    a = fine[g:-g, g:-g, g:-g]
+    n = a.shape[0] // coarse
+    m = a.reshape(n, coarse, n, coarse, n, coarse).mean(axis=(1, 3, 5))
+    out = np.zeros((n + 2 * g,) * 3, dtype=fine.dtype)
+    out[g:-g, g:-g, g:-g] = m
+    return out
+
+
+_DIPOLE_BASIS = {}
+
+
+def dipole_start(p):
+    """The vacuum-dipole start of a rotator (pulsar_fields), from a cached
+    pair of basis fields: the dipole is linear in its moment (sin a, 0, cos a),
+    so each inclination costs one combination instead of a new evaluation
+    (which takes seconds at 384^3).  Agrees with pulsar_fields to FP32
+    rounding."""
+    key = (tuple(p.N), tuple(p.lower), p.b0, p.radius)
+    if key not in _DIPOLE_BASIS:
+        import copy
+        q = copy.deepcopy(p)
+        q.p1, q.p2, q.p3 = 1.0, 0.0, 0.0
+        bx = problems.pulsar_fields(q, np.float32)[3:6]
+        q.p1, q.p3 = 0.0, 1.0
+        bz = problems.pulsar_fields(q, np.float32)[3:6]
+        _DIPOLE_BASIS.clear()
+        _DIPOLE_BASIS[key] = (bx, bz)
+    bx, bz = _DIPOLE_BASIS[key]
+    zero = np.zeros_like(bx[0])
+    b = [(np.float32(p.p1) * bx[c] + np.float32(p.p3) * bz[c]).astype(np.float32)
+         for c in range(3)]
+    return [zero, zero.copy(), zero.copy()] + b + [zero.copy()]
+
+
+def rotator_sample(incl, r_lc, periods=2.0, N=ROT_N):
+    """One training sample: the N^3 rotator run `periods` of its rotation
+    periods from the vacuum dipole; returns the network's input, target and
+    mask on its coarse grid (host arrays)."""
+    p = rotator_params(N, incl, r_lc)
+    pc = coarse_params(p)
+    start = dipole_start(p)
+    steps = int(round(periods * period_steps(p)))
+    steady, _ = star_run(p, start, steps, 0.75 * r_lc, steps)
+    start_c = problems.pulsar_fields(pc, np.float32)
+    steady_c = [start_c[c] + _pool(steady[c] - start[c], p) for c in range(7)]
+    x = features(pc, start_c, incl, ROT_OMEGA_REF)
+    t, m = target_and_mask(pc, start_c, steady_c)
+    return x, t, m
+
+
+def rotator_training_set(n, periods=2.0, seed=20261203, N=ROT_N, r_lc_range=ROT_RLC_TRAIN):
+    """n samples with seeded inclinations in [0, 90] degrees and R_LC drawn
+    from r_lc_range (cells), on the GPU."""
     torch = _torch()
-    xs, ts, ms = [], [], []
-    for p, incl, start, steady in samples:
-        xs.append(features(p, start, incl))
-        t, m = target_and_mask(p, start, steady)
-        ts.append(t)
-        ms.append(m)
-    x = torch.from_numpy(np.stack(xs)).cuda().to(torch.bfloat16)
-    return x, torch.from_numpy(np.stack(ts)).cuda(), torch.from_numpy(np.stack(ms)).cuda()
+    rng = np.random.default_rng(seed)
+    xs, ts, ms, pairs = [], [], [], []
+    for _ in range(n):
+        incl = float(rng.uniform(0.0, 90.0))
+        r_lc = float(rng.uniform(*r_lc_range))
+        x, t, m = rotator_sample(incl, r_lc, periods, N)
+        xs.append(torch.from_numpy(x[None]).cuda().to(torch.bfloat16))
+        ts.append(torch.from_numpy(t[None]).cuda())
+        ms.append(torch.from_numpy(m[None]).cuda())
+        pairs.append((incl, r_lc))
+    return xs, ts, ms, pairs
 
 
-def train(net, samples, iters, lr=2e-3, log_every=50):
-    """Full-batch Adam on the library's kernels over samples
-    [(params, inclination, start fields, target fields)]; returns the loss
-    history."""
-    x, tgt, mask = _batch(samples)
+def train_stream(net, xs, ts, ms, iters, lr=2e-3, batch=2, seed=0, log_every=100):
+    """Adam over random mini-batches of the samples (xs, ts, ms on the GPU)."""
+    torch = _torch()
+    rng = np.random.default_rng(seed)
     losses = []
     for it in range(iters):
+        idx = rng.choice(len(xs), size=min(batch, len(xs)), replace=False)
+        x = torch.cat([xs[i] for i in idx])
+        t = torch.cat([ts[i] for i in idx])
+        m = torch.cat([ms[i] for i in idx])
         out = net.forward(x)
-        loss, dout = net.loss(out, tgt, mask)
+        loss, dout = net.loss(out, t, m)
         net.backward(dout)
-        rate = lr * (0.1 ** (it / max(1, iters)))
-        net.step(rate)
+        net.step(lr * (0.1 ** (it / max(1, iters))))
         if it % log_every == 0 or it == iters - 1:
             losses.append((it, float(loss)))
     check_tc()
     return losses
 
 
-def predict(net, p, start, incl):
+def upsampled_warm_start(net, p, start, incl):
+    """The warm start of the rotator p: the network's prediction on the
+    coarse grid, trilinearly upsampled to p's grid on the GPU and added to
+    the vacuum dipole outside 1.5 star radii and inside the absorbing layer.
+    Returns host arrays."""
     torch = _torch()
-    x = torch.from_numpy(features(p, start, incl)[None]).cuda().to(torch.bfloat16)
-    out = net.forward(x)
+    pc = coarse_params(p)
+    start_c = problems.pulsar_fields(pc, np.float32)
+    x = torch.from_numpy(features(pc, start_c, incl, ROT_OMEGA_REF)[None]).cuda()
+    out = net.forward(x.to(torch.bfloat16))  # (1, n, n, n, 16): scaled corrections
     check_tc()
-    return apply_prediction(p, start, out[0].cpu().numpy())
+    g = p.guard[0]
+    Z, Y, X = (c[g:-g, g:-g, g:-g] for c in problems._xyz(p, np.float32))
+    R = np.sqrt(X * X + Y * Y + Z * Z)
+    edge = p.size[0] / 2 - p.pml[0] * p.size[0] / p.N[0]
+    keep = ((R > STAR_EDGE * p.radius) & (np.abs(X) < edge) & (np.abs(Y) < edge) &
+            (np.abs(Z) < edge))
+    gc = pc.guard[0]
+    Zc, Yc, Xc = (c[gc:-gc, gc:-gc, gc:-gc] for c in problems._xyz(pc, np.float32))
+    Rc = np.sqrt(Xc * Xc + Yc * Yc + Zc * Zc)
+    scale_c = np.minimum((np.maximum(Rc, p.radius) / p.radius) ** 3, 1e4).astype(np.float32)
+    corr = out[0, ..., :7].permute(3, 0, 1, 2) / torch.from_numpy(scale_c).cuda()
+    up = torch.nn.functional.interpolate(corr[None], scale_factor=ROT_COARSE, mode="trilinear",
+                                         align_corners=False)[0].cpu().numpy()
+    warm = [a.copy() for a in start]
+    for c in range(7):
+        inner = warm[c][g:-g, g:-g, g:-g]
+        warm[c][g:-g, g:-g, g:-g] = np.where(keep, inner + up[c], inner)
+    return warm
 
 
-def warm_start_study(N=64, train_set=((0, 0.15), (15, 0.15), (30, 0.15), (45, 0.15), (60, 0.15),
-                                   (75, 0.15), (90, 0.15)),
-                     test_set=((38, 0.15), (68, 0.15)), periods=4.0, iters=2000, lum_radius=4.5,
-                     seed=0):
-    """Train the network on rotating-star runs at the (inclination in
-    degrees, spin) pairs of `train_set`, each run `periods` rotation periods from
-    its dipole; then for every held-out pair of `test_set` run the plain cold
-    start and the warm start for as long and compare when their spindown
-    luminosity (the mean over the last rotation period) settles within 2% of
-    the cold run's final value, and how far each start is from the cold
-    run's final fields."""
+def rotator_study(n_train=40, iters=2000, batch=2, train_periods=2.0, N=ROT_N,
+                  test_incl=(38.0, 68.0), r_lc=ROT_RLC_TEST, periods=3.0, seed=0,
+                  r_lc_train=ROT_RLC_TRAIN):
+    """The configured warm-start study.  Train on n_train N^3 runs pooled to
+    the network's grid, then for each test inclination run the N^3 rotator
+    (R_LC = r_lc) from its vacuum dipole (cold) and from the network's warm
+    start for `periods` rotation periods, record the FP64 Poynting
+    luminosity through the sphere r = 0.75 R_LC every 1/40 period, and
+    compare the wall time until it stays within 2% of the cold run's steady
+    value (the mean over its last period): inference (input features, the
+    network, the upsampling and the upload) included for the warm start,
+    step time measured with CUDA events without the diagnostics."""
     import time
-
-    def period_steps(p):
-        return int(round(2 * math.pi / (p.omega * float(np.float32(p.dt)))))
+    torch = _torch()
     t0 = time.time()
-    samples = []
-    for incl, om in train_set:
-        p = star_params(N, incl, om)
-        period = period_steps(p)
-        start = problems.pulsar_fields(p, np.float32)
-        steady, _ = star_run(p, start, int(round(periods * period)), lum_radius,
-                             max(1, period // 20))
-        samples.append((p, float(incl), start, steady))
+    xs, ts, ms, pairs = rotator_training_set(n_train, train_periods, N=N, r_lc_range=r_lc_train)
+    torch.cuda.synchronize()
     t_gen = time.time() - t0
     net = UNet(seed=seed)
     t1 = time.time()
-    losses = train(net, samples, iters)
-    _torch().cuda.synchronize()
+    losses = train_stream(net, xs, ts, ms, iters, batch=batch)
+    torch.cuda.synchronize()
     t_train = time.time() - t1
+    del xs, ts, ms
     results = []
-    for incl, om in test_set:
-        p = star_params(N, incl, om)
-        period = period_steps(p)
-        steps = int(round(periods * period))
-        every = max(1, period // 20)
+    for incl in test_incl:
+        p = rotator_params(N, incl, r_lc)
+        per = period_steps(p)
+        steps = int(round(periods * per))
+        every = max(1, int(per // 40))
+        lum_r = 0.75 * r_lc
         start = problems.pulsar_fields(p, np.float32)
-        cold, hist_c = star_run(p, start, steps, lum_radius, every)
+        step_ms = _step_ms(p, start)
+        cold, hist_c = star_run(p, start, steps, lum_r, every)
+        torch.cuda.synchronize()
         t2 = time.time()
-        warm0 = predict(net, p, start, incl)
+        warm0 = upsampled_warm_start(net, p, start, incl)
+        torch.cuda.synchronize()
         t_infer = time.time() - t2
-        _, hist_w = star_run(p, warm0, steps, lum_radius, every)
-        mean_c, mean_w = rotation_mean(hist_c, period), rotation_mean(hist_w, period)
-        l_ref = mean_c[-1][1]
+        _, hist_w = star_run(p, warm0, steps, lum_r, every)
+        nper = int(round(per / every))
+        l_ref = float(np.mean([l for _, l in hist_c[-nper:]]))
+        sc, sw = settle_step(hist_c, l_ref), settle_step(hist_w, l_ref)
+        wall_c = sc * step_ms / 1e3
+        wall_w = t_infer + sw * step_ms / 1e3
         g = p.guard[0]
         sl = (slice(g, -g),) * 3
-        _, mask = target_and_mask(p, start, cold)
 
         def err(f):
-            num = sum(float(((f[c] - cold[c])[sl] ** 2 * mask).sum()) for c in range(6))
-            den = sum(float((cold[c][sl] ** 2 * mask).sum()) for c in range(6))
+            num = sum(float(((f[c] - cold[c])[sl].astype(np.float64) ** 2).sum()) for c in range(6))
+            den = sum(float((cold[c][sl].astype(np.float64) ** 2).sum()) for c in range(6))
             return math.sqrt(num / den)
-        sc, sw = settle_step(mean_c, l_ref), settle_step(mean_w, l_ref)
-        # the instantaneous luminosity (steady for an aligned rotator; an
-        # oblique one's is modulated at the rotation period)
-        ic, iw = settle_step(hist_c, l_ref), settle_step(hist_w, l_ref)
-        results.append({"inclination": incl, "omega": om, "L_steady": l_ref,
-                        "period_steps": period, "steps": steps,
-                        "settle_step_cold": sc, "settle_step_warm": sw, "gain": sc / max(sw, 1),
-                        "settle_step_cold_instantaneous": ic,
-                        "settle_step_warm_instantaneous": iw,
-                        "gain_instantaneous": ic / max(iw, 1),
-                        "L_cold_history": [round(l, 6) for _, l in hist_c[:40]],
-                        "L_warm_history": [round(l, 6) for _, l in hist_w[:40]],
-                        "L_first_period_cold": mean_c[0][1], "L_first_period_warm": mean_w[0][1],
-                        "field_error_dipole": err(start), "field_error_warm": err(warm0),
-                        "seconds_inference": t_infer})
-    return {"N": N, "periods": periods, "train": [list(x) for x in train_set], "test": results,
-            "loss": losses, "seconds_generate": t_gen, "seconds_train": t_train}
+        results.append({
+            "inclination": incl, "R_LC": r_lc, "N": N, "L_steady": l_ref,
+            "period_steps": per, "steps": steps,
+            "settle_step_cold": sc, "settle_step_warm": sw,
+            "settle_periods_cold": sc / per, "settle_periods_warm": sw / per,
+            "step_ms": step_ms, "seconds_inference": t_infer,
+            "wall_to_settle_cold_s": wall_c, "wall_to_settle_warm_s": wall_w,
+            "gain": wall_c / max(wall_w, 1e-9),
+            "field_error_dipole": err(start), "field_error_warm": err(warm0),
+            "L_cold": [round(l, 5) for _, l in hist_c[::4]],
+            "L_warm": [round(l, 5) for _, l in hist_w[::4]]})
+    return {"train": {"n": n_train, "periods": train_periods, "grid": N,
+                      "network_grid": N // ROT_COARSE, "R_LC": list(r_lc_train),
+                      "iters": iters, "batch": batch, "loss": losses,
+                      "seconds_generate": t_gen, "seconds_train": t_train},
+            "test": results}
+
+
+def _step_ms(p, fields, steps=100):
+    """Device milliseconds per step of the flat solver on p (CUDA events)."""
+    from .solver import FieldSolverEZ, SimData, SimEnvironment
+    env = SimEnvironment(p)
+    data = SimData(env, np.float32)
+    data.upload(fields)
+    s = FieldSolverEZ(data, env, "gpu")
+    s.step(0.0, 5)
+    s.set_timing(True)
+    s.step(0.0, steps)
+    ms = s.last_timing()["total_ms"] / steps
+    s.close()
+    data.close()
+    env.close()
+    return ms

@@ -325,6 +325,19 @@ COFFEE_API int coffee_batch_step(coffee_batch* b, double* times, int nsteps);
 COFFEE_API int coffee_batch_info(coffee_batch* b, int* tile_x, int* tile_y, int* order,
                                  double* tuned_ms);
 COFFEE_API int coffee_batch_destroy(coffee_batch* b);
+/* The persistent mode (on != 0): every coffee_batch_step call runs all of
+ * its steps in one cooperative launch (all CTAs resident) that separates the
+ * phases by grid-wide barriers instead of launch boundaries; results are
+ * bitwise those of the default mode.  Each barrier wait is bounded (2 s by
+ * default): a wait that runs out ends the launch, and coffee_batch_step
+ * returns COFFEE_E_TIMEOUT with the barrier and CTA in the error string; the
+ * fields are then partly advanced.  In this mode coffee_batch_step
+ * synchronises its stream before it returns (it reads the barrier status). */
+COFFEE_API int coffee_batch_set_persistent(coffee_batch* b, int on);
+/* Limit of one barrier wait of the persistent mode, in ns (> 0).
+ * stall_block >= 0 is a test hook: that CTA leaves out its arrival at the
+ * first barrier, so the other CTAs' waits run out; -1 turns it off. */
+COFFEE_API int coffee_batch_set_wait_limit(coffee_batch* b, long long limit_ns, int stall_block);
 
 /* ---- one step loop that allocates nothing ------------------------------
  * No counterpart in the reference.  For callers that must not allocate

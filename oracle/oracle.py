@@ -161,7 +161,7 @@ def run_reference(p: SimParams, fields, nsteps: int, time0: float = 0.0, aux: bo
     dt = fields[0].dtype
     exe = ref_binary(dt)
     if not os.path.exists(exe):
-        raise RuntimeError(f"{exe} missing: run `make -C oracle ref`")
+        raise RuntimeError(f"{exe} missing: run `make -C oracle ref REF=<reference checkout>`")
     own = workdir is None
     wd = tempfile.mkdtemp(prefix="coffee_ref_") if own else workdir
     try:
@@ -204,7 +204,7 @@ def run_reference_gpu(solver: str, p: SimParams, fields, nsteps: int, time0: flo
     (fields, aux_or_None, info) like run_reference."""
     exe = refgpu_binary(fields[0].dtype)
     if not os.path.exists(exe):
-        raise RuntimeError(f"{exe} missing: run `make -C oracle gpuref`")
+        raise RuntimeError(f"{exe} missing: run `make -C oracle gpuref REF=<reference checkout>`")
     wd = tempfile.mkdtemp(prefix="coffee_refgpu_")
     try:
         cfg = os.path.join(wd, "config.toml")

@@ -205,3 +205,23 @@ def test_energy_diagnostics_bit_for_bit(name):
         _, _, info = oracle.run_reference(p, f32, 3, diag=True)
         for k in range(6):
             assert count_differing(extra[k][sl], info["diag"][k][sl]) == 0, (name, "ref dU", k)
+
+
+def test_fp64_with_the_float_builds_taper_lanes():
+    """FP64 with the float build's 16 taper lanes (coffee_solver_set_taper_lanes)
+    is the float build's algorithm without FP32 rounding: it matches the
+    restatement in FP64 with 16 lanes (the fixtures' out_f64_l16)."""
+    from coffee_b200.solver import FieldSolverEZ, SimData, SimEnvironment
+    p, d = load_golden("alfven16")
+    env = SimEnvironment(p)
+    data = SimData(env, np.float64)
+    data.upload([a.astype(np.float64) for a in d["in_f32"]])
+    s = FieldSolverEZ(data, env, "cpu")
+    s.set_taper_lanes(16)
+    s.step(float(d["time0"]), int(d["steps"]))
+    out = data.download()
+    s.close()
+    data.close()
+    env.close()
+    for f in range(7):
+        assert rel_l2(out[f], d["out_f64_l16"][f]) < 1e-12, f

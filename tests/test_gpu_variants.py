@@ -18,6 +18,7 @@ import numpy as np
 import pytest
 
 from coffee_b200 import problems
+from coffee_b200._lib import COFFEE_E_TIMEOUT, CoffeeError
 from coffee_b200.solver import FieldSolverEZCylindrical, FieldSolverEZSpherical, \
     FieldSolverGrEZ, SimData, SimEnvironment, SphBatch
 from helpers import fp32_parity, rel_l2
@@ -31,12 +32,12 @@ pytestmark = pytest.mark.gpu
 def _need_refgpu():
     for dt in (np.float32, np.float64):
         if not os.path.exists(oracle.refgpu_binary(dt)):
-            pytest.fail(f"{oracle.refgpu_binary(dt)} missing: build it with `make -C oracle gpuref`")
+            pytest.fail(f"{oracle.refgpu_binary(dt)} missing: build it with `make -C oracle gpuref REF=<reference checkout>`")
 
 
-def _run_ours(cls, p, fields32, nsteps, aux=False):
+def _run_ours(cls, p, fields32, nsteps, aux=False, dtype=np.float32):
     env = SimEnvironment(p)
-    data = SimData(env, np.float32)
+    data = SimData(env, dtype)
     data.upload(fields32)
     solver = cls(data, env)
     if aux:
@@ -168,34 +169,85 @@ def test_logsph_rejects_short_theta_guard():
         FieldSolverEZSpherical(data, env)
 
 
-def test_logsph_batch_equals_single_runs():
-    """One launch per phase over runs of different sizes, spins and layers
-    gives bitwise the results of stepping each run alone."""
+def _batch_runs(dtype, nsteps=7):
+    """Three log-spherical runs of different sizes, spins and layers: their
+    single-run results after nsteps steps, their initial fields, and a
+    (env, data, solver) of each for a batch."""
     cfgs = [dict(nr=64, nth=32, omega=0.2, pml=8), dict(nr=96, nth=48, omega=0.3, pml=0),
             dict(nr=48, nth=24, omega=0.1, pml=6)]
-    singles, runs = [], []
+    singles, inits, runs = [], [], []
     for k, cfg in enumerate(cfgs):
         p = problems.sph_pulsar_params(guard=4, **cfg)
         if k == 0:
             p.tp_start, p.tp_end, p.dw0, p.thp1, p.thp2 = 0.0, 0.5, 0.1, 0.6, 1.2
-        f = problems.sph_pulsar_fields(p, np.float32)
-        out, _ = _run_ours(FieldSolverEZSpherical, p, f, 7)
+        f = problems.sph_pulsar_fields(p, dtype)
+        out, _ = _run_ours(FieldSolverEZSpherical, p, f, nsteps, dtype=dtype)
         singles.append(out)
+        inits.append(f)
         env = SimEnvironment(p)
-        data = SimData(env, np.float32)
+        data = SimData(env, dtype)
         data.upload(f)
         runs.append((env, data, FieldSolverEZSpherical(data, env)))
-    batch = SphBatch([r[2] for r in runs])
-    info = batch.info()  # the autotuner's choice: any candidate gives the same fields
-    assert info["tile"] in ([32, 8], [64, 4], [128, 2], [16, 16]) and info["first_stage_ms"] > 0
-    batch.step(3)  # captures the step graph, replays it 3 times
-    batch.step(4)  # replays it from the new times
+    return singles, inits, runs
+
+
+def _check_batch(runs, singles):
     for k, (env, data, solver) in enumerate(runs):
         got = data.download()
         for f in range(7):
             assert np.array_equal(got[f], singles[k][f]), f"run {k} field {f} differs"
+
+
+def _close_runs(batch, runs):
     batch.close()
     for env, data, solver in runs:
         solver.close()
         data.close()
         env.close()
+
+
+def test_logsph_batch_equals_single_runs():
+    """One launch per phase over runs of different sizes, spins and layers
+    gives bitwise the results of stepping each run alone."""
+    singles, _, runs = _batch_runs(np.float32)
+    batch = SphBatch([r[2] for r in runs])
+    info = batch.info()  # the autotuner's choice: any candidate gives the same fields
+    assert info["tile"] in ([32, 8], [64, 4], [128, 2], [16, 16]) and info["first_stage_ms"] > 0
+    batch.step(3)  # captures the step graph, replays it 3 times
+    batch.step(4)  # replays it from the new times
+    _check_batch(runs, singles)
+    _close_runs(batch, runs)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_logsph_persistent_batch_equals_single_runs(dtype):
+    """The persistent mode (one cooperative launch per call, grid-wide
+    barriers between the phases) gives bitwise the single runs' results."""
+    singles, _, runs = _batch_runs(dtype)
+    batch = SphBatch([r[2] for r in runs])
+    batch.set_persistent(True)
+    batch.step(3)
+    batch.step(4)
+    _check_batch(runs, singles)
+    _close_runs(batch, runs)
+
+
+def test_logsph_persistent_batch_wait_limit():
+    """A barrier wait that runs out ends the persistent launch with
+    COFFEE_E_TIMEOUT (one CTA leaves out its first arrival, so the others
+    wait for it until the 1 ms limit); the context stays usable and the next
+    calls, from the initial fields again, give the single runs' results."""
+    singles, inits, runs = _batch_runs(np.float32)
+    batch = SphBatch([r[2] for r in runs])
+    batch.set_persistent(True)
+    batch.set_wait_limit(1_000_000, stall_block=0)
+    with pytest.raises(CoffeeError) as err:
+        batch.step(2)
+    assert err.value.code == COFFEE_E_TIMEOUT and "grid barrier 0" in str(err.value)
+    batch.set_wait_limit(2_000_000_000, stall_block=-1)
+    for (env, data, solver), f in zip(runs, inits):
+        data.upload(f)
+    batch.times[:] = 0.0
+    batch.step(7)
+    _check_batch(runs, singles)
+    _close_runs(batch, runs)

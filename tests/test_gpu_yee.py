@@ -33,7 +33,7 @@ pytestmark = pytest.mark.gpu
 def _need_refgpu():
     for dt in (np.float32, np.float64):
         if not os.path.exists(oracle.refgpu_binary(dt)):
-            pytest.fail(f"{oracle.refgpu_binary(dt)} missing: build it with `make -C oracle gpuref`")
+            pytest.fail(f"{oracle.refgpu_binary(dt)} missing: build it with `make -C oracle gpuref REF=<reference checkout>`")
 
 
 def _run_ours(p, fields32, nsteps, b0=None, time0=0.0):
