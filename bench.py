@@ -870,6 +870,29 @@ def run_surrogate(args):
     except Exception:
         peak, kind = 1590.0, "fallback"
     achieved = flops / (conv_ms / 1e3) / 1e12
+
+    # the weight gradient of the same two layers, tcgen05 against mma.sync
+    def wgrad_time(fn, L, xin):
+        dyb = torch.zeros(xin.shape[:4] + (L.cout,), dtype=torch.bfloat16, device=dev)
+        dyb.normal_()
+        wsb = torch.empty(sg.workspace_bytes(L.cout, L.cin), dtype=torch.uint8, device=dev)
+        dw = torch.empty((L.cout, 27, L.cin), dtype=torch.float32, device=dev)
+        for _ in range(3):
+            fn(dyb, xin, dw, wsb)
+        e0.record(stream)
+        for _ in range(10):
+            fn(dyb, xin, dw, wsb)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        t = e0.elapsed_time(e1) / 10
+        return {"ms": t, "tflops": 2.0 * 27 * L.cin * L.cout * xin[..., 0].numel() / (t / 1e3) / 1e12}
+
+    wgrad = {}
+    for name, L, xin in (("32_32", net.layers[3], net._saved["a3"]),
+                         ("48_16", net.layers[4], net._saved["cat"])):
+        wgrad[name] = {"tcgen05": wgrad_time(sg.conv_backward_weight_tc, L, xin),
+                       "mma_sync": wgrad_time(sg.conv_backward_weight, L, xin)}
+    sg.check_tc()
     line = {"metric": "training voxels/s", "value": vox / (ms / 1e3), "unit": "voxels/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
@@ -883,6 +906,7 @@ def run_surrogate(args):
                          "peak_kind": kind, "frac": achieved / peak, "traffic": None,
                          "avg_launch_ms": conv_ms, "flops_per_launch": flops},
             "conv_48_16_mma_sync": {"ms": mma_ms, "tflops": mma_flops / (mma_ms / 1e3) / 1e12},
+            "weight_gradient": wgrad,
             "gpu_launches": None, "clocks": clk}
     if args.study:
         # the configured oblique rotator: 384^3, R* = 12 and R_LC = 60 cells,

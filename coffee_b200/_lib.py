@@ -132,6 +132,7 @@ SIGNATURES = {
     "coffee_conv3d_backward_data": (_i, [_vp, _i, _i, _i, _i, _i, _vp, _i, _vp, _vp]),
     "coffee_conv3d_backward_weight_workspace": (ctypes.c_size_t, [_i, _i]),
     "coffee_conv3d_backward_weight": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp]),
+    "coffee_conv3d_backward_weight_tc": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp]),
     "coffee_bias_grad": (_i, [_vp, ctypes.c_longlong, _i, _vp, _vp]),
     "coffee_leaky_backward": (_i, [_vp, _vp, ctypes.c_longlong, ctypes.c_float, _vp, _vp, _vp]),
     "coffee_pool2_forward": (_i, [_vp, _i, _i, _i, _i, _i, _vp, _vp]),

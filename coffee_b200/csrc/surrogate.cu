@@ -268,19 +268,38 @@ void launch_wgrad(const bf16* dy, const bf16* x, Grid4 g, int K, float* part, cu
 
 // ------------------------------------------------------------ elementwise
 
-__global__ void bias_grad_kernel(const float* __restrict__ dz, long long npts, int K,
-                                 float* __restrict__ db) {
-  const int k = blockIdx.x;
-  float s = 0.f;
-  for (long long p = threadIdx.x; p < npts; p += blockDim.x) s += dz[p * K + k];
+// db[k] = sum over points of dz[p][k], in two deterministic passes: block b
+// of bias_grad_part_kernel sums points [b * per, (b + 1) * per) with
+// coalesced reads (blockDim = K * R threads: thread t always adds channel
+// t % K, rows t / K, t / K + R, ...), reduces its R rows per channel in a
+// fixed order and writes g_bias_part[b][k]; bias_grad_sum_kernel adds the
+// blocks in order.
+constexpr int kBiasBlocks = 296;
+constexpr int kBiasMaxK = 64;
+__device__ float g_bias_part[kBiasBlocks * kBiasMaxK];
+
+__global__ void bias_grad_part_kernel(const float* __restrict__ dz, long long npts, int K,
+                                      long long per) {
   __shared__ float red[256];
-  red[threadIdx.x] = s;
+  const int t = threadIdx.x, R = blockDim.x / K, k = t % K, r = t / K;
+  const long long p0 = blockIdx.x * per, p1 = min(npts, p0 + per);
+  float s = 0.f;
+  for (long long p = p0 + r; p < p1; p += R) s += dz[p * K + k];
+  red[t] = s;
   __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-    __syncthreads();
+  if (r == 0) {
+    float a = 0.f;
+    for (int q = 0; q < R; ++q) a += red[q * K + k];
+    g_bias_part[blockIdx.x * kBiasMaxK + k] = a;
   }
-  if (threadIdx.x == 0) db[k] = red[0];
+}
+
+__global__ void bias_grad_sum_kernel(int K, int blocks, float* __restrict__ db) {
+  const int k = threadIdx.x;
+  if (k >= K) return;
+  float s = 0.f;
+  for (int b = 0; b < blocks; ++b) s += g_bias_part[b * kBiasMaxK + k];
+  db[k] = s;
 }
 
 __global__ void leaky_bwd_kernel(const float* __restrict__ da, const float* __restrict__ z,
@@ -911,6 +930,328 @@ int launch_fwd_tc(const bf16* x, Grid4 g, int C, const bf16* w, const float* bia
   return COFFEE_OK;
 }
 
+
+// ------------------------------------- weight gradient on tcgen05 (sm_100a)
+// dW[k][tap][c] = sum over points p of dy[p][k] x[p + tap][c], as a GEMM
+// whose reduction runs over points: D (M 128 x N K) += A (M x 16 points) B
+// (16 points x N), with M = TPM taps x CBW channels (TPM = 128 / CBW; CBW
+// = 16, 32 or 64 channels, a box of 48 channels zero-filled to 64) and N = K
+// output channels.  Both operands are stored point-major, so both are
+// MN-major: a 128-point box of x shifted by a tap, loaded by TMA with the
+// swizzle of its 2 CBW-byte rows, is one MN atom column of A (TPM such
+// boxes side by side, LBO apart, one per tap of the CTA's tap group); the
+// unshifted dy box is B.  A CTA owns one tap group and a range of boxes:
+// it accumulates in tensor memory over all of them (the TMA unit's zero
+// fill outside the grid is the convolution's padding, and zero dy rows
+// cover ragged boxes), then writes its 128 x N partial sums; a second kernel
+// adds the partials of the point ranges in a fixed order (deterministic).
+// Roles, ring, bounded waits and the drain on a timeout are those of
+// conv3d_fwd_tc_kernel.
+constexpr int kWgTcStages = 4;
+
+template <int CBW, int KN>
+__global__ void __launch_bounds__(kTcThreads) conv3d_wgrad_tc_kernel(
+    const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap dymap,
+    TcBox box, int ngroups, long long nboxes, long long per_chunk, float* __restrict__ part,
+    const TcWaitParams wp) {
+  static_assert(CBW == 16 || CBW == 32 || CBW == 64, "x boxes of 16, 32 or 64 channels");
+  static_assert(KN == 16 || KN == 32 || KN == 64, "16, 32 or 64 output channels");
+  constexpr int TPM = 128 / CBW;                        // taps per M tile
+  constexpr uint32_t kAbytes = 128u * 128u * 2u;        // TPM boxes of 128 points x CBW
+  constexpr uint32_t kTapBox = 128u * CBW * 2u;         // one x box
+  constexpr uint32_t kBbytes = 128u * KN * 2u;          // the dy box
+  constexpr uint32_t kSlot = kAbytes + kBbytes;         // multiple of 1024
+  constexpr uint32_t kLayoutA = CBW == 16 ? 6u : (CBW == 32 ? 4u : 2u);
+  constexpr uint32_t kLayoutB = KN == 16 ? 6u : (KN == 32 ? 4u : 2u);
+  constexpr int NCOLS = KN <= 32 ? 32 : 64;
+  // kind::f16, FP32 accumulator, BF16 operands, A and B MN-major (bits 15, 16)
+  constexpr uint32_t kIdesc = tc_idesc(kTcM, KN) | (1u << 15) | (1u << 16);
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  __shared__ __align__(8) unsigned long long full_s[kWgTcStages], empty_s[kWgTcStages];
+  __shared__ __align__(8) unsigned long long ready_s;
+  __shared__ uint32_t tmem_s;
+  __shared__ int abort_s;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tg = (int)(blockIdx.x % (unsigned)ngroups);
+  const long long chunk = blockIdx.x / (unsigned)ngroups;
+  const long long b0 = chunk * per_chunk;
+  const long long b1 = min(nboxes, b0 + per_chunk);
+  const uint32_t base = (smem_addr(tc_smem) + 1023u) & ~1023u;
+  const uint32_t full0 = smem_addr(full_s), empty0 = smem_addr(empty_s);
+  const uint32_t ready0 = smem_addr(&ready_s);
+  volatile int* abort = &abort_s;
+
+  if (tid == 0) {
+    abort_s = 0;
+    for (int b = 0; b < kWgTcStages; ++b) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full0 + 8 * b) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(empty0 + 8 * b) : "memory");
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(ready0) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(&tmem_s)),
+                 "r"(NCOLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_s;
+
+  const long long per_n = (long long)box.tx * box.ty * box.tz;
+  auto box_origin = [&](long long t, int& n, int& x0, int& y0, int& z0) {
+    n = (int)(t / per_n);
+    long long r = t - (long long)n * per_n;
+    z0 = (int)(r / ((long long)box.tx * box.ty)) * box.bz;
+    r %= (long long)box.tx * box.ty;
+    y0 = (int)(r / box.tx) * box.by;
+    x0 = (int)(r % box.tx) * box.bx;
+  };
+  const uint32_t nsteps = (uint32_t)max(0LL, b1 - b0);
+
+  if (warp == 4) {
+    // ---- producer: per box, TPM shifted x boxes and the dy box into a slot
+    if (lane == 0) {
+      uint32_t step = 0;
+      const uint64_t xm = reinterpret_cast<uint64_t>(&xmap);
+      const uint64_t dm = reinterpret_cast<uint64_t>(&dymap);
+      for (; step < nsteps && !wp.stall_producer; ++step) {
+        const uint32_t b = step % kWgTcStages;
+        if (step >= kWgTcStages &&
+            !tc_wait(empty0 + 8 * b, ((step / kWgTcStages) - 1) & 1, abort, wp))
+          break;
+        int n, x0, y0, z0;
+        box_origin(b0 + step, n, x0, y0, z0);
+        const uint32_t slot = base + b * kSlot;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full0 + 8 * b),
+                     "r"(kSlot)
+                     : "memory");
+#pragma unroll 1
+        for (int j = 0; j < TPM; ++j) {
+          // taps past the last of the group's (the last group is short) load
+          // tap 26 again: their rows of the result are not read
+          const int tap = min(tg * TPM + j, 26);
+          const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+          asm volatile(
+              "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+              "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(slot + (uint32_t)j * kTapBox),
+              "l"(xm), "r"(0), "r"(x0 + dx), "r"(y0 + dy), "r"(z0 + dz), "r"(n), "r"(full0 + 8 * b)
+              : "memory");
+        }
+        asm volatile(
+            "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+            "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(slot + kAbytes),
+            "l"(dm), "r"(0), "r"(x0), "r"(y0), "r"(z0), "r"(n), "r"(full0 + 8 * b)
+            : "memory");
+      }
+      if (*abort) {
+        // the loads of the last kWgTcStages steps may be in flight
+        const uint32_t first = step > kWgTcStages ? step - kWgTcStages : 0;
+        for (uint32_t s2 = first; s2 < step; ++s2)
+          tc_drain_wait(full0 + 8 * (s2 % kWgTcStages), (s2 / kWgTcStages) & 1);
+      }
+    }
+  } else if (warp == 5) {
+    // ---- MMA issuer: 8 MMAs of 16 points per box into one accumulator
+    if (lane == 0) {
+      uint32_t step = 0;
+      bool ok = true;
+      for (; step < nsteps; ++step) {
+        const uint32_t b = step % kWgTcStages;
+        if (!tc_wait(full0 + 8 * b, (step / kWgTcStages) & 1, abort, wp)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t slot = base + b * kSlot;
+#pragma unroll
+        for (int ks = 0; ks < 8; ++ks) {
+          // 16 points: two 8-row groups (SBO apart) of every atom
+          const uint64_t ad = tc_sdesc(slot + (uint32_t)ks * 32u * CBW, kTapBox, 16u * CBW, kLayoutA);
+          const uint64_t bd =
+              tc_sdesc(slot + kAbytes + (uint32_t)ks * 32u * KN, kBbytes, 16u * KN, kLayoutB);
+          asm volatile(
+              "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+              "l"(ad), "l"(bd), "r"(kIdesc), "r"((step > 0 || ks > 0) ? 1 : 0)
+              : "memory");
+        }
+        asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                empty0 + 8 * b)
+            : "memory");
+      }
+      if (ok && nsteps > 0) {
+        asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                ready0)
+            : "memory");
+      } else if (!ok && step > 0) {
+        const uint32_t last = step - 1;
+        tc_drain_wait(empty0 + 8 * (last % kWgTcStages), (last / kWgTcStages) & 1);
+      }
+    }
+  } else {
+    // ---- epilogue: warp w reads accumulator rows 32 w .. 32 w + 31
+    const int m = tid;  // row of D: tap tg * TPM + m / CBW, channel m % CBW
+    float* out = part + ((long long)blockIdx.x * 128 + m) * KN;
+    if (nsteps > 0 && tc_wait(ready0, 0, abort, wp)) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      uint32_t r[KN];
+#pragma unroll
+      for (int c16 = 0; c16 < KN / 16; ++c16) {
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c16 * 16);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
+            "%10, %11, %12, %13, %14, %15}, [%16];\n"
+            : "=r"(r[c16 * 16 + 0]), "=r"(r[c16 * 16 + 1]), "=r"(r[c16 * 16 + 2]),
+              "=r"(r[c16 * 16 + 3]), "=r"(r[c16 * 16 + 4]), "=r"(r[c16 * 16 + 5]),
+              "=r"(r[c16 * 16 + 6]), "=r"(r[c16 * 16 + 7]), "=r"(r[c16 * 16 + 8]),
+              "=r"(r[c16 * 16 + 9]), "=r"(r[c16 * 16 + 10]), "=r"(r[c16 * 16 + 11]),
+              "=r"(r[c16 * 16 + 12]), "=r"(r[c16 * 16 + 13]), "=r"(r[c16 * 16 + 14]),
+              "=r"(r[c16 * 16 + 15])
+            : "r"(taddr)
+            : "memory");
+      }
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int n4 = 0; n4 < KN; n4 += 4)
+        *reinterpret_cast<float4*>(out + n4) =
+            make_float4(__uint_as_float(r[n4]), __uint_as_float(r[n4 + 1]),
+                        __uint_as_float(r[n4 + 2]), __uint_as_float(r[n4 + 3]));
+    } else {
+#pragma unroll
+      for (int n4 = 0; n4 < KN; n4 += 4)
+        *reinterpret_cast<float4*>(out + n4) = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOLS)
+                 : "memory");
+  }
+}
+
+// dw[k][tap][c] = the sum over the chunks, in chunk order, of the partial
+// sums of conv3d_wgrad_tc_kernel (CTA chunk * ngroups + tap / TPM, row
+// (tap % TPM) * CBW + c, column k).
+__global__ void wgrad_tc_reduce_kernel(const float* __restrict__ part, int K, int C, int CBW,
+                                       int ngroups, int nchunks, float* __restrict__ dw) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n = (long long)K * 27 * C;
+  if (i >= n) return;
+  const int k = (int)(i / (27 * C)), r = (int)(i % (27 * C)), tap = r / C, c = r % C;
+  const int tpm = 128 / CBW, tg = tap / tpm, m = (tap % tpm) * CBW + c;
+  float s = 0.f;
+  for (int q = 0; q < nchunks; ++q) s += part[(((long long)q * ngroups + tg) * 128 + m) * K + k];
+  dw[i] = s;
+}
+
+// Most SMs the chunk count is sized for (the workspace bound).
+constexpr int kWgTcMaxSms = 192;
+
+// channels of one x box of the tcgen05 weight gradient (0: not supported)
+int wgrad_tc_cbw(int C) { return C == 16 ? 16 : (C == 32 ? 32 : ((C == 48 || C == 64) ? 64 : 0)); }
+
+size_t wgrad_tc_workspace(int K, int C) {
+  const int cbw = wgrad_tc_cbw(C);
+  if (!cbw) return 0;
+  const int groups = (27 + 128 / cbw - 1) / (128 / cbw);
+  const long long chunks = std::max(1, kWgTcMaxSms / groups);
+  return (size_t)chunks * groups * 128 * (size_t)K * sizeof(float);
+}
+
+template <int CBW, int KN>
+int launch_wgrad_tc(const bf16* dy, const bf16* x, Grid4 g, int C, float* dw, float* part,
+                    cudaStream_t st) {
+  if (int rc = tc_fault_word()) return rc;
+  if (*g_tc_fault_host)
+    return fail(COFFEE_E_TIMEOUT,
+                "an earlier tcgen05 convolution ran out of time waiting on its pipeline "
+                "(its results are invalid); clear the fault with coffee_conv3d_tc_fault");
+  constexpr int TPM = 128 / CBW;
+  const int groups = (27 + TPM - 1) / TPM;
+  TcBox box;
+  box.bx = std::min(128, std::max(8, pow2_at_least(g.w)));
+  box.by = std::min(128 / box.bx, pow2_at_least(g.h));
+  box.bz = 128 / (box.bx * box.by);
+  box.tx = (g.w + box.bx - 1) / box.bx;
+  box.ty = (g.h + box.by - 1) / box.by;
+  box.tz = (g.d + box.bz - 1) / box.bz;
+  if (box.bz > 256) return fail(COFFEE_E_INVALID, "tcgen05 weight gradient: box too deep");
+  const long long nboxes = (long long)g.n * box.tx * box.ty * box.tz;
+  int dev = 0, sms = 0;
+  COFFEE_CUDA_TRY(cudaGetDevice(&dev));
+  COFFEE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  sms = std::min(sms, kWgTcMaxSms);
+  // one CTA per SM (its ring takes most of the shared memory) over all tap
+  // groups, in one wave; every chunk non-empty
+  long long chunks = std::max(1LL, std::min(nboxes, (long long)(sms / groups)));
+  const long long per_chunk = (nboxes + chunks - 1) / chunks;
+  chunks = (nboxes + per_chunk - 1) / per_chunk;
+  EncodeTiledFn enc;
+  if (int rc = encode_fn(&enc)) return rc;
+  auto make = [&](CUtensorMap* map, const bf16* base, int ch, int boxc,
+                  CUtensorMapSwizzle sw) -> int {
+    const cuuint64_t dims[5] = {(cuuint64_t)ch, (cuuint64_t)g.w, (cuuint64_t)g.h,
+                                (cuuint64_t)g.d, (cuuint64_t)g.n};
+    const cuuint64_t strides[4] = {(cuuint64_t)ch * 2, (cuuint64_t)ch * 2 * g.w,
+                                   (cuuint64_t)ch * 2 * g.w * g.h,
+                                   (cuuint64_t)ch * 2 * g.w * g.h * g.d};
+    const cuuint32_t boxdim[5] = {(cuuint32_t)boxc, (cuuint32_t)box.bx, (cuuint32_t)box.by,
+                                  (cuuint32_t)box.bz, 1};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    const CUresult cr = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<bf16*>(base),
+                            dims, strides, boxdim, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS)
+      return fail(COFFEE_E_INVALID, "tcgen05 weight gradient: tensor map rejected (%d)", (int)cr);
+    return COFFEE_OK;
+  };
+  auto swz = [](int bytes) {
+    return bytes == 32 ? CU_TENSOR_MAP_SWIZZLE_32B
+                       : (bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B);
+  };
+  CUtensorMap xmap, dymap;
+  if (int rc = make(&xmap, x, C, CBW, swz(2 * CBW))) return rc;
+  if (int rc = make(&dymap, dy, KN, KN, swz(2 * KN))) return rc;
+  // the ring, plus 32 KB of slack past it: the operands' last 8-row groups
+  // stay inside the allocation even if the descriptors' strides were read
+  // the other way round
+  const size_t smem = 1024 + (size_t)kWgTcStages * (128u * 128u * 2u + 128u * KN * 2u) + 32768;
+  auto kern = conv3d_wgrad_tc_kernel<CBW, KN>;
+  COFFEE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  COFFEE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared));
+  const TcWaitParams wp{g_tc_cycles, g_tc_stall, g_tc_fault_dev};
+  const long long blocks = chunks * groups;
+  kern<<<(unsigned)blocks, kTcThreads, smem, st>>>(xmap, dymap, box, groups, nboxes, per_chunk,
+                                                   part, wp);
+  COFFEE_CUDA_TRY(cudaGetLastError());
+  const long long nw = (long long)KN * 27 * C;
+  wgrad_tc_reduce_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>(part, KN, C, CBW, groups,
+                                                                        (int)chunks, dw);
+  COFFEE_CUDA_TRY(cudaGetLastError());
+  return COFFEE_OK;
+}
+
+template <int KN>
+int wgrad_tc_dispatch_c(const bf16* dy, const bf16* x, Grid4 g, int C, float* dw, float* part,
+                        cudaStream_t st) {
+  switch (wgrad_tc_cbw(C)) {
+    case 16: return launch_wgrad_tc<16, KN>(dy, x, g, C, dw, part, st);
+    case 32: return launch_wgrad_tc<32, KN>(dy, x, g, C, dw, part, st);
+    case 64: return launch_wgrad_tc<64, KN>(dy, x, g, C, dw, part, st);
+    default: return fail(COFFEE_E_INVALID, "tcgen05 weight gradient: input channels 16, 32, 48 or 64 (%d)", C);
+  }
+}
 }  // namespace
 }  // namespace coffee
 
@@ -998,7 +1339,8 @@ extern "C" int coffee_conv3d_backward_data(const void* dy, int n, int d, int h, 
 }
 
 extern "C" size_t coffee_conv3d_backward_weight_workspace(int k, int c) {
-  return (size_t)kWgradChunks * (size_t)k * 27 * (size_t)c * sizeof(float);
+  return std::max((size_t)kWgradChunks * (size_t)k * 27 * (size_t)c * sizeof(float),
+                  wgrad_tc_workspace(k, c));
 }
 
 extern "C" int coffee_conv3d_backward_weight(const void* dy, const void* x, int n, int d, int h,
@@ -1033,10 +1375,43 @@ extern "C" int coffee_conv3d_backward_weight(const void* dy, const void* x, int 
   return COFFEE_OK;
 }
 
+extern "C" int coffee_conv3d_backward_weight_tc(const void* dy, const void* x, int n, int d,
+                                                int h, int w, int k, int c, float* dw,
+                                                void* workspace, void* stream) {
+  clear_error();
+  if (!dy || !x || !dw || !workspace)
+    return fail(COFFEE_E_INVALID, "coffee_conv3d_backward_weight_tc: null argument");
+  if (int rc = check_grid(n, d, h, w)) return rc;
+  if (reinterpret_cast<uintptr_t>(dy) % 16 || reinterpret_cast<uintptr_t>(x) % 16 ||
+      reinterpret_cast<uintptr_t>(workspace) % 16)
+    return fail(COFFEE_E_INVALID,
+                "coffee_conv3d_backward_weight_tc: dy, x and workspace must be 16-byte aligned");
+  if (!wgrad_tc_cbw(c))
+    return fail(COFFEE_E_INVALID, "tcgen05 weight gradient: input channels 16, 32, 48 or 64 (%d)", c);
+  const Grid4 g{n, d, h, w};
+  const bf16* dyb = static_cast<const bf16*>(dy);
+  const bf16* xb = static_cast<const bf16*>(x);
+  float* part = static_cast<float*>(workspace);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  switch (k) {
+    case 16: return wgrad_tc_dispatch_c<16>(dyb, xb, g, c, dw, part, st);
+    case 32: return wgrad_tc_dispatch_c<32>(dyb, xb, g, c, dw, part, st);
+    case 64: return wgrad_tc_dispatch_c<64>(dyb, xb, g, c, dw, part, st);
+    default: return fail(COFFEE_E_INVALID, "tcgen05 weight gradient: output channels 16, 32 or 64 (%d)", k);
+  }
+}
+
 extern "C" int coffee_bias_grad(const float* dz, long long npts, int k, float* db, void* stream) {
   clear_error();
   if (!dz || !db || npts <= 0 || k <= 0) return fail(COFFEE_E_INVALID, "coffee_bias_grad: bad argument");
-  bias_grad_kernel<<<(unsigned)k, 256, 0, static_cast<cudaStream_t>(stream)>>>(dz, npts, k, db);
+  if (k > kBiasMaxK) return fail(COFFEE_E_INVALID, "coffee_bias_grad: at most %d channels", kBiasMaxK);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const long long per = (npts + kBiasBlocks - 1) / kBiasBlocks;
+  const int blocks = (int)((npts + per - 1) / per);
+  const int threads = k * std::max(1, 256 / k);
+  bias_grad_part_kernel<<<(unsigned)blocks, (unsigned)threads, 0, st>>>(dz, npts, k, per);
+  COFFEE_CUDA_TRY(cudaGetLastError());
+  bias_grad_sum_kernel<<<1, kBiasMaxK, 0, st>>>(k, blocks, db);
   COFFEE_CUDA_TRY(cudaGetLastError());
   return COFFEE_OK;
 }

@@ -80,6 +80,13 @@ def use_tc(c, k):
     return c in (16, 32, 64) and k in (16, 32, 48, 64)
 
 
+def use_tc_wgrad(c, k):
+    """True where the weight gradient runs on the tcgen05 kernel: inputs of
+    16, 32, 48 or 64 channels and 16, 32 or 64 outputs (the results agree
+    with the mma.sync kernel's to FP32 rounding)."""
+    return c in (16, 32, 48, 64) and k in (16, 32, 64)
+
+
 def tc_fault(clear=True):
     """True if a wait of the tcgen05 convolution ran out of time (results invalid)."""
     flag = ctypes.c_int(0)
@@ -109,6 +116,15 @@ def conv_backward_weight(dy, x, dw, workspace):
     c = x.shape[-1]
     check(_lib.load().coffee_conv3d_backward_weight(_ptr(dy), _ptr(x), n, d, h, w, k, c,
                                                     _ptr(dw), _ptr(workspace), _stream()))
+    return dw
+
+
+def conv_backward_weight_tc(dy, x, dw, workspace):
+    """The weight gradient on the tcgen05 kernel (C in 16, 32, 48, 64)."""
+    n, d, h, w, k = dy.shape
+    c = x.shape[-1]
+    check(_lib.load().coffee_conv3d_backward_weight_tc(_ptr(dy), _ptr(x), n, d, h, w, k, c,
+                                                       _ptr(dw), _ptr(workspace), _stream()))
     return dw
 
 
@@ -216,7 +232,8 @@ class UNet:
         need = workspace_bytes(L.cout, L.cin)
         if self._ws is None or self._ws.numel() < need:
             self._ws = torch.empty(need, dtype=torch.uint8, device=self.dev)
-        conv_backward_weight(dzb, x_in, L.gw, self._ws)
+        wgrad = conv_backward_weight_tc if use_tc_wgrad(L.cin, L.cout) else conv_backward_weight
+        wgrad(dzb, x_in, L.gw, self._ws)
 
     def backward(self, dout):
         """Gradients of every layer for dL/dout (FP32, the output's shape)."""

@@ -71,7 +71,22 @@ COFFEE_API size_t coffee_conv3d_backward_weight_workspace(int k, int c);
 COFFEE_API int coffee_conv3d_backward_weight(const void* dy, const void* x, int n, int d, int h,
                                              int w, int k, int c, float* dw, void* workspace,
                                              void* stream);
-/* db[k] = sum over points of dz[., k] (FP32). */
+/* The same weight gradient on the fifth-generation tensor cores (sm_100a):
+ * a GEMM over points with both operands MN-major in shared memory (the layer
+ * input shifted by each tap and dy, loaded by TMA, zeros outside the grid),
+ * FP32 accumulation in tensor memory, per-chunk partial sums added in a
+ * fixed order (deterministic; the summation order differs from
+ * coffee_conv3d_backward_weight's, so the two agree to FP32 rounding).
+ * C in {16, 32, 48, 64}, K in {16, 32, 64}; dy, x and workspace 16-byte
+ * aligned; workspace as above.  Bounded waits as coffee_conv3d_forward_tc
+ * (the same fault word and COFFEE_E_TIMEOUT). */
+COFFEE_API int coffee_conv3d_backward_weight_tc(const void* dy, const void* x, int n, int d,
+                                                int h, int w, int k, int c, float* dw,
+                                                void* workspace, void* stream);
+/* db[k] = sum over points of dz[., k] (FP32), k <= 64: per-range partial
+ * sums in a library-owned device buffer, added in a fixed order
+ * (deterministic); calls that could overlap on the GPU (other streams, other
+ * host threads) must not share a device. */
 COFFEE_API int coffee_bias_grad(const float* dz, long long npts, int k, float* db, void* stream);
 /* dz = da * leaky'(z) (FP32 and a BF16 copy). */
 COFFEE_API int coffee_leaky_backward(const float* da, const float* z, long long count, float slope,

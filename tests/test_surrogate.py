@@ -157,6 +157,59 @@ def test_tcgen05_forward_matches_oracle_and_mma_sync(c, k, shape):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("c,k,shape", [(16, 16, (2, 6, 5, 7)), (16, 32, (1, 9, 4, 5)),
+                                       (48, 16, (2, 6, 5, 7)), (32, 32, (1, 4, 4, 9)),
+                                       (64, 64, (1, 5, 6, 7)), (32, 16, (2, 24, 40, 40))])
+def test_tcgen05_weight_gradient_matches_oracle_and_mma_sync(c, k, shape):
+    """The tcgen05 weight gradient (both operands MN-major, the reduction
+    over points) against the FP64 restatement on the same BF16 operands and
+    against the mma.sync kernel: every tap group of 16-, 32- and 64-channel
+    boxes (48 channels zero-filled to 64), ragged boxes, and a grid with
+    many boxes per CTA."""
+    from coffee_b200 import surrogate as sg
+    torch = _torch()
+    rng = np.random.default_rng(11 * c + k)
+    x = co.bf16(rng.standard_normal(shape + (c,)))
+    dy = co.bf16(rng.standard_normal(shape + (k,)))
+    xt, dyt = _bf16_tensor(x), _bf16_tensor(dy)
+    ws = torch.empty(sg.workspace_bytes(k, c), dtype=torch.uint8, device="cuda")
+    sg.tc_fault(clear=True)
+    dw = torch.full((k, 27, c), float("nan"), dtype=torch.float32, device="cuda")
+    sg.conv_backward_weight_tc(dyt, xt, dw, ws)
+    dw_ref = torch.empty_like(dw)
+    sg.conv_backward_weight(dyt, xt, dw_ref, ws)
+    torch.cuda.synchronize()
+    assert not sg.tc_fault()
+    got = _np(dw)
+    assert np.isfinite(got).all()
+    assert _rel(got, _np(dw_ref)) < 1e-5
+    if np.prod(shape) <= 1000:
+        assert _rel(got, co.conv3d_grad_weight(dy, x)) < 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k,npts", [(16, 100003), (48, 77), (64, 2 * 64 ** 3)])
+def test_bias_gradient_matches_numpy(k, npts):
+    """The bias gradient's two passes (block partial sums, then their sum in
+    block order) against an FP64 sum; bitwise the same on a second call."""
+    from coffee_b200 import _lib
+    from coffee_b200._lib import check
+    from coffee_b200.surrogate import _ptr, _stream
+    torch = _torch()
+    rng = np.random.default_rng(k)
+    dz = rng.standard_normal((npts, k)).astype(np.float32)
+    dzt = torch.from_numpy(dz).cuda()
+    db = torch.empty(k, dtype=torch.float32, device="cuda")
+    lib = _lib.load()
+    check(lib.coffee_bias_grad(_ptr(dzt), npts, k, _ptr(db), _stream()))
+    first = db.cpu().numpy().copy()
+    check(lib.coffee_bias_grad(_ptr(dzt), npts, k, _ptr(db), _stream()))
+    assert np.array_equal(db.cpu().numpy(), first)
+    ref = dz.astype(np.float64).sum(axis=0)
+    assert np.abs(first - ref).max() <= 1e-5 * np.abs(dz).sum(axis=0).max()
+
+
+@pytest.mark.gpu
 def test_tcgen05_wait_that_runs_out_is_reported_and_recovers():
     """A pipeline wait of the tcgen05 convolution that runs out.  The test
     hook makes the producer issue no loads and bounds the waits at 20,000
