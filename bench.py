@@ -562,12 +562,15 @@ def run_ours(args):
 # GPU build, which --impl reference times on the same case.
 
 # Algorithmic bytes per cell of the timed kernel: the LSRK stage kernels of
-# the EZ solvers; for the staggered solver the update pass of substeps 2-3,
+# the EZ solvers (GR: read D, B, P, dU, E and H, write D', B', P', dU' and
+# the E', H' of the output, 20 + 20 arrays of 4 bytes; the sqrt(gamma)
+# table, 4 more, is not counted); for the staggered solver the update pass
+# of substeps 2-3,
 # which reads E, B and their start-of-step copies and writes E*, B'
 # (12 + 6 arrays of 4 bytes).
 # The Kerr-Schild staggered solver's update pass reads E, H, B, the lowered
 # B, rho, D and the start-of-step copies and writes D*, B' (22 + 6 arrays).
-VARIANT_STAGE_BYTES = {"gr-wald": 136, "logsph-batch": 112, "logsph": 112, "cyl-pulsar": 112,
+VARIANT_STAGE_BYTES = {"gr-wald": 160, "logsph-batch": 112, "logsph": 112, "cyl-pulsar": 112,
                        "yee-wave": 72, "yee-pulsar": 72, "gryee-wald": 112}
 
 
@@ -721,6 +724,9 @@ def run_variant(args):
                 "avg_launch_ms": avg}
         launches = sum(timing["launches"].values())
         launch_note = "stage + KO kernels counted by the solver's launch hooks"
+        if args.workload == "gr-wald":
+            launches += 2  # the E, H passes of the call, over both field buffers
+            launch_note += ", plus the two E, H passes of the call"
         if args.workload == "gryee-wald":
             launches = objs[0][2].launches_per_step() * args.steps
             launch_note = ("per substep: E/H, rho, shell, update and clamp passes, and the "

@@ -760,7 +760,7 @@ extern "C" int coffee_solver_set_timing(coffee_solver* s, int enable) {
 
 extern "C" int coffee_solver_launches_per_step(coffee_solver* s) {
   if (s && s->variant == COFFEE_VARIANT_LOGSPH) return 12;  // + axis after each, + 1 per call
-  if (s && s->variant == COFFEE_VARIANT_GR) return 11;      // + an E, H pass before each stage
+  if (s && s->variant == COFFEE_VARIANT_GR) return 6;       // + two E, H passes per call
   if (s && s->variant == COFFEE_VARIANT_YEE)
     // shell + update + clamp per substep; the star boundary adds its three
     // passes and the guard pass (the box problem: one guard pass per call)

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 #include "coffee_b200.h"
 #include "coffee_internal.h"
@@ -95,37 +96,59 @@ int gr_steps_t(const coffee_env* env, void* ehbuf, void* const A_[7], void* cons
   F5<T> aux;
   for (int k = 0; k < 5; ++k) aux.p[k] = aux_ ? static_cast<T*>(aux_[k]) : nullptr;
   const size_t n = (size_t)c.d[0] * c.d[1] * c.d[2];
-  F7<T> eh;
-  for (int k = 0; k < 6; ++k) eh.p[k] = static_cast<T*>(ehbuf) + k * n;
-  eh.p[6] = nullptr;
-  const T* sgt = static_cast<const T*>(ehbuf) + 6 * n;  // sqrt(gamma), set up by gr_setup
-  const T* mt = sgt + n;                                 // the near-horizon metric table
+  // E and H of each field buffer: ehA of A, ehB of B
+  F7<T> ehA, ehB, none;
+  for (int k = 0; k < 6; ++k) {
+    ehA.p[k] = static_cast<T*>(ehbuf) + k * n;
+    ehB.p[k] = static_cast<T*>(ehbuf) + (6 + k) * n;
+  }
+  ehA.p[6] = ehB.p[6] = nullptr;
+  for (int k = 0; k < 7; ++k) none.p[k] = nullptr;
+  const T* sgt = static_cast<const T*>(ehbuf) + 12 * n;  // sqrt(gamma), set up by gr_setup
+  const T* mt = sgt + n;                                  // the near-horizon metric table
   const dim3 gfull = grid_over(c.d[0], c.d[1], c.d[2]);
   const dim3 gbox = grid_over(c.hi[0] - c.lo[0], c.hi[1] - c.lo[1], c.hi[2] - c.lo[2]);
+  // COFFEE_GR_EH_PER_STAGE=1: the E, H pass before every stage instead
+  // (the same values; for comparisons)
+  const char* ev = std::getenv("COFFEE_GR_EH_PER_STAGE");
+  const bool per_stage = ev != nullptr && ev[0] == '1';
+  if (nsteps > 0 && !per_stage) {
+    // the fields may have changed since the last call (upload, pointer
+    // access): E and H of both buffers, guards included; B's interior is
+    // rewritten by the first stage
+    gr_eh_kernel<T><<<gfull, kBlock, 0, st>>>(c, A, ehA, mt);
+    COFFEE_CUDA_TRY(cudaGetLastError());
+    gr_eh_kernel<T><<<gfull, kBlock, 0, st>>>(c, Bb, ehB, mt);
+    COFFEE_CUDA_TRY(cudaGetLastError());
+  }
   for (int step = 0; step < nsteps; ++step) {
     for (int s = 0; s < 5; ++s) {
       const F7<T>& src = (s % 2 == 0) ? A : Bb;
       const F7<T>& dst = (s % 2 == 0) ? Bb : A;
+      const F7<T>& ehs = (s % 2 == 0) ? ehA : ehB;
+      const F7<T>& ehd = per_stage ? none : ((s % 2 == 0) ? ehB : ehA);
       int flags = 0;
       if (s == 4) flags |= AX_LAST | (aux_ ? AX_AUX : 0);
       if (s == 0) flags |= AX_WRITE_UN;
-      gr_eh_kernel<T><<<gfull, kBlock, 0, st>>>(c, src, eh, mt);
-      COFFEE_CUDA_TRY(cudaGetLastError());
+      if (per_stage) {
+        gr_eh_kernel<T><<<gfull, kBlock, 0, st>>>(c, src, ehs, mt);
+        COFFEE_CUDA_TRY(cudaGetLastError());
+      }
       const int kind = s == 0 ? COFFEE_KERNEL_STAGE_FIRST : COFFEE_KERNEL_STAGE;
       int rc = hook ? hook->before(kind) : COFFEE_OK;
       if (rc) return rc;
       if (s == 0)
-        gr_stage_kernel<T, true><<<gbox, kBlock, 0, st>>>(c, src, eh, dst, dU, Un, aux, mt, sgt,
-                                                          (T)kAs[s], (T)kBs[s], flags);
+        gr_stage_kernel<T, true><<<gbox, kBlock, 0, st>>>(c, src, ehs, dst, dU, Un, aux, mt, sgt,
+                                                          (T)kAs[s], (T)kBs[s], flags, ehd);
       else
-        gr_stage_kernel<T, false><<<gbox, kBlock, 0, st>>>(c, src, eh, dst, dU, Un, aux, mt, sgt,
-                                                           (T)kAs[s], (T)kBs[s], flags);
+        gr_stage_kernel<T, false><<<gbox, kBlock, 0, st>>>(c, src, ehs, dst, dU, Un, aux, mt, sgt,
+                                                           (T)kAs[s], (T)kBs[s], flags, ehd);
       COFFEE_CUDA_TRY(cudaGetLastError());
       if (hook && (rc = hook->after(kind))) return rc;
     }
     int rc = hook ? hook->before(COFFEE_KERNEL_KO) : COFFEE_OK;
     if (rc) return rc;
-    gr_ko_kernel<T><<<gbox, kBlock, 0, st>>>(c, Bb, A, mt);
+    gr_ko_kernel<T><<<gbox, kBlock, 0, st>>>(c, Bb, A, mt, per_stage ? none : ehA);
     COFFEE_CUDA_TRY(cudaGetLastError());
     if (hook && (rc = hook->after(COFFEE_KERNEL_KO))) return rc;
   }
@@ -152,7 +175,7 @@ int gr_fill_metric(const coffee_env* env, void* ehbuf) {
   GrConst<T> c;
   fill_gr_const<T>(env, &c);
   const size_t n = (size_t)c.d[0] * c.d[1] * c.d[2];
-  T* sg = static_cast<T*>(ehbuf) + 6 * n;
+  T* sg = static_cast<T*>(ehbuf) + 12 * n;
   gr_metric_kernel<T><<<grid_over(c.d[0], c.d[1], c.d[2]), kBlock>>>(c, sg + n, sg);
   COFFEE_CUDA_TRY(cudaGetLastError());
   COFFEE_CUDA_TRY(cudaDeviceSynchronize());
@@ -160,15 +183,15 @@ int gr_fill_metric(const coffee_env* env, void* ehbuf) {
 }
 }  // namespace
 
-// Scratch of the GR solver: E and H (6 arrays), sqrt(gamma) of every point
-// and the near-horizon metric table (kMetricComps arrays over the box), all
-// evaluated in FP64.
+// Scratch of the GR solver: E and H of each field buffer (2 x 6 arrays),
+// sqrt(gamma) of every point and the near-horizon metric table
+// (kMetricComps arrays over the box), the last two evaluated in FP64.
 int gr_setup(const coffee_env* env, int elem, void** ehbuf) {
   const coffee_grid& g = env->grid;
   const size_t n = (size_t)g.dims[0] * g.dims[1] * g.dims[2];
   const size_t nt = elem == 4 ? near_points<float>(env) : near_points<double>(env);
   *ehbuf = nullptr;
-  cudaError_t err = cudaMalloc(ehbuf, (7 * n + kMetricComps * nt + 1) * (size_t)elem);
+  cudaError_t err = cudaMalloc(ehbuf, (13 * n + kMetricComps * nt + 1) * (size_t)elem);
   if (err != cudaSuccess) {
     *ehbuf = nullptr;
     return fail(COFFEE_E_NOMEM, "GR scratch (E, H, metric table) allocation failed: %s",

@@ -198,8 +198,29 @@ __device__ __forceinline__ Cks<T> metric_at(const GrConst<T>& c, const T* __rest
   return q;
 }
 
-// E and H over the whole grid (kernel_compute_E_gr / kernel_compute_H_gr,
-// field_solver_gr_EZ.cu:88-186).  eh[0..2] = E, eh[3..5] = H.
+// E = alpha D + sqrt(gamma) beta x B and H = alpha B - sqrt(gamma) beta x D
+// (lowered D, B) at one point, stored at offset o of eh[0..5]
+// (kernel_compute_E_gr / kernel_compute_H_gr, field_solver_gr_EZ.cu:88-186).
+// Every kernel that writes D and B at a point also writes E and H there
+// through this function, so they are computed the same way everywhere.
+template <typename T>
+__device__ __forceinline__ void gr_eh_store(const Cks<T>& m, const T* D, const T* B,
+                                            const F7<T>& eh, long long o) {
+  T Dd[3], Bd[3];
+  m.lower(D, Dd);
+  m.lower(B, Bd);
+  eh.p[0][o] = m.alpha * Dd[0] + m.sg * (m.bu[1] * B[2] - m.bu[2] * B[1]);
+  eh.p[1][o] = m.alpha * Dd[1] + m.sg * (m.bu[2] * B[0] - m.bu[0] * B[2]);
+  eh.p[2][o] = m.alpha * Dd[2] + m.sg * (m.bu[0] * B[1] - m.bu[1] * B[0]);
+  eh.p[3][o] = m.alpha * Bd[0] - m.sg * (m.bu[1] * D[2] - m.bu[2] * D[1]);
+  eh.p[4][o] = m.alpha * Bd[1] - m.sg * (m.bu[2] * D[0] - m.bu[0] * D[2]);
+  eh.p[5][o] = m.alpha * Bd[2] - m.sg * (m.bu[0] * D[1] - m.bu[1] * D[0]);
+}
+
+// E and H over the whole grid (guards included): once per call of the
+// solver, for both field buffers; afterwards every stage and KO pass writes
+// E and H of the points it updates (ehout), so the next kernel finds those
+// of its input.  eh[0..2] = E, eh[3..5] = H.
 template <typename T>
 __global__ void __launch_bounds__(256) gr_eh_kernel(const __grid_constant__ GrConst<T> c,
                                                     const F7<T> u, const F7<T> eh,
@@ -213,15 +234,7 @@ __global__ void __launch_bounds__(256) gr_eh_kernel(const __grid_constant__ GrCo
       metric_at(c, mt, i, j, k, gr_pos(c, 0, i), gr_pos(c, 1, j), gr_pos(c, 2, k));
   const T D[3] = {__ldg(u.p[0] + o), __ldg(u.p[1] + o), __ldg(u.p[2] + o)};
   const T B[3] = {__ldg(u.p[3] + o), __ldg(u.p[4] + o), __ldg(u.p[5] + o)};
-  T Dd[3], Bd[3];
-  m.lower(D, Dd);
-  m.lower(B, Bd);
-  eh.p[0][o] = m.alpha * Dd[0] + m.sg * (m.bu[1] * B[2] - m.bu[2] * B[1]);
-  eh.p[1][o] = m.alpha * Dd[1] + m.sg * (m.bu[2] * B[0] - m.bu[0] * B[2]);
-  eh.p[2][o] = m.alpha * Dd[2] + m.sg * (m.bu[0] * B[1] - m.bu[1] * B[0]);
-  eh.p[3][o] = m.alpha * Bd[0] - m.sg * (m.bu[1] * D[2] - m.bu[2] * D[1]);
-  eh.p[4][o] = m.alpha * Bd[1] - m.sg * (m.bu[2] * D[0] - m.bu[0] * D[2]);
-  eh.p[5][o] = m.alpha * Bd[2] - m.sg * (m.bu[0] * D[1] - m.bu[1] * D[0]);
+  gr_eh_store(m, D, B, eh, o);
 }
 
 // clean_epar / check_eGTb with the 3-metric (kernel_clean_epar_gr,
@@ -306,7 +319,8 @@ __global__ void __launch_bounds__(256, COFFEE_GR_STAGE_MIN_BLOCKS) gr_stage_kern
                                                        const F7<T> un, const F5<T> aux,
                                                        const T* __restrict__ mt,
                                                        const T* __restrict__ sgt, const T As,
-                                                       const T Bs, const int flags) {
+                                                       const T Bs, const int flags,
+                                                       const F7<T> ehout) {
   const int i = c.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = c.lo[1] + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = c.lo[2] + blockIdx.z * blockDim.z + threadIdx.z;
@@ -412,6 +426,7 @@ __global__ void __launch_bounds__(256, COFFEE_GR_STAGE_MIN_BLOCKS) gr_stage_kern
   }
 #pragma unroll
   for (int a = 0; a < 7; ++a) out.p[a][o] = w.v[a];
+  if (ehout.p[0]) gr_eh_store(m, w.v, w.v + 3, ehout, o);
 }
 
 // Kreiss-Oliger pass (kernel_KO_step1_gr / _step2_gr, :523-608, with the
@@ -419,7 +434,8 @@ __global__ void __launch_bounds__(256, COFFEE_GR_STAGE_MIN_BLOCKS) gr_stage_kern
 template <typename T>
 __global__ void __launch_bounds__(256) gr_ko_kernel(const __grid_constant__ GrConst<T> c,
                                                     const F7<T> u, const F7<T> out,
-                                                    const T* __restrict__ mt) {
+                                                    const T* __restrict__ mt,
+                                                    const F7<T> ehout) {
   const int i = c.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = c.lo[1] + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = c.lo[2] + blockIdx.z * blockDim.z + threadIdx.z;
@@ -445,6 +461,7 @@ __global__ void __launch_bounds__(256) gr_ko_kernel(const __grid_constant__ GrCo
   gr_clamps(c, m, v);
 #pragma unroll
   for (int a = 0; a < 7; ++a) out.p[a][o] = v[a];
+  if (ehout.p[0]) gr_eh_store(m, v, v + 3, ehout, o);
 }
 
 }  // namespace coffee

@@ -133,6 +133,35 @@ def test_gr_matches_reference_gpu_build(case):
     _compare(case, out, r32, r64, list(np64))
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_gr_eh_from_the_writing_kernel_is_bitwise(dtype, monkeypatch):
+    """E and H written by the stage and KO kernels for the next kernel (with
+    one E, H pass per call) give bitwise the fields of an E, H pass before
+    every stage, over calls of several steps and single steps, with the
+    inner and outer absorbing layers active."""
+    p = problems.wald_params(N=40, half_size=5.0, a=0.9, pml=6)
+    f = [a.astype(dtype) for a in problems.wald_fields(p, np.float64)]
+
+    def run(per_stage):
+        monkeypatch.setenv("COFFEE_GR_EH_PER_STAGE", "1" if per_stage else "0")
+        env = SimEnvironment(p)
+        data = SimData(env, dtype)
+        data.upload(f)
+        solver = FieldSolverGrEZ(data, env)
+        solver.step(0.0, 5)
+        solver.step(0.0, 1)
+        solver.step(0.0, 3)
+        out = data.download()
+        solver.close()
+        data.close()
+        env.close()
+        return out
+
+    a, b = run(False), run(True)
+    for k in range(7):
+        assert np.array_equal(a[k], b[k]), k
+
+
 FLAT_CASES = {
     "flat_pulsar": lambda: problems.pulsar_params(N=40, guard=3, half_size=10.0, radius=2.5,
                                                   omega=0.1, pml=6),
