@@ -492,8 +492,8 @@ int check_grid(int n, int d, int h, int w) {
 // the CTA frees its tensor memory and returns.  The launching call of the
 // next convolution reports COFFEE_E_TIMEOUT until the fault is cleared.
 constexpr int kTcM = 128;                         // points per tile = MMA M
-constexpr int kTcStages = 8;                      // A ring slots at most (32 KB of ring)
-constexpr int kTcRing = 32768;                    // bytes of the A ring
+constexpr int kTcStages = 8;                      // A ring slots at most
+constexpr int kTcSlot = 16384;                    // bytes of one A ring slot (64 channels)
 constexpr int kTcThreads = 192;                   // 4 epilogue warps, producer, MMA
 constexpr long long kTcWaitCycles = 4000000000LL; // about 2 s at 1.9 GHz
 
@@ -582,7 +582,7 @@ template <int N, int CB>
 __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
     const __grid_constant__ CUtensorMap xmap, Grid4 g, int C, const bf16* __restrict__ w,
     const float* __restrict__ bias, float* __restrict__ z, bf16* __restrict__ a, int act,
-    float slope, TcBox box, const TcWaitParams wp) {
+    float slope, TcBox box, const TcWaitParams wp, const int nslots) {
   static_assert(N % 16 == 0 && N >= 16 && N <= 64, "N = 16, 32, 48 or 64");
   static_assert(CB == 16 || CB == 32 || CB == 64, "boxes of 16, 32 or 64 channels");
   constexpr int NCOLS = N <= 32 ? 32 : 64;  // columns of one accumulator (power of two >= 32)
@@ -595,19 +595,25 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int cchunks = C / 16, nks = 27 * cchunks;
-  // A stage: one box of cb channels (16, 32 or 64: rows of 32, 64 or 128
-  // bytes under the swizzle of that width), cb / 16 MMAs
+  // A box: 128 points x cb channels (16, 32 or 64: rows of 32, 64 or 128
+  // bytes under the swizzle of that width), cb / 16 MMAs.  A stage (one ring
+  // slot, one full / empty barrier pair) holds U = 64 / cb consecutive boxes,
+  // so that every stage feeds up to four MMAs: the barrier round trip per
+  // stage, not the tensor pipe, bounded the kernel with one box per stage.
   constexpr int sub = CB / 16;
-  constexpr uint32_t slot = (uint32_t)(kTcM * CB * 2);
-  constexpr uint32_t stages = (uint32_t)(kTcRing / (kTcM * CB * 2));
+  constexpr int U = 64 / CB;
+  constexpr uint32_t boxb = (uint32_t)(kTcM * CB * 2);
+  constexpr uint32_t slot = (uint32_t)kTcSlot;
+  static_assert(U * boxb == slot, "a stage fills one slot");
   constexpr uint32_t layout = CB == 16 ? 6u : (CB == 32 ? 4u : 2u);  // 32B / 64B / 128B swizzle
   // boxes per tap; a box may reach past C (C = 48 in 64-channel boxes): the
   // TMA unit fills those channels with zeros and no MMA reads them
-  const int bchunks = (C + CB - 1) / CB, nstage = 27 * bchunks;
+  const int bchunks = (C + CB - 1) / CB, units = 27 * bchunks, nstage = (units + U - 1) / U;
+  const uint32_t stages = (uint32_t)nslots;
   // A ring at the first 1024-byte boundary (the swizzle atoms repeat every
   // 256 to 1024 bytes), the weights after it
   const uint32_t abase = (smem_addr(tc_smem) + 1023u) & ~1023u;
-  const uint32_t wbase = abase + (uint32_t)kTcRing;
+  const uint32_t wbase = abase + stages * slot;
   const uint32_t full0 = smem_addr(full_s), empty0 = smem_addr(empty_s);
   const uint32_t ready0 = smem_addr(ready_s), free0 = smem_addr(free_s);
   volatile int* abort = &abort_s;
@@ -658,7 +664,7 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
   if (warp == 4) {
     // ---- producer: one TMA load per K step into the ring
     if (lane == 0) {
-      uint32_t step = 0;
+      uint32_t step = 0, b = 0, ph = 0;  // slot and phase of step: step % stages, (step / stages) & 1
       const uint64_t map = reinterpret_cast<uint64_t>(&xmap);
       for (long long t = blockIdx.x; t < ntiles && !wp.stall_producer; t += gridDim.x) {
         int n, x0, y0, z0;
@@ -666,25 +672,31 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
         bool ok = true;
         int tap = 0, q = 0;
         for (int s = 0; s < nstage && ok; ++s, ++step) {
-          const uint32_t b = step % stages;
-          if (step >= stages && !tc_wait(empty0 + 8 * b, ((step / stages) - 1) & 1, abort, wp)) {
+          if (step >= stages && !tc_wait(empty0 + 8 * b, ph ^ 1u, abort, wp)) {
             ok = false;
             break;
           }
-          const int c0 = q * CB;
-          const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+          const int nb = min(U, units - s * U);  // boxes of this stage
           asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(full0 + 8 * b),
-                       "r"(slot)
+                       "r"((uint32_t)nb * boxb)
                        : "memory");
-          asm volatile(
-              "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
-              "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(abase + b * slot),
-              "l"(map), "r"(c0), "r"(x0 + dx), "r"(y0 + dy), "r"(z0 + dz), "r"(n),
-              "r"(full0 + 8 * b)
-              : "memory");
-          if (++q == bchunks) {
-            q = 0;
-            ++tap;
+          for (int j = 0; j < nb; ++j) {
+            const int c0 = q * CB;
+            const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+            asm volatile(
+                "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+                "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(abase + b * slot + (uint32_t)j * boxb),
+                "l"(map), "r"(c0), "r"(x0 + dx), "r"(y0 + dy), "r"(z0 + dz), "r"(n),
+                "r"(full0 + 8 * b)
+                : "memory");
+            if (++q == bchunks) {
+              q = 0;
+              ++tap;
+            }
+          }
+          if (++b == stages) {
+            b = 0;
+            ph ^= 1u;
           }
         }
         if (!ok) break;
@@ -702,7 +714,7 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
   } else if (warp == 5) {
     // ---- MMA issuer
     if (lane == 0) {
-      uint32_t step = 0, tiles = 0;
+      uint32_t step = 0, tiles = 0, b = 0, ph = 0;
       bool ok = true;
       for (long long t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++tiles) {
         const uint32_t acc = tiles & 1, use = tiles >> 1;
@@ -712,33 +724,41 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_fwd_tc_kernel(
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t d = tmem + acc * NCOLS;
-        int s16 = 0;  // 16-channel K step of the stage's first MMA
-        int cq = 0;   // first channel of the stage's box
+        int s16 = 0;  // 16-channel K step of the next MMA
+        int cq = 0;   // first channel of the next box
         for (int s = 0; s < nstage; ++s, ++step) {
-          const uint32_t b = step % stages;
-          if (!tc_wait(full0 + 8 * b, (step / stages) & 1, abort, wp)) {
+          if (!tc_wait(full0 + 8 * b, ph, abort, wp)) {
             ok = false;
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const int nb = min(U, units - s * U);
+          for (int jb = 0; jb < nb; ++jb) {
 #pragma unroll
-          for (int j = 0; j < sub; ++j, ++s16) {
-            if (cq + 16 * j >= C) break;  // past the tensor's channels
-            // K slice j of the swizzled rows: the descriptor start moves 32 bytes
-            const uint64_t ad = tc_sdesc(abase + b * slot + 32u * j, 16, 8u * CB * 2, layout);
-            const uint64_t bd = tc_sdesc(wbase + (uint32_t)(s16 * N * 32), (N / 8) * 128, 128, 0);
-            asm volatile(
-                "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
-                "l"(ad), "l"(bd), "r"(kIdesc), "r"((s > 0 || j > 0) ? 1 : 0)
-                : "memory");
+            for (int j = 0; j < sub; ++j) {
+              if (cq + 16 * j >= C) break;  // past the tensor's channels
+              // K slice j of box jb's swizzled rows: the descriptor start moves 32 bytes
+              const uint64_t ad =
+                  tc_sdesc(abase + b * slot + (uint32_t)jb * boxb + 32u * j, 16, 8u * CB * 2, layout);
+              const uint64_t bd = tc_sdesc(wbase + (uint32_t)(s16 * N * 32), (N / 8) * 128, 128, 0);
+              asm volatile(
+                  "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                  " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+                  "l"(ad), "l"(bd), "r"(kIdesc), "r"(s16 > 0 ? 1 : 0)
+                  : "memory");
+              ++s16;
+            }
+            cq += CB;
+            if (cq >= C) cq = 0;
           }
           asm volatile(
               "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                   empty0 + 8 * b)
               : "memory");
-          cq += CB;
-          if (cq >= C) cq = 0;
+          if (++b == stages) {
+            b = 0;
+            ph ^= 1u;
+          }
         }
         if (!ok) break;
         asm volatile(
@@ -873,11 +893,19 @@ int launch_fwd_tc(const bf16* x, Grid4 g, int C, const bf16* w, const float* bia
     return fail(COFFEE_E_TIMEOUT,
                 "an earlier tcgen05 convolution ran out of time waiting on its pipeline "
                 "(its results are invalid); clear the fault with coffee_conv3d_tc_fault");
-  const size_t smem = 1024 + (size_t)kTcRing + (size_t)27 * C * N * 2;
+  // ring slots: as many as let two CTAs share an SM (113 KB each), at least
+  // two, at most kTcStages; with large weights one CTA per SM and a deeper ring
+  const size_t wbytes = (size_t)27 * C * N * 2;
+  int nslots = (int)std::min<long long>(
+      kTcStages, ((long long)113 * 1024 - 1024 - (long long)wbytes) / kTcSlot);
+  if (nslots < 2)
+    nslots = (int)std::min<long long>(
+        kTcStages, ((long long)227 * 1024 - 1024 - (long long)wbytes) / kTcSlot);
+  const size_t smem = 1024 + (size_t)nslots * kTcSlot + wbytes;
   // channels per TMA box: the widest that divides C; 48 channels in one
   // 64-channel box (the last 16 zero-filled, not multiplied)
   const int cb = (C % 64 == 0 || C == 48) ? 64 : (C % 32 == 0 ? 32 : 16);
-  if (smem > 200 * 1024)
+  if (nslots < 2 || smem > 227 * 1024)
     return fail(COFFEE_E_INVALID, "tcgen05 convolution: %d x %d weights exceed shared memory", N,
                 C);
   // the box: x extent a power of two in [8, 128], then y, then z
@@ -925,7 +953,7 @@ int launch_fwd_tc(const bf16* x, Grid4 g, int C, const bf16* w, const float* bia
   const long long ntiles = (long long)g.n * box.tx * box.ty * box.tz;
   const unsigned blocks = (unsigned)std::min<long long>(ntiles, (long long)sms * per_sm);
   const TcWaitParams wp{g_tc_cycles, g_tc_stall, g_tc_fault_dev};
-  kern<<<blocks, kTcThreads, smem, st>>>(map, g, C, w, bias, z, a, act, slope, box, wp);
+  kern<<<blocks, kTcThreads, smem, st>>>(map, g, C, w, bias, z, a, act, slope, box, wp, nslots);
   COFFEE_CUDA_TRY(cudaGetLastError());
   return COFFEE_OK;
 }
