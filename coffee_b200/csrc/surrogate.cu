@@ -494,6 +494,10 @@ int check_grid(int n, int d, int h, int w) {
 constexpr int kTcM = 128;                         // points per tile = MMA M
 constexpr int kTcStages = 8;                      // A ring slots at most
 constexpr int kTcSlot = 16384;                    // bytes of one A ring slot (64 channels)
+#ifndef COFFEE_TC_CB48
+#define COFFEE_TC_CB48 64
+#endif
+static_assert(COFFEE_TC_CB48 == 16 || COFFEE_TC_CB48 == 64, "48 channels in 16- or 64-channel boxes");
 constexpr int kTcThreads = 192;                   // 4 epilogue warps, producer, MMA
 constexpr long long kTcWaitCycles = 4000000000LL; // about 2 s at 1.9 GHz
 
@@ -902,9 +906,10 @@ int launch_fwd_tc(const bf16* x, Grid4 g, int C, const bf16* w, const float* bia
     nslots = (int)std::min<long long>(
         kTcStages, ((long long)227 * 1024 - 1024 - (long long)wbytes) / kTcSlot);
   const size_t smem = 1024 + (size_t)nslots * kTcSlot + wbytes;
-  // channels per TMA box: the widest that divides C; 48 channels in one
-  // 64-channel box (the last 16 zero-filled, not multiplied)
-  const int cb = (C % 64 == 0 || C == 48) ? 64 : (C % 32 == 0 ? 32 : 16);
+  // channels per TMA box: the widest that divides C; 48 channels in
+  // COFFEE_TC_CB48-channel boxes: 64 (one box per tap, the last 16 channels
+  // zero-filled and not multiplied) or 16 (three boxes per tap, no waste)
+  const int cb = C == 48 ? COFFEE_TC_CB48 : (C % 64 == 0 ? 64 : (C % 32 == 0 ? 32 : 16));
   if (nslots < 2 || smem > 227 * 1024)
     return fail(COFFEE_E_INVALID, "tcgen05 convolution: %d x %d weights exceed shared memory", N,
                 C);
