@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <type_traits>
 
 #include "coffee_b200.h"
 #include "coffee_internal.h"
@@ -112,6 +113,25 @@ int gr_steps_t(const coffee_env* env, void* ehbuf, void* const A_[7], void* cons
   // (the same values; for comparisons)
   const char* ev = std::getenv("COFFEE_GR_EH_PER_STAGE");
   const bool per_stage = ev != nullptr && ev[0] == '1';
+  // COFFEE_GR_TILED=1: FP32 stages stream through shared-memory tiles
+  // (gr_stage_tile_kernel, the same arithmetic as gr_stage_kernel)
+  const char* et = std::getenv("COFFEE_GR_TILED");
+  const bool tiled = std::is_same<T, float>::value && et != nullptr && et[0] == '1';
+  const int kchunk = COFFEE_GR_KCHUNK;
+  const dim3 tblock(kGrTX, kGrTY, 1);
+  const dim3 gtile((unsigned)((c.hi[0] - c.lo[0] + kGrTX - 1) / kGrTX),
+                   (unsigned)((c.hi[1] - c.lo[1] + kGrTY - 1) / kGrTY),
+                   (unsigned)((c.hi[2] - c.lo[2] + kchunk - 1) / kchunk));
+  if (tiled && nsteps > 0) {
+    static bool attr_set[2] = {false, false};
+    for (int f = 0; f < 2; ++f) {
+      if (attr_set[f]) continue;
+      const void* fn = f ? (const void*)gr_stage_tile_kernel<true> : (const void*)gr_stage_tile_kernel<false>;
+      COFFEE_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)gr_tile_smem_bytes()));
+      attr_set[f] = true;
+    }
+  }
   if (nsteps > 0 && !per_stage) {
     // the fields may have changed since the last call (upload, pointer
     // access): E and H of both buffers, guards included; B's interior is
@@ -137,12 +157,22 @@ int gr_steps_t(const coffee_env* env, void* ehbuf, void* const A_[7], void* cons
       const int kind = s == 0 ? COFFEE_KERNEL_STAGE_FIRST : COFFEE_KERNEL_STAGE;
       int rc = hook ? hook->before(kind) : COFFEE_OK;
       if (rc) return rc;
-      if (s == 0)
+      if (tiled) {
+        if constexpr (std::is_same<T, float>::value) {
+          if (s == 0)
+            gr_stage_tile_kernel<true><<<gtile, tblock, gr_tile_smem_bytes(), st>>>(
+                c, src, ehs, dst, dU, Un, aux, mt, sgt, (T)kAs[s], (T)kBs[s], flags, ehd, kchunk);
+          else
+            gr_stage_tile_kernel<false><<<gtile, tblock, gr_tile_smem_bytes(), st>>>(
+                c, src, ehs, dst, dU, Un, aux, mt, sgt, (T)kAs[s], (T)kBs[s], flags, ehd, kchunk);
+        }
+      } else if (s == 0) {
         gr_stage_kernel<T, true><<<gbox, kBlock, 0, st>>>(c, src, ehs, dst, dU, Un, aux, mt, sgt,
                                                           (T)kAs[s], (T)kBs[s], flags, ehd);
-      else
+      } else {
         gr_stage_kernel<T, false><<<gbox, kBlock, 0, st>>>(c, src, ehs, dst, dU, Un, aux, mt, sgt,
                                                            (T)kAs[s], (T)kBs[s], flags, ehd);
+      }
       COFFEE_CUDA_TRY(cudaGetLastError());
       if (hook && (rc = hook->after(kind))) return rc;
     }

@@ -312,59 +312,60 @@ __device__ __noinline__ V7<T> gr_absorb(const GrConst<T>& c, V7<T> v, V7<T> n, T
 #ifndef COFFEE_GR_STAGE_MIN_BLOCKS
 #define COFFEE_GR_STAGE_MIN_BLOCKS 6
 #endif
-template <typename T, bool FIRST>
-__global__ void __launch_bounds__(256, COFFEE_GR_STAGE_MIN_BLOCKS) gr_stage_kernel(const __grid_constant__ GrConst<T> c,
-                                                       const F7<T> u, const F7<T> eh,
-                                                       const F7<T> out, const F7<T> du,
-                                                       const F7<T> un, const F5<T> aux,
-                                                       const T* __restrict__ mt,
-                                                       const T* __restrict__ sgt, const T As,
-                                                       const T Bs, const int flags,
-                                                       const F7<T> ehout) {
-  const int i = c.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = c.lo[1] + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = c.lo[2] + blockIdx.z * blockDim.z + threadIdx.z;
-  if (i >= c.hi[0] || j >= c.hi[1] || k >= c.hi[2]) return;
-  const long long sx = 1, sy = c.d[0], sz = (long long)c.d[0] * c.d[1];
-  const long long o = i + sy * j + sz * k;
-  const long long st[3] = {sx, sy, sz};
-  const T x = gr_pos(c, 0, i), y = gr_pos(c, 1, j), z = gr_pos(c, 2, k);
-  const Cks<T> m = metric_at(c, mt, i, j, k, x, y, z);
+// The stage at one point, given its stencil values through fetch(q, ax,
+// n): array q (0-2 E, 3-5 H, 6-8 D, 9-11 B, 12 P, 13 sqrt(gamma)) at offset
+// n = -2, -1, 1, 2 along axis ax from the point, and own(q), array q at the
+// point (read where the values are first needed, which keeps them out of
+// the registers of the stencil sums).  Both stage kernels (global stencil
+// loads, shared-memory tiles) run this code, so their arithmetic is the
+// same.
+template <typename T, bool FIRST, typename Fetch, typename Own>
+__device__ __forceinline__ void gr_stage_point(const GrConst<T>& c, const Cks<T>& m, const T x,
+                                               const T y, const T z, const long long o,
+                                               Fetch&& f, Own&& own,
+                                               const F7<T>& out, const F7<T>& du,
+                                               const F7<T>& un, const F5<T>& aux, const T As,
+                                               const T Bs, const int flags,
+                                               const F7<T>& ehout) {
   const T igms = T(1) / m.sg;
-
-  auto d1 = [&](const T* f, int ax) {
-    const long long s = st[ax];
-    return d1_4w(__ldg(f + o - 2 * s), __ldg(f + o - s), __ldg(f + o + s), __ldg(f + o + 2 * s)) *
-           c.inv_delta[ax];
+  auto d1 = [&](auto qc, auto ac) {
+    constexpr int ax = decltype(ac)::value;
+    return d1_4w(f(qc, ac, -2), f(qc, ac, -1), f(qc, ac, 1), f(qc, ac, 2)) * c.inv_delta[ax];
   };
-  const T rotH[3] = {(d1(eh.p[5], 1) - d1(eh.p[4], 2)) * igms,
-                     (d1(eh.p[3], 2) - d1(eh.p[5], 0)) * igms,
-                     (d1(eh.p[4], 0) - d1(eh.p[3], 1)) * igms};
-  const T rotE[3] = {(d1(eh.p[2], 1) - d1(eh.p[1], 2)) * igms,
-                     (d1(eh.p[0], 2) - d1(eh.p[2], 0)) * igms,
-                     (d1(eh.p[1], 0) - d1(eh.p[0], 1)) * igms};
+  using I0 = std::integral_constant<int, 0>;
+  using I1 = std::integral_constant<int, 1>;
+  using I2 = std::integral_constant<int, 2>;
+  const T rotH[3] = {(d1(std::integral_constant<int, 5>{}, I1{}) -
+                      d1(std::integral_constant<int, 4>{}, I2{})) * igms,
+                     (d1(std::integral_constant<int, 3>{}, I2{}) -
+                      d1(std::integral_constant<int, 5>{}, I0{})) * igms,
+                     (d1(std::integral_constant<int, 4>{}, I0{}) -
+                      d1(std::integral_constant<int, 3>{}, I1{})) * igms};
+  const T rotE[3] = {(d1(std::integral_constant<int, 2>{}, I1{}) -
+                      d1(std::integral_constant<int, 1>{}, I2{})) * igms,
+                     (d1(std::integral_constant<int, 0>{}, I2{}) -
+                      d1(std::integral_constant<int, 2>{}, I0{})) * igms,
+                     (d1(std::integral_constant<int, 1>{}, I0{}) -
+                      d1(std::integral_constant<int, 0>{}, I1{})) * igms};
   // div4 (:44-86): each neighbour weighted by sqrt(gamma) there (the
   // per-solver table; the reference evaluates it at the shifted coordinates)
   T divD = T(0), divB = T(0);
-  {
-#pragma unroll
-    for (int ax = 0; ax < 3; ++ax) {
-      const long long s = st[ax];
-      const T w[4] = {__ldg(sgt + o - 2 * s), __ldg(sgt + o - s), __ldg(sgt + o + s),
-                      __ldg(sgt + o + 2 * s)};
-      const T* fD = u.p[ax];
-      const T* fB = u.p[3 + ax];
-      divD += d1_4w(__ldg(fD + o - 2 * s) * w[0], __ldg(fD + o - s) * w[1],
-                    __ldg(fD + o + s) * w[2], __ldg(fD + o + 2 * s) * w[3]) * c.inv_delta[ax];
-      divB += d1_4w(__ldg(fB + o - 2 * s) * w[0], __ldg(fB + o - s) * w[1],
-                    __ldg(fB + o + s) * w[2], __ldg(fB + o + 2 * s) * w[3]) * c.inv_delta[ax];
-    }
-    divD *= igms;
-    divB *= igms;
-  }
+  static_for<3>([&](auto ac) {
+    constexpr int ax = decltype(ac)::value;
+    using QS = std::integral_constant<int, 13>;
+    using QD = std::integral_constant<int, 6 + ax>;
+    using QB = std::integral_constant<int, 9 + ax>;
+    const T w[4] = {f(QS{}, ac, -2), f(QS{}, ac, -1), f(QS{}, ac, 1), f(QS{}, ac, 2)};
+    divD += d1_4w(f(QD{}, ac, -2) * w[0], f(QD{}, ac, -1) * w[1], f(QD{}, ac, 1) * w[2],
+                  f(QD{}, ac, 2) * w[3]) * c.inv_delta[ax];
+    divB += d1_4w(f(QB{}, ac, -2) * w[0], f(QB{}, ac, -1) * w[1], f(QB{}, ac, 1) * w[2],
+                  f(QB{}, ac, 2) * w[3]) * c.inv_delta[ax];
+  });
+  divD *= igms;
+  divB *= igms;
   T v[7];
 #pragma unroll
-  for (int a = 0; a < 7; ++a) v[a] = __ldg(u.p[a] + o);
+  for (int a = 0; a < 7; ++a) v[a] = own(6 + a);
   T Bd[3], Dd[3];
   m.lower(v + 3, Bd);
   m.lower(v, Dd);
@@ -374,13 +375,14 @@ __global__ void __launch_bounds__(256, COFFEE_GR_STAGE_MIN_BLOCKS) gr_stage_kern
     if (B2 < Tiny<T>::v) B2 = Tiny<T>::v;
     const T Jp = (Bd[0] * rotH[0] + Bd[1] * rotH[1] + Bd[2] * rotH[2]) -
                  (Dd[0] * rotE[0] + Dd[1] * rotE[1] + Dd[2] * rotE[2]);
-    const T e0 = __ldg(eh.p[0] + o), e1 = __ldg(eh.p[1] + o), e2 = __ldg(eh.p[2] + o);
+    const T e0 = own(0), e1 = own(1), e2 = own(2);
     const T iB2 = fdiv(T(1), B2);
     J[0] = (divD * (e1 * Bd[2] - e2 * Bd[1]) * igms + Jp * v[3]) * iB2;
     J[1] = (divD * (e2 * Bd[0] - e0 * Bd[2]) * igms + Jp * v[4]) * iB2;
     J[2] = (divD * (e0 * Bd[1] - e1 * Bd[0]) * igms + Jp * v[5]) * iB2;
   }
-  const T Pd[3] = {d1(u.p[6], 0), d1(u.p[6], 1), d1(u.p[6], 2)};
+  using QP = std::integral_constant<int, 12>;
+  const T Pd[3] = {d1(QP{}, I0{}), d1(QP{}, I1{}), d1(QP{}, I2{})};
   T Pu[3];
   m.raise(Pd, Pu);
   const T shape = T(0.5) * (T(1) - tanh((m.r - T(5)) / T(1)));  // r0 = 5, del = 1 (:276-278)
@@ -427,6 +429,170 @@ __global__ void __launch_bounds__(256, COFFEE_GR_STAGE_MIN_BLOCKS) gr_stage_kern
 #pragma unroll
   for (int a = 0; a < 7; ++a) out.p[a][o] = w.v[a];
   if (ehout.p[0]) gr_eh_store(m, w.v, w.v + 3, ehout, o);
+}
+
+template <typename T, bool FIRST>
+__global__ void __launch_bounds__(256, COFFEE_GR_STAGE_MIN_BLOCKS) gr_stage_kernel(const __grid_constant__ GrConst<T> c,
+                                                       const F7<T> u, const F7<T> eh,
+                                                       const F7<T> out, const F7<T> du,
+                                                       const F7<T> un, const F5<T> aux,
+                                                       const T* __restrict__ mt,
+                                                       const T* __restrict__ sgt, const T As,
+                                                       const T Bs, const int flags,
+                                                       const F7<T> ehout) {
+  const int i = c.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = c.lo[1] + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = c.lo[2] + blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= c.hi[0] || j >= c.hi[1] || k >= c.hi[2]) return;
+  const long long sx = 1, sy = c.d[0], sz = (long long)c.d[0] * c.d[1];
+  const long long o = i + sy * j + sz * k;
+  const long long st[3] = {sx, sy, sz};
+  const T x = gr_pos(c, 0, i), y = gr_pos(c, 1, j), z = gr_pos(c, 2, k);
+  const Cks<T> m = metric_at(c, mt, i, j, k, x, y, z);
+  // the array pointers straight from the kernel parameters (a local array
+  // of them would take registers this kernel does not have)
+  auto fetch = [&](auto qc, auto ac, int n) {
+    constexpr int q = decltype(qc)::value;
+    const T* p;
+    if constexpr (q < 6) p = eh.p[q];
+    else if constexpr (q < 13) p = u.p[q - 6];
+    else p = sgt;
+    return __ldg(p + o + n * st[decltype(ac)::value]);
+  };
+  auto own = [&](int q) { return __ldg((q < 6 ? eh.p[q] : u.p[q - 6]) + o); };
+  gr_stage_point<T, FIRST>(c, m, x, y, z, o, fetch, own, out, du, un, aux, As, Bs, flags, ehout);
+}
+
+// The same stage streamed along z through shared memory (FP32; opt-in with
+// COFFEE_GR_TILED=1).  A CTA owns a 32 x 8 column of points and a chunk of
+// z planes; each plane of the 14 stencil arrays (E, H, D, B, P,
+// sqrt(gamma)) with its 2-point x / y halo is copied by cp.async into a ring
+// of kGrRing planes ahead of the one computed, and the z neighbours of the
+// point's own column of the 8 arrays that are differentiated along z (E_x,
+// E_y, H_x, H_y, D_z, B_z, P, sqrt(gamma)) are kept in a register window of
+// planes k-2 .. k+2.  The per-point global stencil loads of gr_stage_kernel
+// become one coalesced copy per array and plane, but the metric, the
+// near-horizon table and the per-point reads and writes of dU, the
+// start-of-step copy, J and E, H keep the kernel latency-bound, and the
+// registers and shared memory of the tiles leave too few warps to hide it.
+// Measured at 256^3 (the Wald run): 5 slots and one CTA per SM (161
+// registers) 2.50 ms per stage, 4 slots and two CTAs per SM (128 registers)
+// 1.59 ms, the per-point gr_stage_kernel 1.28 ms, which stays the default.
+#ifndef COFFEE_GR_TILE_RING
+#define COFFEE_GR_TILE_RING 4
+#endif
+#ifndef COFFEE_GR_TILE_MINB
+#define COFFEE_GR_TILE_MINB 2
+#endif
+// ring slots: planes k .. k+2, PF = kGrRing - 4 planes in flight, the spare
+constexpr int kGrTX = 32, kGrTY = 8, kGrRing = COFFEE_GR_TILE_RING, kGrArrays = 14;
+constexpr int kGrPF = kGrRing - 4;
+static_assert(kGrPF == 0 || kGrPF == 1, "a ring of 4 or 5 planes");
+constexpr int kGrSX = kGrTX + 4, kGrSP = kGrSX * (kGrTY + 4);
+#ifndef COFFEE_GR_KCHUNK
+#define COFFEE_GR_KCHUNK 64
+#endif
+
+__host__ __device__ constexpr size_t gr_tile_smem_bytes() {
+  return (size_t)kGrRing * kGrArrays * kGrSP * sizeof(float);
+}
+
+// window slot of array q (only the 8 arrays differentiated along z)
+template <int Q>
+__device__ __forceinline__ constexpr int gr_wslot() {
+  return Q == 0 ? 0 : Q == 1 ? 1 : Q == 3 ? 2 : Q == 4 ? 3 : Q == 8 ? 4 : Q == 11 ? 5 : Q == 12 ? 6 : 7;
+}
+
+template <bool FIRST>
+__global__ void __launch_bounds__(kGrTX * kGrTY, COFFEE_GR_TILE_MINB) gr_stage_tile_kernel(
+    const __grid_constant__ GrConst<float> c, const F7<float> u, const F7<float> eh,
+    const F7<float> out, const F7<float> du, const F7<float> un, const F5<float> aux,
+    const float* __restrict__ mt, const float* __restrict__ sgt, const float As, const float Bs,
+    const int flags, const F7<float> ehout, const int kchunk) {
+  constexpr int NT = kGrTX * kGrTY, NLOAD = (kGrSP + NT - 1) / NT;
+  constexpr int WQ[8] = {0, 1, 3, 4, 8, 11, 12, 13};  // the window's arrays
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* ring = reinterpret_cast<float*>(smem_raw);  // [kGrRing][kGrArrays][kGrSP]
+  const uint32_t rbase = smem_u32(smem_raw);
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kGrTX + tx;
+  const int i = c.lo[0] + blockIdx.x * kGrTX + tx;
+  const int j = c.lo[1] + blockIdx.y * kGrTY + ty;
+  const int k0 = c.lo[2] + blockIdx.z * kchunk;
+  const int k1 = min(k0 + kchunk, c.hi[2]);
+  const bool active = i < c.hi[0] && j < c.hi[1];
+  const long long sy = c.d[0], sz = (long long)c.d[0] * c.d[1];
+  const float* arr[kGrArrays] = {eh.p[0], eh.p[1], eh.p[2], eh.p[3], eh.p[4],
+                                 eh.p[5], u.p[0],  u.p[1],  u.p[2],  u.p[3],
+                                 u.p[4],  u.p[5],  u.p[6],  sgt};
+  // this thread's copies of a plane: tile point e -> shared slot, global offset
+  const int gx0 = c.lo[0] + (int)blockIdx.x * kGrTX - 2, gy0 = c.lo[1] + (int)blockIdx.y * kGrTY - 2;
+  int soff[NLOAD];
+  long long goff[NLOAD];
+  bool lv[NLOAD];
+#pragma unroll
+  for (int m = 0; m < NLOAD; ++m) {
+    const int e = tid + m * NT, r = e / kGrSX, cl = e - r * kGrSX;
+    lv[m] = e < kGrSP && gx0 + cl < c.d[0] && gy0 + r < c.d[1];
+    soff[m] = e;
+    goff[m] = (long long)(gy0 + r) * sy + gx0 + cl;
+  }
+  const int kend = k1 + 2;  // planes [k0 - 2, k1 + 2) are read
+  auto slot_of = [&](int kp) { return (kp - k0) % kGrRing; };
+  auto issue = [&](int kp) {
+    if (kp < kend) {
+      const uint32_t sb = rbase + (uint32_t)(slot_of(kp) * kGrArrays * kGrSP) * 4u;
+#pragma unroll
+      for (int m = 0; m < NLOAD; ++m) {
+        if (!lv[m]) continue;
+        const long long g = (long long)kp * sz + goff[m];
+#pragma unroll
+        for (int q = 0; q < kGrArrays; ++q)
+          cp_async<4>(sb + (uint32_t)(q * kGrSP + soff[m]) * 4u, arr[q] + g);
+      }
+    }
+    cp_async_commit();
+  };
+#pragma unroll 1
+  for (int p = 0; p < 3 + kGrPF; ++p) issue(k0 + p);
+
+  const int own = (ty + 2) * kGrSX + tx + 2;
+  const long long ocol = (long long)j * sy + i;
+  // window: w[s][q'] = array WQ[q'] at (i, j, k - 2 + s)
+  float w[5][8];
+  if (active) {
+#pragma unroll
+    for (int s2 = 0; s2 < 4; ++s2)
+#pragma unroll
+      for (int q = 0; q < 8; ++q) w[s2][q] = arr[WQ[q]][(long long)(k0 - 2 + s2) * sz + ocol];
+  }
+#pragma unroll 1
+  for (int k = k0; k < k1; ++k) {
+    cp_async_wait<kGrPF>();  // planes up to k + 2 have landed
+    __syncthreads();
+    issue(k + 3 + kGrPF);    // into the slot of plane k - 1
+    if (active) {
+      const float* cs = ring + slot_of(k) * kGrArrays * kGrSP;
+      const float* c2 = ring + slot_of(k + 2) * kGrArrays * kGrSP;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) w[4][q] = c2[WQ[q] * kGrSP + own];
+      auto fetch = [&](auto qc, auto ac, int n) -> float {
+        constexpr int q = decltype(qc)::value, ax = decltype(ac)::value;
+        if constexpr (ax == 2) return w[2 + n][gr_wslot<q>()];
+        else if constexpr (ax == 0) return cs[q * kGrSP + own + n];
+        else return cs[q * kGrSP + own + n * kGrSX];
+      };
+      auto ownv = [&](int q) { return cs[q * kGrSP + own]; };
+      const float x = gr_pos(c, 0, i), y = gr_pos(c, 1, j), z = gr_pos(c, 2, k);
+      const Cks<float> m = metric_at(c, mt, i, j, k, x, y, z);
+      gr_stage_point<float, FIRST>(c, m, x, y, z, (long long)k * sz + ocol, fetch, ownv, out, du,
+                                   un, aux, As, Bs, flags, ehout);
+#pragma unroll
+      for (int s2 = 0; s2 < 4; ++s2)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) w[s2][q] = w[s2 + 1][q];
+    }
+  }
+  cp_async_wait<0>();
 }
 
 // Kreiss-Oliger pass (kernel_KO_step1_gr / _step2_gr, :523-608, with the

@@ -162,6 +162,37 @@ def test_gr_eh_from_the_writing_kernel_is_bitwise(dtype, monkeypatch):
         assert np.array_equal(a[k], b[k]), k
 
 
+def test_gr_tiled_stage_is_bitwise(monkeypatch):
+    """The FP32 stage streamed through shared-memory tiles gives bitwise the
+    fields of the per-point stage kernel: an 80^3 Wald run (two z chunks of
+    the tiled kernel, a ragged last one), both absorbing layers, the
+    near-horizon metric table, over several calls."""
+    p = problems.wald_params(N=80, half_size=10.0, a=0.9, pml=8)
+    f = [a.astype(np.float32) for a in problems.wald_fields(p, np.float64)]
+
+    def run(untiled):
+        monkeypatch.setenv("COFFEE_GR_TILED", "0" if untiled else "1")
+        env = SimEnvironment(p)
+        data = SimData(env, np.float32)
+        data.upload(f)
+        solver = FieldSolverGrEZ(data, env)
+        solver.set_aux(True)
+        solver.step(0.0, 3)
+        solver.step(0.0, 2)
+        out = data.download()
+        aux = data.download(("Jx", "Jy", "Jz", "divE", "divB"))
+        solver.close()
+        data.close()
+        env.close()
+        return out, aux
+
+    (a, xa), (b, xb) = run(False), run(True)
+    for k in range(7):
+        assert np.array_equal(a[k], b[k]), k
+    for k in range(5):
+        assert np.array_equal(xa[k], xb[k]), ("aux", k)
+
+
 FLAT_CASES = {
     "flat_pulsar": lambda: problems.pulsar_params(N=40, guard=3, half_size=10.0, radius=2.5,
                                                   omega=0.1, pml=6),
