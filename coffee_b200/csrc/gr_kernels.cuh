@@ -319,15 +319,14 @@ __device__ __noinline__ V7<T> gr_absorb(const GrConst<T>& c, V7<T> v, V7<T> n, T
 // the registers of the stencil sums).  Both stage kernels (global stencil
 // loads, shared-memory tiles) run this code, so their arithmetic is the
 // same.
-template <typename T, bool FIRST, typename Fetch, typename Own>
-__device__ __forceinline__ void gr_stage_point(const GrConst<T>& c, const Cks<T>& m, const T x,
+template <typename T, bool FIRST, typename Metric, typename Fetch, typename Own>
+__device__ __forceinline__ void gr_stage_point(const GrConst<T>& c, Metric&& metric, const T x,
                                                const T y, const T z, const long long o,
                                                Fetch&& f, Own&& own,
                                                const F7<T>& out, const F7<T>& du,
                                                const F7<T>& un, const F5<T>& aux, const T As,
                                                const T Bs, const int flags,
                                                const F7<T>& ehout) {
-  const T igms = T(1) / m.sg;
   auto d1 = [&](auto qc, auto ac) {
     constexpr int ax = decltype(ac)::value;
     return d1_4w(f(qc, ac, -2), f(qc, ac, -1), f(qc, ac, 1), f(qc, ac, 2)) * c.inv_delta[ax];
@@ -335,18 +334,21 @@ __device__ __forceinline__ void gr_stage_point(const GrConst<T>& c, const Cks<T>
   using I0 = std::integral_constant<int, 0>;
   using I1 = std::integral_constant<int, 1>;
   using I2 = std::integral_constant<int, 2>;
-  const T rotH[3] = {(d1(std::integral_constant<int, 5>{}, I1{}) -
-                      d1(std::integral_constant<int, 4>{}, I2{})) * igms,
-                     (d1(std::integral_constant<int, 3>{}, I2{}) -
-                      d1(std::integral_constant<int, 5>{}, I0{})) * igms,
-                     (d1(std::integral_constant<int, 4>{}, I0{}) -
-                      d1(std::integral_constant<int, 3>{}, I1{})) * igms};
-  const T rotE[3] = {(d1(std::integral_constant<int, 2>{}, I1{}) -
-                      d1(std::integral_constant<int, 1>{}, I2{})) * igms,
-                     (d1(std::integral_constant<int, 0>{}, I2{}) -
-                      d1(std::integral_constant<int, 2>{}, I0{})) * igms,
-                     (d1(std::integral_constant<int, 1>{}, I0{}) -
-                      d1(std::integral_constant<int, 0>{}, I1{})) * igms};
+  // the curls and divergences before their 1 / sqrt(gamma) factor: the
+  // metric is evaluated after the stencil sums, so that its values do not
+  // take registers while those are formed (the same operations either way)
+  T rotH[3] = {d1(std::integral_constant<int, 5>{}, I1{}) -
+                   d1(std::integral_constant<int, 4>{}, I2{}),
+               d1(std::integral_constant<int, 3>{}, I2{}) -
+                   d1(std::integral_constant<int, 5>{}, I0{}),
+               d1(std::integral_constant<int, 4>{}, I0{}) -
+                   d1(std::integral_constant<int, 3>{}, I1{})};
+  T rotE[3] = {d1(std::integral_constant<int, 2>{}, I1{}) -
+                   d1(std::integral_constant<int, 1>{}, I2{}),
+               d1(std::integral_constant<int, 0>{}, I2{}) -
+                   d1(std::integral_constant<int, 2>{}, I0{}),
+               d1(std::integral_constant<int, 1>{}, I0{}) -
+                   d1(std::integral_constant<int, 0>{}, I1{})};
   // div4 (:44-86): each neighbour weighted by sqrt(gamma) there (the
   // per-solver table; the reference evaluates it at the shifted coordinates)
   T divD = T(0), divB = T(0);
@@ -361,6 +363,13 @@ __device__ __forceinline__ void gr_stage_point(const GrConst<T>& c, const Cks<T>
     divB += d1_4w(f(QB{}, ac, -2) * w[0], f(QB{}, ac, -1) * w[1], f(QB{}, ac, 1) * w[2],
                   f(QB{}, ac, 2) * w[3]) * c.inv_delta[ax];
   });
+  const Cks<T> m = metric();
+  const T igms = T(1) / m.sg;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    rotH[a] *= igms;
+    rotE[a] *= igms;
+  }
   divD *= igms;
   divB *= igms;
   T v[7];
@@ -448,7 +457,7 @@ __global__ void __launch_bounds__(256, COFFEE_GR_STAGE_MIN_BLOCKS) gr_stage_kern
   const long long o = i + sy * j + sz * k;
   const long long st[3] = {sx, sy, sz};
   const T x = gr_pos(c, 0, i), y = gr_pos(c, 1, j), z = gr_pos(c, 2, k);
-  const Cks<T> m = metric_at(c, mt, i, j, k, x, y, z);
+  auto metric = [&]() { return metric_at(c, mt, i, j, k, x, y, z); };
   // the array pointers straight from the kernel parameters (a local array
   // of them would take registers this kernel does not have)
   auto fetch = [&](auto qc, auto ac, int n) {
@@ -460,7 +469,8 @@ __global__ void __launch_bounds__(256, COFFEE_GR_STAGE_MIN_BLOCKS) gr_stage_kern
     return __ldg(p + o + n * st[decltype(ac)::value]);
   };
   auto own = [&](int q) { return __ldg((q < 6 ? eh.p[q] : u.p[q - 6]) + o); };
-  gr_stage_point<T, FIRST>(c, m, x, y, z, o, fetch, own, out, du, un, aux, As, Bs, flags, ehout);
+  gr_stage_point<T, FIRST>(c, metric, x, y, z, o, fetch, own, out, du, un, aux, As, Bs, flags,
+                           ehout);
 }
 
 // The same stage streamed along z through shared memory (FP32; opt-in with
@@ -475,9 +485,9 @@ __global__ void __launch_bounds__(256, COFFEE_GR_STAGE_MIN_BLOCKS) gr_stage_kern
 // near-horizon table and the per-point reads and writes of dU, the
 // start-of-step copy, J and E, H keep the kernel latency-bound, and the
 // registers and shared memory of the tiles leave too few warps to hide it.
-// Measured at 256^3 (the Wald run): 5 slots and one CTA per SM (161
-// registers) 2.50 ms per stage, 4 slots and two CTAs per SM (128 registers)
-// 1.59 ms, the per-point gr_stage_kernel 1.28 ms, which stays the default.
+// Measured at 256^3 (the Wald run): 5 slots and one CTA per SM 2.50 ms per
+// stage, 4 slots and two CTAs per SM 1.61 ms, the per-point gr_stage_kernel
+// 1.09 ms, which stays the default.
 #ifndef COFFEE_GR_TILE_RING
 #define COFFEE_GR_TILE_RING 4
 #endif
@@ -583,9 +593,9 @@ __global__ void __launch_bounds__(kGrTX * kGrTY, COFFEE_GR_TILE_MINB) gr_stage_t
       };
       auto ownv = [&](int q) { return cs[q * kGrSP + own]; };
       const float x = gr_pos(c, 0, i), y = gr_pos(c, 1, j), z = gr_pos(c, 2, k);
-      const Cks<float> m = metric_at(c, mt, i, j, k, x, y, z);
-      gr_stage_point<float, FIRST>(c, m, x, y, z, (long long)k * sz + ocol, fetch, ownv, out, du,
-                                   un, aux, As, Bs, flags, ehout);
+      auto metric = [&]() { return metric_at(c, mt, i, j, k, x, y, z); };
+      gr_stage_point<float, FIRST>(c, metric, x, y, z, (long long)k * sz + ocol, fetch, ownv, out,
+                                   du, un, aux, As, Bs, flags, ehout);
 #pragma unroll
       for (int s2 = 0; s2 < 4; ++s2)
 #pragma unroll
