@@ -194,3 +194,29 @@ def test_env_create_rejects_bad_configs():
     h = ctypes.c_void_p()
     assert lib.coffee_env_create(ctypes.byref(cp), 0, ctypes.byref(h)) == -2
     assert b"guard" in lib.coffee_last_error_string()
+
+
+@pytest.mark.parametrize("k,c", [(16, 16), (32, 16), (16, 32), (32, 32), (16, 48), (64, 64)])
+def test_weight_gradient_workspace_covers_both_kernels(k, c):
+    """The workspace size the library reports holds the mma.sync kernel's
+    128 chunk partials and the tcgen05 kernel's per-CTA 128 x k partials
+    for one CTA per SM on up to 192 SMs, over every tap group."""
+    need_mma = 128 * k * 27 * c * 4
+    cbw = {16: 16, 32: 32, 48: 64, 64: 64}[c]
+    groups = -(-27 // (128 // cbw))
+    need_tc = max(1, 192 // groups) * groups * 128 * k * 4
+    got = _lib.load().coffee_conv3d_backward_weight_workspace(k, c)
+    assert got >= need_mma and got >= need_tc
+
+
+def test_surrogate_entry_points_reject_bad_sizes_without_a_gpu():
+    """Argument checks that come before any device work: too many bias
+    channels, unsupported channel counts of the tcgen05 weight gradient."""
+    lib = _lib.load()
+    fake = ctypes.c_void_p(16)  # never dereferenced: the checks fail first
+    rc = lib.coffee_bias_grad(fake, 100, 65, fake, None)
+    assert rc == -1 and b"64" in lib.coffee_last_error_string()
+    rc = lib.coffee_conv3d_backward_weight_tc(fake, fake, 1, 4, 4, 4, 16, 24, fake, fake, None)
+    assert rc == -1 and b"16, 32, 48 or 64" in lib.coffee_last_error_string()
+    rc = lib.coffee_conv3d_backward_weight_tc(fake, fake, 1, 4, 4, 4, 48, 16, fake, fake, None)
+    assert rc == -1 and b"output channels" in lib.coffee_last_error_string()
