@@ -494,6 +494,9 @@ int check_grid(int n, int d, int h, int w) {
 constexpr int kTcM = 128;                         // points per tile = MMA M
 constexpr int kTcStages = 8;                      // A ring slots at most
 constexpr int kTcSlot = 16384;                    // bytes of one A ring slot (64 channels)
+#ifndef COFFEE_TC_FWD_CTAS
+#define COFFEE_TC_FWD_CTAS 2
+#endif
 #ifndef COFFEE_TC_CB48
 #define COFFEE_TC_CB48 64
 #endif
@@ -897,20 +900,22 @@ int launch_fwd_tc(const bf16* x, Grid4 g, int C, const bf16* w, const float* bia
     return fail(COFFEE_E_TIMEOUT,
                 "an earlier tcgen05 convolution ran out of time waiting on its pipeline "
                 "(its results are invalid); clear the fault with coffee_conv3d_tc_fault");
-  // ring slots: as many as let two CTAs share an SM (113 KB each), at least
-  // two, at most kTcStages; with large weights one CTA per SM and a deeper ring
+  // CTAs per SM and ring slots: the most CTAs (up to COFFEE_TC_FWD_CTAS)
+  // whose shares of the SM's 228 KB (less 1 KB reserved per CTA) hold the
+  // weights and at least two slots; as many slots as fit, at most kTcStages
   const size_t wbytes = (size_t)27 * C * N * 2;
-  int nslots = (int)std::min<long long>(
-      kTcStages, ((long long)113 * 1024 - 1024 - (long long)wbytes) / kTcSlot);
-  if (nslots < 2)
-    nslots = (int)std::min<long long>(
-        kTcStages, ((long long)227 * 1024 - 1024 - (long long)wbytes) / kTcSlot);
+  int nslots = 0, ctas = COFFEE_TC_FWD_CTAS;
+  for (; ctas >= 1; --ctas) {
+    const long long share = std::min<long long>(227 * 1024, 228LL * 1024 / ctas - 1024);
+    nslots = (int)std::min<long long>(kTcStages, (share - 1024 - (long long)wbytes) / kTcSlot);
+    if (nslots >= 2) break;
+  }
   const size_t smem = 1024 + (size_t)nslots * kTcSlot + wbytes;
   // channels per TMA box: the widest that divides C; 48 channels in
   // COFFEE_TC_CB48-channel boxes: 64 (one box per tap, the last 16 channels
   // zero-filled and not multiplied) or 16 (three boxes per tap, no waste)
   const int cb = C == 48 ? COFFEE_TC_CB48 : (C % 64 == 0 ? 64 : (C % 32 == 0 ? 32 : 16));
-  if (nslots < 2 || smem > 227 * 1024)
+  if (ctas < 1 || nslots < 2 || smem > 227 * 1024)
     return fail(COFFEE_E_INVALID, "tcgen05 convolution: %d x %d weights exceed shared memory", N,
                 C);
   // the box: x extent a power of two in [8, 128], then y, then z
@@ -954,6 +959,10 @@ int launch_fwd_tc(const bf16* x, Grid4 g, int C, const bf16* w, const float* bia
   COFFEE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTcThreads, smem));
   // the resident CTAs of one SM must fit its 512 tensor-memory columns
   // together, so that no tcgen05.alloc waits
+  // the occupancy query reported one CTA per SM where the shared memory
+  // holds `ctas` (and two measured 1.2-1.6x faster): launch for the shared
+  // memory's count; CTAs that do not fit simply start later
+  per_sm = std::max(per_sm, ctas);
   per_sm = std::max(1, std::min(per_sm, 512 / (2 * (N <= 32 ? 32 : 64))));
   const long long ntiles = (long long)g.n * box.tx * box.ty * box.tz;
   const unsigned blocks = (unsigned)std::min<long long>(ntiles, (long long)sms * per_sm);

@@ -74,10 +74,10 @@ def conv_forward_tc(x, w_bf16, bias, k, act, z=None, a=None):
 
 
 def use_tc(c, k):
-    """True where the tcgen05 convolution is the faster one: inputs of 16, 32
-    or 64 channels (one TMA box of 16, 32 or 64 channels per tap); the results
-    are those of the mma.sync kernel."""
-    return c in (16, 32, 64) and k in (16, 32, 48, 64)
+    """True where the tcgen05 convolution runs (it is the faster one for every
+    layer of the network, the 48-channel input included since two CTAs share
+    an SM); its results are those of the mma.sync kernel."""
+    return c in (16, 32, 48, 64) and k in (16, 32, 48, 64)
 
 
 def use_tc_wgrad(c, k):
