@@ -989,13 +989,16 @@ int launch_fwd_tc(const bf16* x, Grid4 g, int C, const bf16* w, const float* bia
 // adds the partials of the point ranges in a fixed order (deterministic).
 // Roles, ring, bounded waits and the drain on a timeout are those of
 // conv3d_fwd_tc_kernel.
-constexpr int kWgTcStages = 4;
+constexpr int kWgTcStages = 4;  // ring slots at most
+#ifndef COFFEE_WG_CTAS
+#define COFFEE_WG_CTAS 2  // CTAs per SM when their rings fit
+#endif
 
 template <int CBW, int KN>
 __global__ void __launch_bounds__(kTcThreads) conv3d_wgrad_tc_kernel(
     const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap dymap,
     TcBox box, int ngroups, long long nboxes, long long per_chunk, float* __restrict__ part,
-    const TcWaitParams wp) {
+    const TcWaitParams wp, const int nslots) {
   static_assert(CBW == 16 || CBW == 32 || CBW == 64, "x boxes of 16, 32 or 64 channels");
   static_assert(KN == 16 || KN == 32 || KN == 64, "16, 32 or 64 output channels");
   constexpr int TPM = 128 / CBW;                        // taps per M tile
@@ -1055,6 +1058,7 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_wgrad_tc_kernel(
     x0 = (int)(r % box.tx) * box.bx;
   };
   const uint32_t nsteps = (uint32_t)max(0LL, b1 - b0);
+  const uint32_t stages = (uint32_t)nslots;
 
   if (warp == 4) {
     // ---- producer: per box, TPM shifted x boxes and the dy box into a slot
@@ -1062,11 +1066,9 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_wgrad_tc_kernel(
       uint32_t step = 0;
       const uint64_t xm = reinterpret_cast<uint64_t>(&xmap);
       const uint64_t dm = reinterpret_cast<uint64_t>(&dymap);
+      uint32_t b = 0, ph = 0;  // step % stages, (step / stages) & 1
       for (; step < nsteps && !wp.stall_producer; ++step) {
-        const uint32_t b = step % kWgTcStages;
-        if (step >= kWgTcStages &&
-            !tc_wait(empty0 + 8 * b, ((step / kWgTcStages) - 1) & 1, abort, wp))
-          break;
+        if (step >= stages && !tc_wait(empty0 + 8 * b, ph ^ 1u, abort, wp)) break;
         int n, x0, y0, z0;
         box_origin(b0 + step, n, x0, y0, z0);
         const uint32_t slot = base + b * kSlot;
@@ -1090,22 +1092,25 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_wgrad_tc_kernel(
             "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(slot + kAbytes),
             "l"(dm), "r"(0), "r"(x0), "r"(y0), "r"(z0), "r"(n), "r"(full0 + 8 * b)
             : "memory");
+        if (++b == stages) {
+          b = 0;
+          ph ^= 1u;
+        }
       }
       if (*abort) {
-        // the loads of the last kWgTcStages steps may be in flight
-        const uint32_t first = step > kWgTcStages ? step - kWgTcStages : 0;
+        // the loads of the last `stages` steps may be in flight
+        const uint32_t first = step > stages ? step - stages : 0;
         for (uint32_t s2 = first; s2 < step; ++s2)
-          tc_drain_wait(full0 + 8 * (s2 % kWgTcStages), (s2 / kWgTcStages) & 1);
+          tc_drain_wait(full0 + 8 * (s2 % stages), (s2 / stages) & 1);
       }
     }
   } else if (warp == 5) {
     // ---- MMA issuer: 8 MMAs of 16 points per box into one accumulator
     if (lane == 0) {
-      uint32_t step = 0;
+      uint32_t step = 0, b = 0, ph = 0;
       bool ok = true;
       for (; step < nsteps; ++step) {
-        const uint32_t b = step % kWgTcStages;
-        if (!tc_wait(full0 + 8 * b, (step / kWgTcStages) & 1, abort, wp)) {
+        if (!tc_wait(full0 + 8 * b, ph, abort, wp)) {
           ok = false;
           break;
         }
@@ -1127,6 +1132,10 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_wgrad_tc_kernel(
             "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                 empty0 + 8 * b)
             : "memory");
+        if (++b == stages) {
+          b = 0;
+          ph ^= 1u;
+        }
       }
       if (ok && nsteps > 0) {
         asm volatile(
@@ -1135,7 +1144,7 @@ __global__ void __launch_bounds__(kTcThreads) conv3d_wgrad_tc_kernel(
             : "memory");
       } else if (!ok && step > 0) {
         const uint32_t last = step - 1;
-        tc_drain_wait(empty0 + 8 * (last % kWgTcStages), (last / kWgTcStages) & 1);
+        tc_drain_wait(empty0 + 8 * (last % stages), (last / stages) & 1);
       }
     }
   } else {
@@ -1206,7 +1215,7 @@ size_t wgrad_tc_workspace(int K, int C) {
   const int cbw = wgrad_tc_cbw(C);
   if (!cbw) return 0;
   const int groups = (27 + 128 / cbw - 1) / (128 / cbw);
-  const long long chunks = std::max(1, kWgTcMaxSms / groups);
+  const long long chunks = std::max(1, COFFEE_WG_CTAS * kWgTcMaxSms / groups);
   return (size_t)chunks * groups * 128 * (size_t)K * sizeof(float);
 }
 
@@ -1233,9 +1242,19 @@ int launch_wgrad_tc(const bf16* dy, const bf16* x, Grid4 g, int C, float* dw, fl
   COFFEE_CUDA_TRY(cudaGetDevice(&dev));
   COFFEE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   sms = std::min(sms, kWgTcMaxSms);
-  // one CTA per SM (its ring takes most of the shared memory) over all tap
-  // groups, in one wave; every chunk non-empty
-  long long chunks = std::max(1LL, std::min(nboxes, (long long)(sms / groups)));
+  // two CTAs per SM when two rings of at least two slots fit (113 KB each),
+  // else one with up to kWgTcStages slots
+  const size_t slotb = 128u * 128u * 2u + 128u * KN * 2u;
+  int wctas = COFFEE_WG_CTAS, nslots = 0;
+  for (; wctas >= 1; --wctas) {
+    const long long share = std::min<long long>(227 * 1024, 228LL * 1024 / wctas - 1024);
+    nslots = (int)std::min<long long>(kWgTcStages, (share - 1024) / (long long)slotb);
+    if (nslots >= 2) break;
+  }
+  if (wctas < 1) return fail(COFFEE_E_INVALID, "tcgen05 weight gradient: ring exceeds shared memory");
+  const size_t smem = 1024 + (size_t)nslots * slotb;
+  // one wave of wctas CTAs per SM over all tap groups; every chunk non-empty
+  long long chunks = std::max(1LL, std::min(nboxes, (long long)(wctas * sms / groups)));
   const long long per_chunk = (nboxes + chunks - 1) / chunks;
   chunks = (nboxes + per_chunk - 1) / per_chunk;
   EncodeTiledFn enc;
@@ -1264,10 +1283,6 @@ int launch_wgrad_tc(const bf16* dy, const bf16* x, Grid4 g, int C, float* dw, fl
   CUtensorMap xmap, dymap;
   if (int rc = make(&xmap, x, C, CBW, swz(2 * CBW))) return rc;
   if (int rc = make(&dymap, dy, KN, KN, swz(2 * KN))) return rc;
-  // the ring, plus 32 KB of slack past it: the operands' last 8-row groups
-  // stay inside the allocation even if the descriptors' strides were read
-  // the other way round
-  const size_t smem = 1024 + (size_t)kWgTcStages * (128u * 128u * 2u + 128u * KN * 2u) + 32768;
   auto kern = conv3d_wgrad_tc_kernel<CBW, KN>;
   COFFEE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   COFFEE_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -1275,7 +1290,7 @@ int launch_wgrad_tc(const bf16* dy, const bf16* x, Grid4 g, int C, float* dw, fl
   const TcWaitParams wp{g_tc_cycles, g_tc_stall, g_tc_fault_dev};
   const long long blocks = chunks * groups;
   kern<<<(unsigned)blocks, kTcThreads, smem, st>>>(xmap, dymap, box, groups, nboxes, per_chunk,
-                                                   part, wp);
+                                                   part, wp, nslots);
   COFFEE_CUDA_TRY(cudaGetLastError());
   const long long nw = (long long)KN * 27 * C;
   wgrad_tc_reduce_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>(part, KN, C, CBW, groups,

@@ -200,11 +200,11 @@ def test_env_create_rejects_bad_configs():
 def test_weight_gradient_workspace_covers_both_kernels(k, c):
     """The workspace size the library reports holds the mma.sync kernel's
     128 chunk partials and the tcgen05 kernel's per-CTA 128 x k partials
-    for one CTA per SM on up to 192 SMs, over every tap group."""
+    for two CTAs per SM on up to 192 SMs, over every tap group."""
     need_mma = 128 * k * 27 * c * 4
     cbw = {16: 16, 32: 32, 48: 64, 64: 64}[c]
     groups = -(-27 // (128 // cbw))
-    need_tc = max(1, 192 // groups) * groups * 128 * k * 4
+    need_tc = max(1, 2 * 192 // groups) * groups * 128 * k * 4
     got = _lib.load().coffee_conv3d_backward_weight_workspace(k, c)
     assert got >= need_mma and got >= need_tc
 
