@@ -314,6 +314,31 @@ def test_training_lowers_the_loss():
 
 
 @pytest.mark.gpu
+def test_warm_start_on_device_matches_the_host_version():
+    """The GPU-resident warm start (the correction added in place to the
+    uploaded dipole) gives the fields of the host version, here for an
+    untrained network on a 96^3 rotator box (network grid 32^3)."""
+    from coffee_b200 import surrogate as sg
+    from coffee_b200.solver import SimData, SimEnvironment
+    p = sg.rotator_params(96, 38.0, 30.0)
+    start = sg.problems.pulsar_fields(p, np.float32)
+    net = sg.UNet(seed=3)
+    host = sg.upsampled_warm_start(net, p, start, 38.0)
+    env = SimEnvironment(p)
+    data = SimData(env, np.float32)
+    data.upload(start)
+    sg.warm_start_on_device(net, p, data, 38.0)
+    dev = data.download()
+    data.close()
+    env.close()
+    changed = 0
+    for c in range(7):
+        assert np.array_equal(dev[c], host[c]), c
+        changed += int((host[c] != start[c]).sum())
+    assert changed > 0
+
+
+@pytest.mark.gpu
 def test_rotator_warm_start_wall_time():
     """The warm start's measure on a reduced rotator: a 192^3 box (star of
     12 cells, R_LC = 30 cells, the network on the 64^3 grid), 4 training runs
