@@ -577,13 +577,15 @@ class _DeviceArray:
                                          "strides": None}
 
 
-def warm_start_on_device(net, p, data, incl):
+def warm_start_on_device(net, p, data, incl, alpha=1.0, comps=range(7)):
     """Add the network's correction to the fields in `data` (the rotator's
     vacuum dipole, already on the device), in place and on the GPU: the
     prediction on the coarse grid, trilinearly upsampled, scaled back by
     (R / R*)^-3 and added outside STAR_EDGE star radii and inside the
     absorbing layer's inner edge.  The same fields as upsampled_warm_start
-    without the host round trip of the full-resolution grid."""
+    without the host round trip of the full-resolution grid.  alpha scales
+    the correction and comps selects the fields it is added to (0-2 E,
+    3-5 B, 6 P)."""
     from .config import Grid
     torch = _torch()
     pc = coarse_params(p)
@@ -609,10 +611,11 @@ def warm_start_on_device(net, p, data, incl):
     keep = ((R > STAR_EDGE * p.radius) & (zf.abs()[:, None, None] < edge) &
             (yf.abs()[None, :, None] < edge) & (xf.abs()[None, None, :] < edge))
     g = p.guard[0]
-    for c in range(7):
+    for c in comps:
         f = torch.as_tensor(_DeviceArray(data.dev_ptr(c), data.shape), device="cuda")
         inner = f[g:-g, g:-g, g:-g]
-        inner += torch.where(keep, up[c], torch.zeros_like(up[c]))
+        add = up[c] if alpha == 1.0 else up[c] * alpha
+        inner += torch.where(keep, add, torch.zeros_like(add))
 
 
 def rotator_study(n_train=40, iters=2000, batch=2, train_periods=2.0, N=ROT_N,
